@@ -1,0 +1,198 @@
+/*
+ * api.cpp -- extern "C" surface of the oracle and its time integrator
+ * (TEST INFRASTRUCTURE).
+ *
+ * Restates:
+ *   TimeIntegrator_ExplicitEuler / WilliamsonRK3 / WilliamsonRK5
+ *                                   Approximation/DGTimeIntegrator.f90:263-365
+ *   TimeIntegrator_EstimateTimeStep (running maxima kept across calls, as the
+ *   reference's implicitly SAVEd umax/amax)  DGTimeIntegrator.f90:462-511
+ *   TimeIntegrator_Integrate (dt truncation at t_end, AlmostEqual end test,
+ *   re-estimate every 100 iterations, steady residual target)
+ *                                   DGTimeIntegrator.f90:159-255
+ *   Mesh_ComputeResiduals           Mesh/QuadMesh_Auxiliars.incf:22-38
+ */
+#include "oracle_internal.h"
+#include <cstring>
+#include <cstdio>
+#include <exception>
+
+using namespace orc;
+
+static void set_err(char* err, int len, const char* msg) {
+  if (err && len > 0) { std::strncpy(err, msg, len - 1); err[len - 1] = 0; }
+}
+
+extern "C" void* or_create(const or_case* c, const or_mesh* m, char* err, int errlen) {
+  try {
+    auto* o = new Oracle();
+    o->cas = *c;
+    o->bcs.assign(c->bcs, c->bcs + c->n_markers);
+    o->cas.bcs = o->bcs.data();
+    init_physics(*o);
+    build_mesh(*o, *m);
+    setup_zones(*o);
+    o->Q.assign(o->ndof, 0.0);
+    o->QDot.assign(o->ndof, 0.0);
+    o->dQ.assign(2 * o->ndof, 0.0);
+    o->G.assign(o->ndof, 0.0);
+    set_err(err, errlen, "");
+    return o;
+  } catch (const std::exception& ex) {
+    set_err(err, errlen, ex.what());
+    return nullptr;
+  }
+}
+
+extern "C" void or_destroy(void* h) { delete static_cast<Oracle*>(h); }
+extern "C" int64_t or_ndof(void* h) { return static_cast<Oracle*>(h)->ndof; }
+extern "C" int or_n_elements(void* h) { return int(static_cast<Oracle*>(h)->el.size()); }
+extern "C" int or_n_edges(void* h) { return int(static_cast<Oracle*>(h)->ed.size()); }
+
+extern "C" void or_element_orders(void* h, int* N) {
+  auto* o = static_cast<Oracle*>(h);
+  for (size_t e = 0; e < o->el.size(); ++e) N[e] = o->el[e].N;
+}
+
+extern "C" void or_node_coords(void* h, double* X) {
+  auto* o = static_cast<Oracle*>(h);
+  for (auto& e : o->el) {
+    const int64_t base = e.offset / 4;
+    for (int q = 0; q < e.P * e.P; ++q) { X[2 * (base + q)] = e.X[2 * q]; X[2 * (base + q) + 1] = e.X[2 * q + 1]; }
+  }
+}
+
+extern "C" void or_set_state(void* h, const double* Q) {
+  auto* o = static_cast<Oracle*>(h);
+  std::memcpy(o->Q.data(), Q, sizeof(double) * o->ndof);
+}
+extern "C" void or_get_state(void* h, double* Q) {
+  auto* o = static_cast<Oracle*>(h);
+  std::memcpy(Q, o->Q.data(), sizeof(double) * o->ndof);
+}
+extern "C" void or_get_qdot(void* h, double* QDot) {
+  auto* o = static_cast<Oracle*>(h);
+  std::memcpy(QDot, o->QDot.data(), sizeof(double) * o->ndof);
+}
+
+extern "C" void or_time_derivative(void* h, double t) { time_derivative(*static_cast<Oracle*>(h), t); }
+
+extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const int64_t n = o.ndof;
+  double* Q = o.Q.data();
+  double* G = o.G.data();
+  const double* QD = o.QDot.data();
+  if (scheme == OR_SCHEME_EULER) {
+    time_derivative(o, t);
+    for (int64_t i = 0; i < n; ++i) Q[i] = Q[i] + dt * QD[i];
+  } else if (scheme == OR_SCHEME_RK3) {
+    const double am[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    const double cm[3] = {0.0, 1.0 / 3.0, 3.0 / 4.0};
+    for (int m = 0; m < 3; ++m) {
+      time_derivative(o, t + dt * cm[m]);
+      if (m == 0) for (int64_t i = 0; i < n; ++i) G[i] = QD[i];
+      else for (int64_t i = 0; i < n; ++i) G[i] = am[m] * G[i] + QD[i];
+      for (int64_t i = 0; i < n; ++i) Q[i] = Q[i] + gm[m] * dt * G[i];
+    }
+  } else {
+    const double am[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
+    const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
+    const double cm[5] = {0.0, 0.1496590219993, 0.3704009573644, 0.6222557631345, 0.9582821306748};
+    for (int m = 0; m < 5; ++m) {
+      time_derivative(o, t + dt * cm[m]);
+      if (m == 0) {
+        for (int64_t i = 0; i < n; ++i) G[i] = dt * QD[i];
+        for (int64_t i = 0; i < n; ++i) Q[i] = Q[i] + gm[m] * G[i];
+      } else {
+        for (int64_t i = 0; i < n; ++i) {
+          G[i] = am[m] * G[i] + dt * QD[i];
+          Q[i] = Q[i] + gm[m] * G[i];
+        }
+      }
+    }
+  }
+}
+
+extern "C" double or_estimate_dt(void* h, double cfl, double dt_cap) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const Physics& ph = o.ph;
+  double dt = dt_cap;
+  for (auto& e : o.el) {
+    const double* Q = &o.Q[e.offset];
+    for (int i = 0; i < e.P; ++i)
+      for (int j = 0; j < e.P; ++j) {
+        const double* q = &Q[4 * (j * e.P + i)];
+        const double nrm = std::sqrt(q[1] * q[1] + q[2] * q[2]);
+        o.save_umax = std::fmax(o.save_umax, nrm / q[0]);
+        const double u = q[1] / q[0], v = q[2] / q[0];
+        o.save_amax = std::fmax(o.save_amax, std::sqrt(ph.gamma * ph.gm1 * (q[3] / q[0] - 0.5 * (u * u) - 0.5 * (v * v))));
+      }
+    auto dist = [&](int a, int b) {
+      const double dx = o.nodeX[2 * e.nodes[a]] - o.nodeX[2 * e.nodes[b]];
+      const double dy = o.nodeX[2 * e.nodes[a] + 1] - o.nodeX[2 * e.nodes[b] + 1];
+      return std::sqrt(dx * dx + dy * dy);
+    };
+    const double dx = std::fmin(std::fmin(dist(0, 1), dist(1, 2)), std::fmin(dist(2, 3), dist(0, 3)));
+    dt = std::fmin(dt, ph.Mach * std::sqrt(ph.gamma) * cfl * dx / (o.save_umax + o.save_amax) / (e.N + 1));
+  }
+  return dt;
+}
+
+extern "C" void or_residuals(void* h, double out[4]) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  for (int k = 0; k < 4; ++k) out[k] = 0.0;
+  for (int64_t i = 0; i < o.ndof; ++i) out[i % 4] = std::fmax(out[i % 4], std::fabs(o.QDot[i]));
+}
+
+extern "C" int or_integrate(void* h, int scheme, int mode, double t0, double t_end, int max_iter,
+                            double cfl, double dt_cap, double residual_target, double* t_out) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  double t = t0;
+  double dt = or_estimate_dt(h, cfl, dt_cap);
+  int iter = 0;
+  for (iter = 1; iter <= max_iter; ++iter) {
+    if (mode == 1 && t + dt >= t_end) dt = t_end - t;
+    or_time_step(h, scheme, t, dt);
+    t = t + dt;
+    if (mode == 1 && almost_equal(t, t_end)) break;
+    if (iter % 100 == 0) dt = or_estimate_dt(h, cfl, dt_cap);
+    if (mode == 0) {
+      double r[4];
+      or_residuals(h, r);
+      const double mx = std::fmax(std::fmax(std::fabs(r[0]), std::fabs(r[1])), std::fmax(std::fabs(r[2]), std::fabs(r[3])));
+      if (mx < residual_target) break;
+    }
+  }
+  if (iter > max_iter) iter = max_iter;
+  if (t_out) *t_out = t;
+  (void)o;
+  return iter;
+}
+
+extern "C" void or_ref_values(void* h, double out[8]) {
+  const Physics& ph = static_cast<Oracle*>(h)->ph;
+  out[0] = ph.rho; out[1] = ph.a; out[2] = ph.p; out[3] = ph.V; out[4] = ph.T; out[5] = ph.L; out[6] = ph.mu;
+  out[7] = ph.invSqrtGammaMach;
+}
+
+extern "C" void or_element_geometry(void* h, double* Ja, double* jac, double* volume) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    const Element& e = o.el[ei];
+    const int64_t base = e.offset / 4;
+    for (int q = 0; q < e.P * e.P; ++q) {
+      for (int k = 0; k < 4; ++k) Ja[4 * (base + q) + k] = e.Ja[4 * q + k];
+      jac[base + q] = e.jac[q];
+    }
+    volume[ei] = e.volume;
+  }
+}
+
+extern "C" int or_edge_count_by_type(void* h, int type) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  int c = 0;
+  for (auto& f : o.ed) if (int(f.kind) == type) ++c;
+  return c;
+}

@@ -1,0 +1,103 @@
+/*
+ * oracle_api.h -- C interface of the CPU FP64 oracle.
+ *
+ * TEST INFRASTRUCTURE ONLY.  The oracle is a plain C++ restatement of the
+ * HORSES2D DGSEM residual and time integrator (Fortran reference), used by
+ * tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py as the
+ * checker.  Nothing in the product package links or calls it.
+ *
+ * Conventions follow the reference:
+ *   - state Q is the flat Storage%Q array (Generic/Storage.f90:31-73): element
+ *     e occupies NCONS*(N_e+1)^2 doubles at offset 4*cumP2(e-1), laid out
+ *     Q[e][eta][xi][var] in C order (var fastest);
+ *   - mesh arrays are the .HiOMesh NetCDF variables with 1-based node ids
+ *     (Mesh/MeshFile.f90:77-279).
+ */
+#ifndef HG_ORACLE_API_H
+#define HG_ORACLE_API_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Boundary-condition kinds (Generic/Defines.h FACE_INTERIOR .. NEWDIRICHLET_BC). */
+enum { OR_BC_PERIODIC = 1, OR_BC_DIRICHLET = 2, OR_BC_EULERWALL = 3, OR_BC_VISCOUSWALL = 4,
+       OR_BC_FARFIELD = 5, OR_BC_PRESSUREOUTLET = 6 };
+/* Riemann solvers (Physics/RiemannSolvers.f90); LXF is new (no reference). */
+enum { OR_RIEMANN_ROE = 0, OR_RIEMANN_HLL = 1, OR_RIEMANN_EXACT = 2, OR_RIEMANN_LXF = 3,
+       OR_RIEMANN_INTERIOR = -1 };
+enum { OR_NODES_LG = 1, OR_NODES_LGL = 2 };
+enum { OR_SCHEME_EULER = 0, OR_SCHEME_RK3 = 1, OR_SCHEME_RK5 = 2 };
+enum { OR_VISC_BR1 = 0, OR_VISC_IP = 1 };
+enum { OR_IP_SIPG = 0, OR_IP_NIPG = 1, OR_IP_IIPG = 2 };
+
+typedef struct {
+  int    type;              /* OR_BC_* */
+  int    riemann;           /* per-zone solver override, OR_RIEMANN_INTERIOR = use interior one */
+  int    periodic_dir;      /* 1 = x, 2 = y */
+  int    connected_marker;  /* periodic partner marker (1-based) */
+  double pressure;          /* Dirichlet / farfield / outlet, dimensional Pa (<=0: reference) */
+  double temperature;       /* K (<=0: reference) */
+  double mach;              /* (<0: case Mach) */
+  double aoa_deg;           /* angle of attack, degrees */
+  int    wall_type;         /* viscous wall: 1 isothermal, 2 adiabatic */
+  double wall_T;            /* isothermal wall temperature, K */
+  double wall_v[2];         /* wall velocity, m/s */
+  int    outflow_type;      /* pressure outlet: 1 reflective, 2 partially non-reflective */
+} or_bc;
+
+typedef struct {
+  int    nodes;             /* OR_NODES_LG / OR_NODES_LGL */
+  int    riemann;           /* interior Riemann solver */
+  int    navier_stokes;     /* 0: Euler build, 1: Navier-Stokes build */
+  int    viscous;           /* OR_VISC_BR1 / OR_VISC_IP */
+  int    ip_method;         /* OR_IP_* */
+  double sigma0_ip;         /* jumps penalty parameter */
+  double sigma1_ip;         /* gradient jumps penalty parameter */
+  double mach, reynolds, prandtl;
+  double pressure_ref, temperature_ref, reynolds_length;
+  int    n_markers;
+  const or_bc* bcs;         /* [n_markers], zone k+1 */
+} or_case;
+
+typedef struct {
+  int n_nodes, n_elements, n_bdry_edges;
+  const double* points;       /* [n_nodes][2], dimensional */
+  const int*    quads;        /* [n_elements][4], 1-based */
+  const int*    bdry_edges;   /* [n_bdry_edges][2], 1-based */
+  const int*    bdry_marker;  /* [n_bdry_edges] */
+  int n_curved, curve_np1;
+  const int*    curved_edges; /* [n_curved][2], 1-based */
+  const double* curve_x;      /* [n_curved][curve_np1], dimensional */
+  const double* curve_y;
+  const int*    poly_order;   /* [n_elements] */
+} or_mesh;
+
+void*   or_create(const or_case* c, const or_mesh* m, char* err, int errlen);
+void    or_destroy(void* h);
+int64_t or_ndof(void* h);
+int     or_n_elements(void* h);
+int     or_n_edges(void* h);
+void    or_element_orders(void* h, int* N_out);
+void    or_node_coords(void* h, double* X);                /* [ndof/4][2] dimensionless */
+void    or_set_state(void* h, const double* Q);
+void    or_get_state(void* h, double* Q);
+void    or_get_qdot(void* h, double* QDot);
+void    or_time_derivative(void* h, double t);
+void    or_time_step(void* h, int scheme, double t, double dt);
+double  or_estimate_dt(void* h, double cfl, double dt_cap);
+void    or_residuals(void* h, double out[4]);
+/* Reference TimeIntegrator_Integrate (Approximation/DGTimeIntegrator.f90:159-255):
+ * mode 1 transient, 0 steady.  Returns the number of iterations run. */
+int     or_integrate(void* h, int scheme, int mode, double t0, double t_end, int max_iter,
+                     double cfl, double dt_cap, double residual_target, double* t_out);
+/* Physics constants resolved by InitializePhysics (Physics/PhysicsNS.f90:405-481). */
+void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless, invSqrtGammaMach */
+/* Geometry export for cross-checking host-side mesh builders. */
+void    or_element_geometry(void* h, double* Ja, double* jac, double* volume); /* Ja [ndof/4][2][2], jac [ndof/4], volume [E] */
+int     or_edge_count_by_type(void* h, int type);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
