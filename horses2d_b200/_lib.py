@@ -1,0 +1,80 @@
+"""ctypes binding of libhorsesgpu.so (C ABI declared in include/horses_gpu.h).
+
+The shared library is built in-tree by ``horses2d_b200.build`` (nvcc, sm_100a).
+There is no CPU fallback: if the library or a Blackwell GPU is missing, calls
+raise.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhorsesgpu.so")
+
+NODES_LG, NODES_LGL = 1, 2
+ROE, HLL, EXACT, LXF, INTERIOR = 0, 1, 2, 3, -1
+SCHEME_EULER, SCHEME_RK3, SCHEME_RK5 = 0, 1, 2
+PREC_FP64, PREC_FP32 = 0, 1
+BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL, BC_FARFIELD, BC_PRESSUREOUTLET = 1, 2, 3, 4, 5, 6
+
+I32P = C.POINTER(C.c_int32)
+F64P = C.POINTER(C.c_double)
+
+
+class PhysicsDesc(C.Structure):
+    _fields_ = [("node_type", C.c_int32), ("riemann", C.c_int32), ("navier_stokes", C.c_int32),
+                ("viscous", C.c_int32), ("mach", C.c_double), ("reynolds", C.c_double), ("prandtl", C.c_double),
+                ("pressure_ref", C.c_double), ("temperature_ref", C.c_double), ("reynolds_length", C.c_double),
+                ("gamma", C.c_double), ("gas_R", C.c_double)]
+
+
+class BCDesc(C.Structure):
+    _fields_ = [("type", C.c_int32), ("riemann", C.c_int32), ("state", C.c_double * 4), ("wall_T", C.c_double),
+                ("wall_type", C.c_int32), ("outflow_type", C.c_int32)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_elements", C.c_int32), ("n_edges", C.c_int32), ("N", I32P), ("Ja", F64P), ("jac", F64P),
+                ("x", F64P), ("volume", F64P), ("vertices", F64P), ("edge_elem", I32P), ("edge_side", I32P),
+                ("edge_inverse", I32P), ("edge_marker", I32P), ("edge_n", F64P), ("edge_dS", F64P),
+                ("periodic_partner", I32P), ("edge_invh", F64P)]
+
+
+_lib = None
+EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_state", "hg_ndof",
+            "hg_time_derivative", "hg_time_step", "hg_time_steps", "hg_residuals", "hg_estimate_dt",
+            "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count")
+
+
+def load():
+    """Load the in-tree CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m horses2d_b200.build` "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.hg_create.restype = C.c_int
+    L.hg_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(PhysicsDesc), C.POINTER(BCDesc), C.c_int32, C.c_int32,
+                            C.POINTER(vp)]
+    L.hg_destroy.argtypes = [vp]
+    L.hg_last_error.restype = C.c_char_p
+    L.hg_last_error.argtypes = [vp]
+    L.hg_set_state.argtypes = [vp, F64P, C.c_int64]
+    L.hg_get_state.argtypes = [vp, F64P, C.c_int64]
+    L.hg_ndof.restype = C.c_int64
+    L.hg_ndof.argtypes = [vp]
+    L.hg_time_derivative.argtypes = [vp, C.c_double, F64P]
+    L.hg_time_step.argtypes = [vp, C.c_int32, C.c_double, C.c_double]
+    L.hg_time_steps.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+    L.hg_residuals.argtypes = [vp, F64P]
+    L.hg_estimate_dt.argtypes = [vp, C.c_double, C.c_double, F64P]
+    L.hg_set_stream.argtypes = [vp, vp]
+    L.hg_synchronize.argtypes = [vp]
+    L.hg_device_state.restype = C.c_void_p
+    L.hg_device_state.argtypes = [vp]
+    L.hg_launch_count.restype = C.c_int64
+    L.hg_launch_count.argtypes = [vp]
+    _lib = L
+    return L

@@ -1,0 +1,465 @@
+// hg_api.cu -- C ABI of libhorsesgpu.so (declared in include/horses_gpu.h).
+//
+// Host responsibilities: validate the flattened mesh, turn the reference's
+// edge-centric connectivity (mesh%edges, Mesh/QuadElement.f90:95-135 after
+// Edge_LinkWithElements / Zone_LinkPeriodicZones) into per-element side tables,
+// upload everything once, and sequence the stage kernels of the low-storage
+// Runge-Kutta schemes (Approximation/DGTimeIntegrator.f90:263-365).
+#include "../../include/horses_gpu.h"
+#include "hg_stage.cuh"
+#include "hg_spectral.h"
+
+#include <cuda_runtime.h>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <stdexcept>
+#include <cmath>
+#include <algorithm>
+
+using namespace hg;
+
+struct hg_ctx {
+  std::string err;
+  int n_el = 0, N = 0, P = 0, node_type = 0, precision = 0, riemann = 0;
+  int64_t ndof = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  PhysConst pc{};
+  double mach = 0, gamma = 1.4;
+  // device buffers
+  int4* d_side = nullptr;
+  double* d_side_geo = nullptr;
+  double* d_vol_geo = nullptr;
+  double* d_mats = nullptr;
+  Zone* d_zones = nullptr;
+  double* d_Q = nullptr;
+  void* d_G = nullptr;
+  void* d_T[2] = {nullptr, nullptr};
+  double* d_QDot = nullptr;
+  unsigned long long* d_resid = nullptr;
+  double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
+  int cur = 0;                    // which trace buffer holds the current traces
+  bool state_set = false;
+  int64_t launches = 0;
+  std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
+  double save_umax = 0.0, save_amax = 0.0;
+};
+
+static std::string g_create_err;
+
+#define HG_CUDA(call)                                                                           \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int fail(hg_ctx* c, const std::exception& ex) {
+  if (c) c->err = ex.what();
+  return 1;
+}
+
+template <typename T>
+static T* dalloc(size_t n) {
+  void* p = nullptr;
+  HG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+static void free_ctx(hg_ctx* c) {
+  if (!c) return;
+  void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
+                  c->d_QDot, c->d_resid, c->d_elmax};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+// ------------------------------------------------------------------ launches
+constexpr int epb_for(int P) {
+  return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : 3;
+}
+
+template <int P, typename real>
+static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
+  constexpr int EPB = epb_for(P);
+  dim3 block(P * P, EPB), grid((a.n_el + EPB - 1) / EPB);
+  stage_kernel<P, EPB, real><<<grid, block, 0, c->stream>>>(a);
+  ++c->launches;
+}
+
+template <int P, typename real>
+static void launch_trace_P(hg_ctx* c) {
+  constexpr int EPB = epb_for(P);
+  dim3 block(P * P, EPB), grid((c->n_el + EPB - 1) / EPB);
+  trace_kernel<P, EPB, real><<<grid, block, 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats, static_cast<real*>(c->d_T[c->cur]));
+  ++c->launches;
+}
+
+#define HG_DISPATCH_P(P_, FN, ...)                      \
+  switch (P_) {                                         \
+    case 2: FN<2, real>(__VA_ARGS__); break;            \
+    case 3: FN<3, real>(__VA_ARGS__); break;            \
+    case 4: FN<4, real>(__VA_ARGS__); break;            \
+    case 5: FN<5, real>(__VA_ARGS__); break;            \
+    case 6: FN<6, real>(__VA_ARGS__); break;            \
+    case 7: FN<7, real>(__VA_ARGS__); break;            \
+    case 8: FN<8, real>(__VA_ARGS__); break;            \
+    case 9: FN<9, real>(__VA_ARGS__); break;            \
+    default: throw std::runtime_error("unsupported polynomial order"); \
+  }
+
+template <typename real>
+static void run_trace(hg_ctx* c) { HG_DISPATCH_P(c->P, launch_trace_P, c); }
+
+template <typename real>
+static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+  StageArgs<real> a{};
+  a.n_el = c->n_el;
+  a.side = c->d_side;
+  a.side_geo = c->d_side_geo;
+  a.vol_geo = c->d_vol_geo;
+  a.mats = c->d_mats;
+  a.zones = c->d_zones;
+  a.Q = c->d_Q;
+  a.G = static_cast<real*>(c->d_G);
+  a.T_in = static_cast<const real*>(c->d_T[c->cur]);
+  a.T_out = static_cast<real*>(c->d_T[c->cur ^ 1]);
+  a.QDot = qdot;
+  a.resid = resid ? c->d_resid : nullptr;
+  a.a = ca; a.b = cb; a.c = cc;
+  a.first = first ? 1 : 0;
+  a.update = update ? 1 : 0;
+  a.riemann = c->riemann;
+  a.pc = c->pc;
+  HG_DISPATCH_P(c->P, launch_stage_P, c, a);
+  if (update) c->cur ^= 1;
+}
+
+static void stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+  if (c->precision == HG_PREC_FP32) run_stage<float>(c, ca, cb, cc, first, update, qdot, resid);
+  else run_stage<double>(c, ca, cb, cc, first, update, qdot, resid);
+}
+
+static void traces(hg_ctx* c) {
+  if (c->precision == HG_PREC_FP32) run_trace<float>(c);
+  else run_trace<double>(c);
+}
+
+// One step of a reference scheme; residual maxima are collected on the last stage.
+static void one_step(hg_ctx* c, int scheme, double t, double dt) {
+  (void)t;
+  if (scheme == HG_SCHEME_EULER) {
+    HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
+    stage(c, 0.0, dt, 1.0, true, true, nullptr, true);
+  } else if (scheme == HG_SCHEME_RK3) {
+    const double am[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    for (int m = 0; m < 3; ++m) {
+      if (m == 2) HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
+      stage(c, am[m], 1.0, gm[m] * dt, m == 0, true, nullptr, m == 2);
+    }
+  } else if (scheme == HG_SCHEME_RK5) {
+    const double am[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
+    const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
+    for (int m = 0; m < 5; ++m) {
+      if (m == 4) HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
+      stage(c, am[m], dt, gm[m], m == 0, true, nullptr, m == 4);
+    }
+  } else {
+    throw std::runtime_error("unknown time scheme");
+  }
+}
+
+// ------------------------------------------------------------------ dt estimate
+__global__ void element_speed_kernel(int n_el, int NP, const double* Q, double gamma, double gm1, double* out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n_el) return;
+  double um = 0.0, am = 0.0;
+  const double* q = Q + size_t(e) * NP * 4;
+  for (int n = 0; n < NP; ++n, q += 4) {
+    const double nrm = sqrt(q[1] * q[1] + q[2] * q[2]);
+    um = fmax(um, nrm / q[0]);
+    const double u = q[1] / q[0], v = q[2] / q[0];
+    am = fmax(am, sqrt(gamma * gm1 * (q[3] / q[0] - 0.5 * (u * u) - 0.5 * (v * v))));
+  }
+  out[2 * e] = um;
+  out[2 * e + 1] = am;
+}
+
+// ------------------------------------------------------------------ creation
+static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
+  if (!m || !ph) throw std::runtime_error("null descriptor");
+  int dev = 0;
+  HG_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  HG_CUDA(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) throw std::runtime_error("libhorsesgpu requires an sm_100 (Blackwell) device");
+  const int E = m->n_elements;
+  if (E <= 0) throw std::runtime_error("mesh has no elements");
+  const int N = m->N[0];
+  for (int e = 0; e < E; ++e)
+    if (m->N[e] != N) throw std::runtime_error("mixed polynomial orders are not supported by this kernel set");
+  if (N < 1 || N > 8) throw std::runtime_error("polynomial order must be in 1..8");
+  if (ph->navier_stokes && ph->reynolds != 0.0)
+    throw std::runtime_error("viscous terms are not available in this kernel set (Reynolds number must be 0)");
+  const int P = N + 1, NP = P * P;
+  c->n_el = E; c->N = N; c->P = P; c->node_type = ph->node_type; c->riemann = ph->riemann;
+  if (c->riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
+  c->ndof = int64_t(E) * NP * 4;
+  const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
+  c->gamma = gamma; c->mach = ph->mach;
+  c->pc.gamma = gamma;
+  c->pc.gm1 = gamma - 1.0;
+  c->pc.cp = gamma / (gamma - 1.0);
+  c->pc.cv = 1.0 / (gamma - 1.0);
+  c->pc.invSqrtGammaMach = 1.0 / (std::sqrt(gamma) * ph->mach);
+
+  // nodal operators
+  NodalOps ops = make_nodal_ops(N, ph->node_type);
+  std::vector<double> mats;
+  mats.insert(mats.end(), ops.hatD.begin(), ops.hatD.end());
+  mats.insert(mats.end(), ops.lb0.begin(), ops.lb0.end());
+  mats.insert(mats.end(), ops.lb1.begin(), ops.lb1.end());
+  mats.insert(mats.end(), ops.lbw0.begin(), ops.lbw0.end());
+  mats.insert(mats.end(), ops.lbw1.begin(), ops.lbw1.end());
+
+  // volume metrics
+  std::vector<double> vg(size_t(E) * NP * 5);
+  for (size_t n = 0; n < size_t(E) * NP; ++n) {
+    for (int k = 0; k < 4; ++k) vg[n * 5 + k] = m->Ja[n * 4 + k];
+    if (!(m->jac[n] > 0.0)) throw std::runtime_error("non-positive mapping jacobian");
+    vg[n * 5 + 4] = 1.0 / m->jac[n];
+  }
+
+  // zones
+  std::vector<Zone> zones(std::max(1, n_bcs));
+  for (int z = 0; z < n_bcs; ++z) {
+    zones[z].type = bcs[z].type;
+    zones[z].riemann = bcs[z].riemann;
+    for (int k = 0; k < 4; ++k) zones[z].q[k] = bcs[z].state[k];
+    if (bcs[z].riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
+  }
+
+  // side tables
+  std::vector<int4> side(size_t(E) * 4, make_int4(-2, 0, -1, 0));
+  std::vector<double> sg(size_t(E) * 4 * P * 3, 0.0);
+  auto set_geo = [&](int e, int s, int edge, bool rev) {
+    for (int k = 0; k < P; ++k) {
+      const int cidx = rev ? (P - 1 - k) : k;
+      double* g = &sg[((size_t(e) * 4 + s) * P + k) * 3];
+      g[0] = m->edge_n[(size_t(edge) * P + cidx) * 2];
+      g[1] = m->edge_n[(size_t(edge) * P + cidx) * 2 + 1];
+      g[2] = m->edge_dS[size_t(edge) * P + cidx];
+    }
+  };
+  for (int f = 0; f < m->n_edges; ++f) {
+    const int L = m->edge_elem[2 * f], R = m->edge_elem[2 * f + 1];
+    const int sL = m->edge_side[2 * f] - 1, sR = m->edge_side[2 * f + 1] - 1;
+    const bool inv = m->edge_inverse[f] != 0;
+    if (L < 0 || L >= E || sL < 0 || sL > 3) throw std::runtime_error("bad edge connectivity");
+    const int marker = m->edge_marker[f];
+    if (marker == 0) {
+      if (R < 0 || R >= E || sR < 0 || sR > 3) throw std::runtime_error("interior edge without RIGHT element");
+      side[size_t(L) * 4 + sL] = make_int4(R * 4 + sR, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), -1, 0);
+      side[size_t(R) * 4 + sR] = make_int4(L * 4 + sL, SIDE_RIGHT | (inv ? SIDE_REVERSED : 0), -1, 0);
+      set_geo(L, sL, f, false);
+      set_geo(R, sR, f, inv);
+    } else {
+      if (marker < 1 || marker > n_bcs) throw std::runtime_error("boundary edge with unknown marker");
+      const hg_bc_desc& b = bcs[marker - 1];
+      const int z = marker - 1;
+      switch (b.type) {
+        case HG_BC_PERIODIC: {
+          const int p = m->periodic_partner ? m->periodic_partner[f] : -1;
+          if (p < 0 || p >= m->n_edges) throw std::runtime_error("periodic edge without partner");
+          const int pe = m->edge_elem[2 * p], ps = m->edge_side[2 * p] - 1;
+          side[size_t(L) * 4 + sL] = make_int4(pe * 4 + ps, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), z, 0);
+          break;
+        }
+        case HG_BC_EULERWALL: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_WALL, z, 0); break;
+        case HG_BC_DIRICHLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
+        default: throw std::runtime_error("boundary condition kind not available on the device in this kernel set");
+      }
+      set_geo(L, sL, f, false);
+    }
+  }
+  for (size_t s = 0; s < side.size(); ++s)
+    if (side[s].x == -2) throw std::runtime_error("element side not covered by any edge");
+
+  // dt support: corner distances
+  c->dx.assign(E, 0.0);
+  if (m->vertices) {
+    for (int e = 0; e < E; ++e) {
+      const double* v = m->vertices + size_t(e) * 8;
+      auto d = [&](int a, int b) { return std::sqrt((v[2 * a] - v[2 * b]) * (v[2 * a] - v[2 * b]) + (v[2 * a + 1] - v[2 * b + 1]) * (v[2 * a + 1] - v[2 * b + 1])); };
+      c->dx[e] = std::fmin(std::fmin(d(0, 1), d(1, 2)), std::fmin(d(2, 3), d(0, 3)));
+    }
+  }
+
+  HG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->own_stream = true;
+  const size_t rs = c->precision == HG_PREC_FP32 ? sizeof(float) : sizeof(double);
+  c->d_side = dalloc<int4>(side.size());
+  c->d_side_geo = dalloc<double>(sg.size());
+  c->d_vol_geo = dalloc<double>(vg.size());
+  c->d_mats = dalloc<double>(mats.size());
+  c->d_zones = dalloc<Zone>(zones.size());
+  c->d_Q = dalloc<double>(c->ndof);
+  c->d_G = dalloc<char>(c->ndof * rs);
+  c->d_T[0] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
+  c->d_T[1] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
+  c->d_QDot = dalloc<double>(c->ndof);
+  c->d_resid = dalloc<unsigned long long>(4);
+  c->d_elmax = dalloc<double>(size_t(E) * 2);
+  HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  HG_CUDA(cudaMemcpy(c->d_side_geo, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice));
+  HG_CUDA(cudaMemcpy(c->d_vol_geo, vg.data(), vg.size() * sizeof(double), cudaMemcpyHostToDevice));
+  HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
+  HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
+  HG_CUDA(cudaMemset(c->d_resid, 0, 4 * sizeof(unsigned long long)));
+}
+
+extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, const hg_bc_desc* bcs, int32_t n_bcs,
+                         int32_t precision, hg_ctx** out) {
+  if (!out) return 1;
+  *out = nullptr;
+  hg_ctx* c = new hg_ctx();
+  c->precision = precision;
+  try {
+    if (precision != HG_PREC_FP64 && precision != HG_PREC_FP32) throw std::runtime_error("unknown precision");
+    build(c, mesh, phys, bcs, n_bcs);
+  } catch (const std::exception& ex) {
+    g_create_err = ex.what();
+    free_ctx(c);
+    delete c;
+    return 1;
+  }
+  g_create_err.clear();
+  *out = c;
+  return 0;
+}
+
+extern "C" void hg_destroy(hg_ctx* c) {
+  if (!c) return;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_ctx(c);
+  delete c;
+}
+
+extern "C" const char* hg_last_error(const hg_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
+extern "C" int64_t hg_ndof(const hg_ctx* c) { return c ? c->ndof : -1; }
+extern "C" double* hg_device_state(hg_ctx* c) { return c ? c->d_Q : nullptr; }
+extern "C" int64_t hg_launch_count(const hg_ctx* c) { return c ? c->launches : -1; }
+
+static void check_ndof(hg_ctx* c, int64_t ndof) {
+  if (ndof != c->ndof) throw std::runtime_error("ndof mismatch: expected " + std::to_string(c->ndof));
+}
+
+extern "C" int hg_set_state(hg_ctx* c, const double* Q, int64_t ndof) {
+  try {
+    check_ndof(c, ndof);
+    HG_CUDA(cudaMemcpyAsync(c->d_Q, Q, ndof * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    c->cur = 0;
+    traces(c);
+    HG_CUDA(cudaGetLastError());
+    c->state_set = true;
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_get_state(hg_ctx* c, double* Q, int64_t ndof) {
+  try {
+    check_ndof(c, ndof);
+    HG_CUDA(cudaMemcpyAsync(Q, c->d_Q, ndof * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+static void require_state(hg_ctx* c) {
+  if (!c->state_set) throw std::runtime_error("state not set (call hg_set_state first)");
+}
+
+extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
+  try {
+    require_state(c);
+    (void)t;
+    HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
+    stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, true);
+    HG_CUDA(cudaGetLastError());
+    if (QDot) {
+      HG_CUDA(cudaMemcpyAsync(QDot, c->d_QDot, c->ndof * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
+  try {
+    require_state(c);
+    one_step(c, scheme, t, dt);
+    HG_CUDA(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double t0, double dt) {
+  try {
+    require_state(c);
+    for (int s = 0; s < n_steps; ++s) one_step(c, scheme, t0 + s * dt, dt);
+    HG_CUDA(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
+  try {
+    unsigned long long r[4];
+    HG_CUDA(cudaMemcpyAsync(r, c->d_resid, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 4; ++k) { double v; std::memcpy(&v, &r[k], 8); out[k] = v; }
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) {
+  try {
+    require_state(c);
+    const int threads = 256;
+    element_speed_kernel<<<(c->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
+        c->n_el, c->P * c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
+    ++c->launches;
+    HG_CUDA(cudaGetLastError());
+    std::vector<double> em(size_t(c->n_el) * 2);
+    HG_CUDA(cudaMemcpyAsync(em.data(), c->d_elmax, em.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    // running maxima over elements in mesh order, kept across calls
+    double d = dt_cap;
+    for (int e = 0; e < c->n_el; ++e) {
+      c->save_umax = std::fmax(c->save_umax, em[2 * e]);
+      c->save_amax = std::fmax(c->save_amax, em[2 * e + 1]);
+      d = std::fmin(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->N + 1));
+    }
+    *dt = d;
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_set_stream(hg_ctx* c, void* s) {
+  try {
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->own_stream) HG_CUDA(cudaStreamDestroy(c->stream));
+    c->own_stream = false;
+    c->stream = static_cast<cudaStream_t>(s);
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_synchronize(hg_ctx* c) {
+  try {
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    HG_CUDA(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}

@@ -1,0 +1,174 @@
+// hg_physics.cuh -- device physics of the DGSEM residual (Euler part).
+//
+// Each function states the reference routine it computes; arithmetic follows the
+// reference's order of operations so the FP64 path agrees with the reference to
+// rounding (the kernels are built with FMA contraction, which changes only the
+// last bits).
+//   inviscid_flux   Physics/InviscidFluxes.f90:104-147 (scaled by 1/(sqrt(gamma) M),
+//                   _DIMENSIONLESS_TAU)
+//   roe / hll       Physics/RiemannSolvers.f90:189-305 / 307-399
+//   lxf             Rusanov flux, no reference counterpart; same rotation and scaling
+//   euler_wall      BoundaryConditions/EulerWall.incf:71-158 (prescribed wall flux)
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace hg {
+
+enum { RIEMANN_ROE = 0, RIEMANN_HLL = 1, RIEMANN_EXACT = 2, RIEMANN_LXF = 3 };
+
+struct PhysConst {
+  double gamma, gm1, cp, cv, invSqrtGammaMach;
+};
+
+template <typename real>
+struct Phys {
+  real gamma, gm1, cp, cv, isgm;
+  __device__ __forceinline__ void load(const PhysConst& c) {
+    gamma = real(c.gamma); gm1 = real(c.gm1); cp = real(c.cp); cv = real(c.cv); isgm = real(c.invSqrtGammaMach);
+  }
+};
+
+template <typename real> __device__ __forceinline__ real rsqrt_(real x);
+template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+
+template <typename real>
+__device__ __forceinline__ void inviscid_flux(const Phys<real>& ph, const real* u, real* f, real* g) {
+  const real invRho = real(1) / u[0];
+  const real vx = u[1] * invRho, vy = u[2] * invRho;
+  const real p = ph.gm1 * (u[3] - real(0.5) * u[1] * vx - real(0.5) * u[2] * vy);
+  f[0] = u[1]; f[1] = u[1] * vx + p; f[2] = u[1] * vy; f[3] = (u[3] + p) * vx;
+  g[0] = u[2]; g[1] = f[2]; g[2] = u[2] * vy + p; g[3] = (u[3] + p) * vy;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { f[k] *= ph.isgm; g[k] *= ph.isgm; }
+}
+
+template <typename real>
+__device__ __forceinline__ void flux_normal(real rho, real u, real v, real p, real H, real* F) {
+  F[0] = rho * u; F[1] = F[0] * u + p; F[2] = F[0] * v; F[3] = H * F[0];
+}
+
+template <typename real>
+__device__ __forceinline__ void rotate_back_scale(const Phys<real>& ph, real* F, real nx, real ny) {
+  const real Ft = F[1] * nx - F[2] * ny;
+  F[2] = F[1] * ny + F[2] * nx;
+  F[1] = Ft;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) F[k] *= ph.isgm;
+}
+
+template <typename real>
+__device__ __forceinline__ void roe(const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny, real* F) {
+  const real rhoL = qL[0], invRhoL = real(1) / rhoL, sqrtRhoL = rsqrt_(rhoL);
+  const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
+  const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
+  const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
+  const real rhoR = qR[0], invRhoR = real(1) / rhoR, sqrtRhoR = rsqrt_(rhoR);
+  const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
+  const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
+  const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
+  const real invrho = real(1) / (sqrtRhoL + sqrtRhoR);
+  const real u = (sqrtRhoL * uL + sqrtRhoR * uR) * invrho;
+  const real v = (sqrtRhoL * vL + sqrtRhoR * vR) * invrho;
+  const real H = (sqrtRhoL * HL + sqrtRhoR * HR) * invrho;
+  const real a = rsqrt_(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
+  const real dq0 = rhoR - rhoL, dq1 = rhoR * uR - rhoL * uL, dq2 = rhoR * vR - rhoL * vL, dq3 = qR[3] - qL[3];
+  const real al2 = dq2 - v * dq0;
+  const real al1 = ph.gm1 * (dq0 * (H - u * u) + u * dq1 - dq3 + (dq2 - v * dq0) * v) / (a * a);
+  const real al0 = (dq0 * (u + a) - dq1 - a * al1) / (real(2) * a);
+  const real al3 = dq0 - (al0 + al1);
+  flux_normal(rhoL, uL, vL, pL, HL, F);
+  // waves with negative speed, added in the reference's order (u-a, u, u, u+a)
+  if (!(u - a > real(0))) {
+    const real s = al0 * (u - a);
+    F[0] += s; F[1] += s * (u - a); F[2] += s * v; F[3] += s * (H - u * a);
+    if (!(u > real(0))) {
+      const real s1 = al1 * u;
+      F[0] += s1; F[1] += s1 * u; F[2] += s1 * v; F[3] += s1 * (real(0.5) * (u * u + v * v));
+      const real s2 = al2 * u;
+      F[2] += s2; F[3] += s2 * v;
+      if (!(u + a > real(0))) {
+        const real s3 = al3 * (u + a);
+        F[0] += s3; F[1] += s3 * (u + a); F[2] += s3 * v; F[3] += s3 * (H + u * a);
+      }
+    }
+  }
+  rotate_back_scale(ph, F, nx, ny);
+}
+
+template <typename real>
+__device__ __forceinline__ void hll(const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny, real* F) {
+  const real rhoL = qL[0], invRhoL = real(1) / rhoL;
+  const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
+  const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
+  const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
+  const real aL = rsqrt_(ph.gamma * pL * invRhoL), rhoeL = qL[3];
+  const real rhoR = qR[0], invRhoR = real(1) / rhoR;
+  const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
+  const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
+  const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
+  const real aR = rsqrt_(ph.gamma * pR * invRhoR), rhoeR = qR[3];
+  const real sqrtRhoL = rsqrt_(rhoL), sqrtRhoR = rsqrt_(rhoR);
+  const real invrho = real(1) / (sqrtRhoL + sqrtRhoR);
+  const real u = (sqrtRhoL * uL + sqrtRhoR * uR) * invrho;
+  const real v = (sqrtRhoL * vL + sqrtRhoR * vR) * invrho;
+  const real H = (sqrtRhoL * HL + sqrtRhoR * HR) * invrho;
+  const real a = rsqrt_(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
+  const real SL = fmin(uL - aL, u - a), SR = fmax(uR + aR, u + a);
+  if (SL >= real(0)) flux_normal(rhoL, uL, vL, pL, HL, F);
+  else if (SR <= real(0)) flux_normal(rhoR, uR, vR, pR, HR, F);
+  else {
+    const real invdS = real(1) / (SR - SL);
+    F[0] = (SR * rhoL * uL - SL * rhoR * uR + SL * SR * (rhoR - rhoL)) * invdS;
+    F[1] = (SR * (rhoL * uL * uL + pL) - SL * (rhoR * uR * uR + pR) + SL * SR * (rhoR * uR - rhoL * uL)) * invdS;
+    F[2] = (SR * rhoL * uL * vL - SL * rhoR * uR * vR + SR * SL * (rhoR * vR - rhoL * vL)) * invdS;
+    F[3] = (SR * uL * rhoL * HL - SL * uR * rhoR * HR + SR * SL * (rhoeR - rhoeL)) * invdS;
+  }
+  rotate_back_scale(ph, F, nx, ny);
+}
+
+template <typename real>
+__device__ __forceinline__ void lxf(const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny, real* F) {
+  const real rhoL = qL[0], invRhoL = real(1) / rhoL;
+  const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
+  const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
+  const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
+  const real aL = rsqrt_(ph.gamma * pL * invRhoL);
+  const real rhoR = qR[0], invRhoR = real(1) / rhoR;
+  const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
+  const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
+  const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
+  const real aR = rsqrt_(ph.gamma * pR * invRhoR);
+  const real lam = fmax(fabs(uL) + aL, fabs(uR) + aR);
+  real FL[4], FR[4];
+  flux_normal(rhoL, uL, vL, pL, HL, FL);
+  flux_normal(rhoR, uR, vR, pR, HR, FR);
+  const real dq[4] = {rhoR - rhoL, rhoR * uR - rhoL * uL, rhoR * vR - rhoL * vL, qR[3] - qL[3]};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) F[k] = real(0.5) * (FL[k] + FR[k]) - real(0.5) * lam * dq[k];
+  rotate_back_scale(ph, F, nx, ny);
+}
+
+template <typename real>
+__device__ __forceinline__ void riemann(int which, const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny,
+                                        real* F) {
+  if (which == RIEMANN_HLL) hll(ph, qL, qR, nx, ny, F);
+  else if (which == RIEMANN_LXF) lxf(ph, qL, qR, nx, ny, F);
+  else roe(ph, qL, qR, nx, ny, F);
+}
+
+// Prescribed Euler-wall flux F(q_wall) . n dS, q_wall = interior state with the normal momentum removed.
+template <typename real>
+__device__ __forceinline__ void euler_wall_flux(const Phys<real>& ph, const real* q0, real nx, real ny, real dS, real* F) {
+  const real rhovn = q0[1] * nx + q0[2] * ny;
+  const real rhovt = -q0[1] * ny + q0[2] * nx;   // enters squared: the sign convention of curved walls is immaterial
+  const real p = ph.gm1 * (q0[3] - real(0.5) * (q0[1] * q0[1] + q0[2] * q0[2]) / q0[0]);
+  real q[4] = {q0[0], q0[1] - rhovn * nx, q0[2] - rhovn * ny, ph.cv * p + real(0.5) * rhovt * rhovt / q0[0]};
+  real f[4], g[4];
+  inviscid_flux(ph, q, f, g);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) F[k] = f[k] * nx * dS + g[k] * ny * dS;
+}
+
+}  // namespace hg

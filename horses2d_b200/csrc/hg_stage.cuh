@@ -1,0 +1,261 @@
+// hg_stage.cuh -- the fused DGSEM stage kernel (Euler) for sm_100a.
+//
+// One launch = one Runge-Kutta stage (or one bare time derivative) over all
+// elements.  Per element (one thread per node, EPB elements per CTA):
+//   1. load Q (reference layout, 32 B per node: coalesced) and the metrics;
+//   2. Euler flux -> contravariant fluxes into shared memory
+//        (Scalar_StdVolumeGreen, Approximation/DGWeakIntegrals.f90:111-181);
+//   3. 4(N+1) face-node tasks: own trace (from shared memory) and the neighbour's
+//      trace of the previous stage (global, written by that element's previous
+//      launch), Riemann solver / boundary state, x dS
+//        (ComputeRiemannSolver_*, DGSpatialDiscretizationMethods.f90:545-1511;
+//         projections types 1-2, Mesh/QuadElement_EdgeProcedures.incf:749-1206);
+//   4. volume contraction with hatD, surface lift with lbw (Scalar_StdFace,
+//      DGWeakIntegrals.f90:183-266), division by J (computeQDot :226-233);
+//   5. low-storage RK update G = a G + b QDot, Q += c G
+//        (DGTimeIntegrator.f90:282-365), in place;
+//   6. traces of the new Q on the 4 sides for the next launch (ping-pong buffer)
+//        (interpolateSolutionToBoundaries, :1520-1574).
+// The Riemann flux of an interior face is evaluated by both of its elements with
+// identical arguments (LEFT trace, RIGHT trace, LEFT's normal), so both see the
+// same value and the face needs no separate launch or flux buffer.
+#pragma once
+#include "hg_physics.cuh"
+
+namespace hg {
+
+// side kinds
+enum { SIDE_LEFT = 0, SIDE_RIGHT = 1, SIDE_STATE = 2, SIDE_WALL = 3 };
+constexpr int SIDE_REVERSED = 16;
+
+struct Zone {
+  int type, riemann;
+  double q[4];
+};
+
+template <typename real>
+struct StageArgs {
+  int n_el;
+  const int4* side;        // [n_el*4] {neighbour trace slot, flags, zone, 0}
+  const double* side_geo;  // [n_el*4][P][3]  nx, ny, dS in this element's side order
+  const double* vol_geo;   // [n_el][P*P][5]  Ja00 Ja01 Ja10 Ja11 1/J
+  const double* mats;      // hatD[P*P], lb0[P], lb1[P], lbw0[P], lbw1[P]
+  const Zone* zones;
+  double* Q;               // [n_el][P*P][4]
+  real* G;                 // [n_el][P*P][4]
+  const real* T_in;        // [n_el*4][P][4]
+  real* T_out;
+  double* QDot;            // optional output (time derivative only)
+  unsigned long long* resid;   // optional max |QDot| per variable (bit patterns of non-negative doubles)
+  double a, b, c;          // G = a G + b QDot ; Q += c G
+  int first;               // a == 0: do not read G
+  int update;              // 1: RK update, 0: only QDot (and traces of the unchanged Q)
+  int riemann;
+  PhysConst pc;
+};
+
+template <int P>
+struct Layout {
+  static constexpr int NP = P * P;
+  static constexpr int FT = 4 * P;   // face-node tasks per element
+};
+
+template <int P, int EPB, typename real>
+__global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
+  constexpr int NP = P * P;
+  constexpr int FT = 4 * P;
+  __shared__ real s_mat[NP + 4 * P];
+  __shared__ real s_Fc[EPB][NP][4];
+  __shared__ real s_Gc[EPB][NP][4];
+  __shared__ real s_Q[EPB][NP][4];
+  __shared__ real s_F[EPB][FT][4];
+
+  const int tid = threadIdx.x;            // node in element
+  const int le = threadIdx.y;             // element in block
+  const int flat = le * NP + tid;
+  for (int k = flat; k < NP + 4 * P; k += NP * EPB) s_mat[k] = real(a.mats[k]);
+  const int e = blockIdx.x * EPB + le;
+  const bool active = e < a.n_el;
+  Phys<real> ph;
+  ph.load(a.pc);
+  const int i = tid % P, j = tid / P;
+
+  real q[4];
+  real geo[5];
+  if (active) {
+    const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
+    const double2 q01 = qp[0], q23 = qp[1];
+    q[0] = real(q01.x); q[1] = real(q01.y); q[2] = real(q23.x); q[3] = real(q23.y);
+    const double* gp = a.vol_geo + (size_t(e) * NP + tid) * 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) geo[k] = real(gp[k]);
+    real f[4], g[4];
+    inviscid_flux(ph, q, f, g);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      s_Fc[le][tid][k] = f[k] * geo[0] + g[k] * geo[2];   // F Ja(1,IX) + G Ja(2,IX)
+      s_Gc[le][tid][k] = f[k] * geo[1] + g[k] * geo[3];   // F Ja(1,IY) + G Ja(2,IY)
+      s_Q[le][tid][k] = q[k];
+    }
+  }
+  __syncthreads();
+  const real* hatD = s_mat;
+  const real* lb0 = s_mat + NP;
+  const real* lb1 = lb0 + P;
+  const real* lbw0 = lb1 + P;
+  const real* lbw1 = lbw0 + P;
+
+  // face-node tasks: Riemann fluxes of the 4 sides (element-local order)
+  if (active) {
+    for (int t = tid; t < FT; t += NP) {
+      const int s = t / P, kk = t % P;
+      const int4 sd = a.side[size_t(e) * 4 + s];
+      const int kind = sd.y & 15;
+      // own trace at side node kk
+      const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
+      real qo[4] = {real(0), real(0), real(0), real(0)};
+      for (int l = 0; l < P; ++l) {
+        const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) qo[k] += s_Q[le][node][k] * lbv[l];
+      }
+      const double* g3 = a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
+      const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
+      real F[4];
+      if (kind == SIDE_WALL) {
+        euler_wall_flux(ph, qo, nx, ny, dS, F);
+      } else {
+        real qn[4];
+        int solver = a.riemann;
+        if (kind == SIDE_STATE) {
+          const Zone& z = a.zones[sd.z];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) qn[k] = real(z.q[k]);
+          if (z.riemann >= 0) solver = z.riemann;
+        } else {
+          const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+          const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) qn[k] = tp[k];
+          if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
+        }
+        if (kind == SIDE_RIGHT) {
+          riemann(solver, ph, qn, qo, nx, ny, F);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) F[k] = -(F[k] * dS);
+        } else {
+          riemann(solver, ph, qo, qn, nx, ny, F);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) F[k] = F[k] * dS;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s_F[le][t][k] = F[k];
+    }
+  }
+  __syncthreads();
+
+  real qd[4] = {real(0), real(0), real(0), real(0)};
+  if (active) {
+#pragma unroll
+    for (int l = 0; l < P; ++l) {
+      const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s_Fc[le][j * P + l][k] + hj * s_Gc[le][l * P + i][k];
+    }
+    // lift: bottom F(i) lbw0(j), right F(j) lbw1(i), top F(i) lbw1(j), left F(j) lbw0(i)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      qd[k] = qd[k] - s_F[le][0 * P + i][k] * lbw0[j];
+      qd[k] = qd[k] - s_F[le][1 * P + j][k] * lbw1[i];
+      qd[k] = qd[k] - s_F[le][2 * P + i][k] * lbw1[j];
+      qd[k] = qd[k] - s_F[le][3 * P + j][k] * lbw0[i];
+      qd[k] = qd[k] * geo[4];
+    }
+    if (a.resid) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double v = fabs(double(qd[k]));
+        atomicMax(&a.resid[k], (unsigned long long)__double_as_longlong(v));
+      }
+    }
+    const size_t off = (size_t(e) * NP + tid) * 4;
+    if (a.QDot) {
+      double2* dp = reinterpret_cast<double2*>(a.QDot + off);
+      dp[0] = make_double2(double(qd[0]), double(qd[1]));
+      dp[1] = make_double2(double(qd[2]), double(qd[3]));
+    }
+    if (a.update) {
+      real gn[4];
+      if (a.first) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gn[k] = real(a.b) * qd[k];
+      } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) gn[k] = real(a.a) * a.G[off + k] + real(a.b) * qd[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a.G[off + k] = gn[k];
+      double2* qp = reinterpret_cast<double2*>(a.Q + off);
+      double2 q01 = qp[0], q23 = qp[1];
+      q01.x = q01.x + a.c * double(gn[0]);
+      q01.y = q01.y + a.c * double(gn[1]);
+      q23.x = q23.x + a.c * double(gn[2]);
+      q23.y = q23.y + a.c * double(gn[3]);
+      qp[0] = q01; qp[1] = q23;
+      s_Q[le][tid][0] = real(q01.x); s_Q[le][tid][1] = real(q01.y);
+      s_Q[le][tid][2] = real(q23.x); s_Q[le][tid][3] = real(q23.y);
+    }
+  }
+  __syncthreads();
+  // traces of the updated state for the next launch
+  if (active && a.update) {
+    for (int t = tid; t < FT; t += NP) {
+      const int s = t / P, kk = t % P;
+      const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
+      real tr[4] = {real(0), real(0), real(0), real(0)};
+      for (int l = 0; l < P; ++l) {
+        const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) tr[k] += s_Q[le][node][k] * lbv[l];
+      }
+      real* tp = a.T_out + ((size_t(e) * 4 + s) * P + kk) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tp[k] = tr[k];
+    }
+  }
+}
+
+// Traces of the resident state (after hg_set_state).
+template <int P, int EPB, typename real>
+__global__ void __launch_bounds__(P * P * EPB) trace_kernel(int n_el, const double* Q, const double* mats, real* T) {
+  constexpr int NP = P * P;
+  constexpr int FT = 4 * P;
+  __shared__ real s_lb[2 * P];
+  __shared__ real s_Q[EPB][NP][4];
+  const int tid = threadIdx.x, le = threadIdx.y;
+  const int flat = le * NP + tid;
+  for (int k = flat; k < 2 * P; k += NP * EPB) s_lb[k] = real(mats[NP + k]);
+  const int e = blockIdx.x * EPB + le;
+  const bool active = e < n_el;
+  if (active)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s_Q[le][tid][k] = real(Q[(size_t(e) * NP + tid) * 4 + k]);
+  __syncthreads();
+  if (!active) return;
+  for (int t = tid; t < FT; t += NP) {
+    const int s = t / P, kk = t % P;
+    const real* lbv = (s == 0 || s == 3) ? s_lb : s_lb + P;
+    real tr[4] = {real(0), real(0), real(0), real(0)};
+    for (int l = 0; l < P; ++l) {
+      const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tr[k] += s_Q[le][node][k] * lbv[l];
+    }
+    real* tp = T + ((size_t(e) * 4 + s) * P + kk) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) tp[k] = tr[k];
+  }
+}
+
+}  // namespace hg

@@ -1,0 +1,155 @@
+"""Host-side mirror of the reference's time-derivative and time-scheme interface.
+
+``GpuDGSEM`` wraps one libhorsesgpu context.  Its methods correspond to the
+reference procedures a HORSES2D driver calls on the hot path:
+
+=========================================  =====================================================
+reference (Solver/src/...)                 here
+=========================================  =====================================================
+DGSpatial_computeTimeDerivative            ``compute_time_derivative(t)``
+ (Approximation/DGSpatialDiscretizationMethods.f90:94-116)
+TimeScheme / TimeIntegrator_WilliamsonRK3  ``time_step(scheme, t, dt)``
+ (Approximation/DGTimeIntegrator.f90:71-83, 263-365)
+TimeIntegrator_EstimateTimeStep            ``estimate_time_step(cfl, dt_cap)``
+ (DGTimeIntegrator.f90:462-511)
+Mesh_ComputeResiduals                      ``residuals()``
+ (Mesh/QuadMesh_Auxiliars.incf:22-38)
+Storage%Q read/write (Generic/Storage.f90)  ``set_state(Q)`` / ``state()``
+=========================================  =====================================================
+
+Errors raise ``HorsesGpuError`` carrying the library's message (the reference
+stops the program instead).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+class HorsesGpuError(RuntimeError):
+    pass
+
+
+def _arr(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class GpuDGSEM:
+    """One mesh + physics + resident state on the GPU."""
+
+    def __init__(self, mesh, *, mach, node_type=L.NODES_LGL, riemann=L.ROE, bcs=(), precision=L.PREC_FP64,
+                 reynolds=0.0, prandtl=0.72, navier_stokes=0, viscous=0, pressure_ref=101325.0,
+                 temperature_ref=273.15, reynolds_length=1.0, gamma=1.4):
+        lib = L.load()
+        self._keep = []
+        md = L.MeshDesc()
+        md.n_elements = int(len(mesh["N"]))
+        md.n_edges = int(len(mesh["edge_marker"]))
+
+        def put(field, key, dtype, ctype, optional=False):
+            if key not in mesh or mesh[key] is None:
+                if not optional:
+                    raise HorsesGpuError(f"mesh descriptor lacks '{key}'")
+                setattr(md, field, C.cast(None, C.POINTER(ctype)))
+                return
+            a = _arr(mesh[key], dtype)
+            self._keep.append(a)
+            setattr(md, field, a.ctypes.data_as(C.POINTER(ctype)))
+
+        put("N", "N", np.int32, C.c_int32)
+        put("Ja", "Ja", np.float64, C.c_double)
+        put("jac", "jac", np.float64, C.c_double)
+        put("x", "x", np.float64, C.c_double, True)
+        put("volume", "volume", np.float64, C.c_double, True)
+        put("vertices", "vertices", np.float64, C.c_double, True)
+        put("edge_elem", "edge_elem", np.int32, C.c_int32)
+        put("edge_side", "edge_side", np.int32, C.c_int32)
+        put("edge_inverse", "edge_inverse", np.int32, C.c_int32)
+        put("edge_marker", "edge_marker", np.int32, C.c_int32)
+        put("edge_n", "edge_n", np.float64, C.c_double)
+        put("edge_dS", "edge_dS", np.float64, C.c_double)
+        put("periodic_partner", "periodic_partner", np.int32, C.c_int32, True)
+        put("edge_invh", "edge_invh", np.float64, C.c_double, True)
+        ph = L.PhysicsDesc(node_type=node_type, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous,
+                           mach=mach, reynolds=reynolds, prandtl=prandtl, pressure_ref=pressure_ref,
+                           temperature_ref=temperature_ref, reynolds_length=reynolds_length, gamma=gamma,
+                           gas_R=287.15)
+        barr = (L.BCDesc * max(1, len(bcs)))()
+        for k, b in enumerate(bcs):
+            barr[k].type = b["type"]
+            barr[k].riemann = b.get("riemann", L.INTERIOR)
+            st = b.get("state", (0.0, 0.0, 0.0, 0.0))
+            for i in range(4):
+                barr[k].state[i] = st[i]
+            barr[k].wall_T = b.get("wall_T", 1.0)
+            barr[k].wall_type = b.get("wall_type", 2)
+            barr[k].outflow_type = b.get("outflow_type", 1)
+        self._keep.append(barr)
+        h = C.c_void_p()
+        rc = lib.hg_create(C.byref(md), C.byref(ph), barr, len(bcs), precision, C.byref(h))
+        if rc != 0:
+            raise HorsesGpuError(lib.hg_last_error(None).decode())
+        self._h = h
+        self._lib = lib
+        self.ndof = lib.hg_ndof(h)
+        self.precision = precision
+
+    def _check(self, rc):
+        if rc != 0:
+            raise HorsesGpuError(self._lib.hg_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hg_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    # --- Storage%Q ---------------------------------------------------------
+    def set_state(self, Q):
+        Q = _arr(Q, np.float64).ravel()
+        self._check(self._lib.hg_set_state(self._h, Q.ctypes.data_as(L.F64P), Q.size))
+
+    def state(self):
+        Q = np.empty(self.ndof)
+        self._check(self._lib.hg_get_state(self._h, Q.ctypes.data_as(L.F64P), Q.size))
+        return Q
+
+    # --- hot path ----------------------------------------------------------
+    def compute_time_derivative(self, t=0.0, return_qdot=True):
+        if return_qdot:
+            out = np.empty(self.ndof)
+            self._check(self._lib.hg_time_derivative(self._h, t, out.ctypes.data_as(L.F64P)))
+            return out
+        self._check(self._lib.hg_time_derivative(self._h, t, None))
+        return None
+
+    def time_step(self, scheme, t, dt):
+        self._check(self._lib.hg_time_step(self._h, scheme, t, dt))
+
+    def time_steps(self, scheme, n_steps, t0, dt):
+        self._check(self._lib.hg_time_steps(self._h, scheme, n_steps, t0, dt))
+
+    def residuals(self):
+        r = np.zeros(4)
+        self._check(self._lib.hg_residuals(self._h, r.ctypes.data_as(L.F64P)))
+        return r
+
+    def estimate_time_step(self, cfl, dt_cap):
+        d = C.c_double(0.0)
+        self._check(self._lib.hg_estimate_dt(self._h, cfl, dt_cap, C.byref(d)))
+        return d.value
+
+    # --- plumbing ----------------------------------------------------------
+    def set_stream(self, cuda_stream_handle):
+        self._check(self._lib.hg_set_stream(self._h, C.c_void_p(cuda_stream_handle)))
+
+    def synchronize(self):
+        self._check(self._lib.hg_synchronize(self._h))
+
+    def device_state_ptr(self):
+        return self._lib.hg_device_state(self._h)
+
+    def launch_count(self):
+        return self._lib.hg_launch_count(self._h)

@@ -1,0 +1,127 @@
+/*
+ * horses_gpu.h -- C ABI of libhorsesgpu.so, the B200 (sm_100a) DGSEM residual
+ * and low-storage Runge-Kutta time stepper that drops into HORSES2D.
+ *
+ * The reference computes the residual in Fortran:
+ *   DGSpatial_computeTimeDerivative(mesh, time)
+ *       Solver/src/Approximation/DGSpatialDiscretizationMethods.f90:94-116
+ *   TimeScheme(mesh, NDOF, time, dt, Storage)   (Explicit Euler, Williamson RK3/RK5)
+ *       Solver/src/Approximation/DGTimeIntegrator.f90:71-83, 263-365
+ *   TimeIntegrator_EstimateTimeStep             DGTimeIntegrator.f90:462-511
+ *   Mesh_ComputeResiduals                       Solver/src/Mesh/QuadMesh_Auxiliars.incf:22-38
+ * A Fortran (iso_c_binding) shim replaces those bodies with calls below; the
+ * driver, case files, NetCDF I/O and the problem-file plugin are unchanged.
+ *
+ * Conventions
+ *  - Every function returns 0 on success, non-zero on error; hg_last_error()
+ *    returns the message (the shim turns it into the reference's `stop`).
+ *  - The state Q is the reference's flat Storage%Q (Generic/Storage.f90:31-73):
+ *    element e holds 4*(N_e+1)^2 doubles at offset 4*cumP2(e), ordered
+ *    Q[e][eta][xi][var] (var fastest).  hg_set_state / hg_get_state copy it
+ *    between host memory and the device; between those calls Q stays resident
+ *    in device memory.
+ *  - One context per mesh; calls on a context are issued on its CUDA stream and
+ *    are asynchronous unless they return data to the host.
+ *  - There is no CPU fallback: without a usable sm_100 device hg_create fails.
+ */
+#ifndef HORSES_GPU_H
+#define HORSES_GPU_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hg_ctx hg_ctx;
+
+enum { HG_NODES_LG = 1, HG_NODES_LGL = 2 };                     /* Generic/Defines.h LG, LGL */
+enum { HG_RIEMANN_ROE = 0, HG_RIEMANN_HLL = 1, HG_RIEMANN_EXACT = 2, HG_RIEMANN_LXF = 3,
+       HG_RIEMANN_INTERIOR = -1 };                              /* Physics/RiemannSolvers.f90; LXF is new */
+enum { HG_SCHEME_EULER = 0, HG_SCHEME_RK3 = 1, HG_SCHEME_RK5 = 2 }; /* DGTimeIntegrator.f90:131-149 */
+enum { HG_PREC_FP64 = 0, HG_PREC_FP32 = 1 };
+/* Boundary-condition kinds, numbered as Generic/Defines.h PERIODIC_BC .. PRESSUREOUTLET_BC. */
+enum { HG_BC_PERIODIC = 1, HG_BC_DIRICHLET = 2, HG_BC_EULERWALL = 3, HG_BC_VISCOUSWALL = 4,
+       HG_BC_FARFIELD = 5, HG_BC_PRESSUREOUTLET = 6 };
+
+/* Physics and discretization choices (Setup_t, PhysicsNS InitializePhysics). */
+typedef struct {
+  int32_t node_type;       /* HG_NODES_LG / HG_NODES_LGL */
+  int32_t riemann;         /* interior inviscid Riemann solver */
+  int32_t navier_stokes;   /* 0: Euler build, 1: Navier-Stokes build */
+  int32_t viscous;         /* 0: BR1, 1: interior penalty */
+  double  mach, reynolds, prandtl;
+  double  pressure_ref, temperature_ref, reynolds_length;
+  double  gamma;           /* 1.4 for the reference's "Air" */
+  double  gas_R;           /* 287.15 */
+} hg_physics_desc;
+
+/* One boundary zone (marker), as constructed by the reference's BC classes
+ * (BoundaryConditions/DGBoundaryConditions.f90).  `state` is the zone's
+ * dimensionless boundary state q (Dirichlet/Farfield/Outlet), already converted
+ * by the host like DirichletBC_Construct does. */
+typedef struct {
+  int32_t type;            /* HG_BC_* */
+  int32_t riemann;         /* zone Riemann solver, HG_RIEMANN_INTERIOR = interior one */
+  double  state[4];
+  double  wall_T;          /* viscous wall temperature (dimensionless), isothermal walls */
+  int32_t wall_type;       /* 1 isothermal, 2 adiabatic */
+  int32_t outflow_type;
+} hg_bc_desc;
+
+/* The mesh after the reference's construction (QuadMesh_t after
+ * constructFromFile + ConstructZones), flattened.  Per-node arrays follow the
+ * Storage%Q node order (offset/4).  Edge arrays follow mesh%edges order. */
+typedef struct {
+  int32_t n_elements;
+  int32_t n_edges;
+  const int32_t* N;             /* [n_elements] polynomial order */
+  const double*  Ja;            /* [nodes][2][2]  Ja(i,j,dim,IX/IY), QuadElement_SetMappings */
+  const double*  jac;           /* [nodes]        mapping jacobian */
+  const double*  x;             /* [nodes][2]     node coordinates (dimensionless); may be NULL */
+  const double*  volume;        /* [n_elements]   element area; may be NULL */
+  const double*  vertices;      /* [n_elements][4][2] corner nodes (dimensionless), for hg_estimate_dt; may be NULL */
+  const int32_t* edge_elem;     /* [n_edges][2]   LEFT, RIGHT element (0-based); RIGHT = -1 on boundaries */
+  const int32_t* edge_side;     /* [n_edges][2]   edgeLocation 1..4 (EBOTTOM,ERIGHT,ETOP,ELEFT) of LEFT, RIGHT */
+  const int32_t* edge_inverse;  /* [n_edges]      RIGHT (or periodic partner) traverses the edge backwards */
+  const int32_t* edge_marker;   /* [n_edges]      0 interior, else boundary marker (1-based zone) */
+  const double*  edge_n;        /* [n_edges][N_edge+1][2] unit normal, outward from LEFT, LEFT's node order */
+  const double*  edge_dS;       /* [n_edges][N_edge+1]    surface jacobian */
+  const int32_t* periodic_partner; /* [n_edges] partner boundary edge of a periodic edge, else -1 */
+  const double*  edge_invh;     /* [n_edges] Area / min(volume) (interior penalty); may be NULL */
+} hg_mesh_desc;
+
+/* Create a context: uploads geometry, connectivity and boundary zones once.
+ * bcs[k] describes marker k+1. */
+int  hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, const hg_bc_desc* bcs, int32_t n_bcs,
+               int32_t precision, hg_ctx** out);
+void hg_destroy(hg_ctx* ctx);
+const char* hg_last_error(const hg_ctx* ctx);   /* ctx may be NULL: last hg_create error */
+
+/* Host <-> device state copies (reference layout). */
+int  hg_set_state(hg_ctx* ctx, const double* Q, int64_t ndof);
+int  hg_get_state(hg_ctx* ctx, double* Q, int64_t ndof);
+int64_t hg_ndof(const hg_ctx* ctx);
+
+/* == DGSpatial_computeTimeDerivative: QDot of the resident state.  QDot may be
+ * NULL (result kept on the device for hg_residuals). */
+int  hg_time_derivative(hg_ctx* ctx, double t, double* QDot);
+/* == TimeScheme: one step of HG_SCHEME_* on the resident state. */
+int  hg_time_step(hg_ctx* ctx, int32_t scheme, double t, double dt);
+/* n_steps steps of constant dt starting at t0, without host synchronisation. */
+int  hg_time_steps(hg_ctx* ctx, int32_t scheme, int32_t n_steps, double t0, double dt);
+/* == Mesh_ComputeResiduals: max |QDot| per variable of the last stage. */
+int  hg_residuals(hg_ctx* ctx, double out[4]);
+/* == EstimateTimeStep, including the reference's running maxima (SAVE). */
+int  hg_estimate_dt(hg_ctx* ctx, double cfl, double dt_cap, double* dt);
+
+/* Stream control: run on the caller's stream (e.g. a framework's current stream). */
+int  hg_set_stream(hg_ctx* ctx, void* cuda_stream);
+int  hg_synchronize(hg_ctx* ctx);
+/* Device pointer of the resident state (reference layout) for in-HBM benchmarking. */
+double* hg_device_state(hg_ctx* ctx);
+/* Number of kernel launches issued by this context so far. */
+int64_t hg_launch_count(const hg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

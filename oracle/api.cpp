@@ -196,3 +196,49 @@ extern "C" int or_edge_count_by_type(void* h, int type) {
   for (auto& f : o.ed) if (int(f.kind) == type) ++c;
   return c;
 }
+
+extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
+                              int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
+                              double* edge_dS, int* periodic_partner, double* edge_invh) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  const int N0 = o.el[0].N;
+  for (auto& e : o.el) if (e.N != N0) return -1;
+  for (auto& f : o.ed) if (f.is_subdiv()) return -1;
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    const Element& e = o.el[ei];
+    N[ei] = e.N;
+    const int64_t base = e.offset / 4;
+    for (int q = 0; q < e.P * e.P; ++q) {
+      for (int k = 0; k < 4; ++k) Ja[4 * (base + q) + k] = e.Ja[4 * q + k];
+      jac[base + q] = e.jac[q];
+      x[2 * (base + q)] = e.X[2 * q];
+      x[2 * (base + q) + 1] = e.X[2 * q + 1];
+    }
+    volume[ei] = e.volume;
+    for (int k = 0; k < 4; ++k) {
+      vertices[ei * 8 + 2 * k] = o.nodeX[2 * e.nodes[k]];
+      vertices[ei * 8 + 2 * k + 1] = o.nodeX[2 * e.nodes[k] + 1];
+    }
+  }
+  const int P = N0 + 1;
+  for (size_t fi = 0; fi < o.ed.size(); ++fi) {
+    const Edge& f = o.ed[fi];
+    if (f.is_bdry()) {
+      edge_elem[2 * fi] = f.quads[0]; edge_elem[2 * fi + 1] = -1;
+      edge_side[2 * fi] = f.edgeLocation[0]; edge_side[2 * fi + 1] = 0;
+    } else {
+      edge_elem[2 * fi] = f.quads[SLOT_LEFT]; edge_elem[2 * fi + 1] = f.quads[SLOT_RIGHT];
+      edge_side[2 * fi] = f.edgeLocation[SLOT_LEFT]; edge_side[2 * fi + 1] = f.edgeLocation[SLOT_RIGHT];
+    }
+    edge_inverse[fi] = f.inverse ? 1 : 0;
+    edge_marker[fi] = f.edgeType;
+    for (int p = 0; p < P; ++p) {
+      edge_n[(fi * P + p) * 2] = f.nx(p);
+      edge_n[(fi * P + p) * 2 + 1] = f.ny(p);
+      edge_dS[fi * P + p] = f.straight_like() ? f.dS[0] : f.dS[p];
+    }
+    periodic_partner[fi] = f.periodic_partner;
+    edge_invh[fi] = f.invh;
+  }
+  return 0;
+}

@@ -80,6 +80,8 @@ def lib():
         L.or_element_geometry.argtypes = [vp, dp, dp, dp]
         L.or_edge_count_by_type.restype = i
         L.or_edge_count_by_type.argtypes = [vp, i]
+        L.or_export_mesh.restype = i
+        L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
         _lib = L
     return _lib
 
@@ -203,3 +205,20 @@ class Oracle:
 
     def edge_count(self, kind):
         return lib().or_edge_count_by_type(self.h, kind)
+
+    def export_mesh(self):
+        """The constructed mesh flattened like include/horses_gpu.h hg_mesh_desc."""
+        E, F, n = self.n_elements, lib().or_n_edges(self.h), self.ndof // 4
+        P = int(self.orders[0]) + 1
+        d = dict(N=np.zeros(E, np.int32), Ja=np.zeros(4 * n), jac=np.zeros(n), x=np.zeros(2 * n), volume=np.zeros(E),
+                 vertices=np.zeros(8 * E), edge_elem=np.zeros(2 * F, np.int32), edge_side=np.zeros(2 * F, np.int32),
+                 edge_inverse=np.zeros(F, np.int32), edge_marker=np.zeros(F, np.int32), edge_n=np.zeros(2 * P * F),
+                 edge_dS=np.zeros(P * F), periodic_partner=np.zeros(F, np.int32), edge_invh=np.zeros(F))
+        ip_, dp_ = C.c_int, C.c_double
+        rc = lib().or_export_mesh(self.h, *[_p(d[k], ip_ if d[k].dtype == np.int32 else dp_) for k in
+                                            ("N", "Ja", "jac", "x", "volume", "vertices", "edge_elem", "edge_side",
+                                             "edge_inverse", "edge_marker", "edge_n", "edge_dS", "periodic_partner",
+                                             "edge_invh")])
+        if rc != 0:
+            raise RuntimeError("mesh has mortars or mixed polynomial orders")
+        return d

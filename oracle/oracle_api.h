@@ -96,6 +96,14 @@ void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless
 /* Geometry export for cross-checking host-side mesh builders. */
 void    or_element_geometry(void* h, double* Ja, double* jac, double* volume); /* Ja [ndof/4][2][2], jac [ndof/4], volume [E] */
 int     or_edge_count_by_type(void* h, int type);
+/* Flattened mesh in the layout of include/horses_gpu.h hg_mesh_desc (conforming,
+ * uniform-order meshes).  Array sizes: N[E], Ja[nodes*4], jac[nodes], x[nodes*2],
+ * volume[E], vertices[E*8], edge_elem[2F], edge_side[2F], edge_inverse[F],
+ * edge_marker[F], edge_n[F*P*2], edge_dS[F*P], periodic_partner[F], edge_invh[F].
+ * Returns 0, or -1 when the mesh has mortars or mixed orders. */
+int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
+                       int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
+                       double* edge_dS, int* periodic_partner, double* edge_invh);
 
 #ifdef __cplusplus
 }

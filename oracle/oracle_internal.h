@@ -97,6 +97,7 @@ struct Edge {
   const std::vector<double>* gB = nullptr;
   std::vector<int> viscousBCType;
   int zone = -1;
+  int periodic_partner = -1;
   // mortars (SubdividedEdge_t)
   int N_N = 0, N_S = 0;
   const Spectral* spN = nullptr;

@@ -346,6 +346,7 @@ void setup_zones(Oracle& o) {
         e1.associated = e2.associated = true;
         e1.inviscidBCType = e2.inviscidBCType = WEAK_RIEMANN;
         e1.uB = &e2.storage[0].Q; e2.uB = &e1.storage[0].Q;
+        e1.periodic_partner = id2; e2.periodic_partner = id1;
         e1.uSB = &e2.storage[0].Q; e2.uSB = &e1.storage[0].Q;
         e1.gB = &e2.storage[0].dQ; e2.gB = &e1.storage[0].dQ;
         e1.viscousBCType.assign(e1.P(), VBC_PERIODIC);

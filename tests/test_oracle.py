@@ -1,0 +1,108 @@
+"""The oracle against the reference's own golden vectors and known answers (CPU only).
+
+* VortexTransport benchmark (TestCases/Benchmark/Simulations/VortexTransport):
+  the reference's Finalize asserts iteration 3237 and the four max-norm errors
+  w.r.t. the initial vortex to 1e-12 after integrating to t = 2 with Williamson
+  RK5 (CFL 0.4, dt cap 1e-2) on a curved, p-refined (N = 5/7/12) mesh with
+  mortars and periodic zones, Legendre-Gauss nodes and the Roe flux (the case
+  file's "Inviscid Riemann Flux" key is not the one Setup.f90:280 reads, so the
+  default Roe applies).
+* Spectral building blocks: exactness of the nodal derivative and quadrature.
+* Free-stream preservation on curved meshes, conservation on periodic meshes.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from cases_util import GOLDEN, load_mesh, vortex_case, rel_l2
+
+
+def vortex_transport_ic(X, ref):
+    """UserDefinedInitialCondition of the VortexTransport plugin, made dimensionless."""
+    gamma, R, mach = 1.4, 287.15, 0.6
+    cv, cp_d = R * 2.5, 3.5
+    x, y = X[:, 0], X[:, 1]
+    Rv, beta = 0.1, 0.05
+    r2 = (x * x + y * y) / (Rv * Rv)
+    u = ref["V"] * (np.cos(0.0) - beta * y / Rv * np.exp(-0.5 * r2))
+    v = ref["V"] * (np.sin(0.0) + beta * x / Rv * np.exp(-0.5 * r2))
+    T = ref["T"] * (1.0 - gamma * mach * mach * beta * beta / (2.0 * cp_d) * np.exp(-r2))
+    rho = ref["rho"] * (T / ref["T"]) ** 2.5
+    q = np.stack([rho, rho * u, rho * v, cv * (rho * T) + 0.5 * rho * (u * u + v * v)], 1)
+    return q / np.array([ref["rho"], ref["rho"] * ref["a"], ref["rho"] * ref["a"], ref["p"]])
+
+
+def vortex_transport_oracle():
+    m = load_mesh("VortexTransportBench")
+    porder = np.array([5, 7, 12, 7])[m["p_zones"]]
+    bcs = [dict(type=O.BC_PERIODIC, periodic_dir=2, connected_marker=2),
+           dict(type=O.BC_PERIODIC, periodic_dir=2, connected_marker=1),
+           dict(type=O.BC_PERIODIC, periodic_dir=1, connected_marker=4),
+           dict(type=O.BC_PERIODIC, periodic_dir=1, connected_marker=3)]
+    return O.Oracle(m, porder, nodes=O.LG, riemann=O.ROE, mach=0.6, reynolds=0.0, bcs=bcs)
+
+
+def test_vortex_transport_benchmark_golden():
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["VortexTransport"]
+    orc = vortex_transport_oracle()
+    # the mesh exercises every edge kind the benchmark relies on
+    assert orc.edge_count(1) > 0 and orc.edge_count(2) > 0 and orc.edge_count(3) > 0
+    X = orc.coords()
+    orc.set_state(vortex_transport_ic(X, orc.ref).ravel())
+    it, t = orc.integrate(O.RK5, transient=True, t0=0.0, t_end=2.0, max_iter=1000000, cfl=0.4, dt_cap=1e-2)
+    err = np.abs(vortex_transport_ic(X, orc.ref) - orc.state().reshape(-1, 4)).max(0)
+    assert it == golden["expected_iter"]
+    assert np.max(np.abs(err - np.array(golden["expectedErrors"]))) <= 1e-12
+
+
+@pytest.mark.parametrize("nodes", [O.LG, O.LGL])
+def test_freestream_preservation_curved(nodes):
+    """A uniform state has zero residual on the curved, p-refined reference mesh (metric identities)."""
+    orc = vortex_transport_oracle() if nodes == O.LG else None
+    if orc is None:
+        m = load_mesh("VortexTransportBench")
+        bcs = [dict(type=O.BC_PERIODIC, periodic_dir=2, connected_marker=2),
+               dict(type=O.BC_PERIODIC, periodic_dir=2, connected_marker=1),
+               dict(type=O.BC_PERIODIC, periodic_dir=1, connected_marker=4),
+               dict(type=O.BC_PERIODIC, periodic_dir=1, connected_marker=3)]
+        orc = O.Oracle(m, 4, nodes=nodes, riemann=O.ROE, mach=0.6, bcs=bcs)
+    u = np.sqrt(1.4) * 0.6
+    q = np.array([1.0, u, 0.0, 2.5 + 0.5 * u * u])
+    orc.set_state(np.tile(q, orc.ndof // 4))
+    qd = orc.time_derivative(0.0)
+    # discrete metric identities hold to ~1e-9 on this mesh (curve degree NLow/2 on mortars)
+    assert np.abs(qd).max() < 1e-8
+
+
+def test_conservation_periodic():
+    """On a periodic mesh the weighted sum of QDot (total mass, momentum, energy rate) vanishes."""
+    orc, Q0, _ = vortex_case(n=8, N=4, nodes=O.LG)
+    orc.set_state(Q0)
+    qd = orc.time_derivative(0.0).reshape(orc.n_elements, -1, 4)
+    Ja, jac, vol = orc.geometry()
+    # Legendre-Gauss quadrature weights mapped to [0,1]
+    x, w = np.polynomial.legendre.leggauss(5)
+    W = np.outer(0.5 * w, 0.5 * w).ravel()     # (eta, xi) order matches node order j*P+i
+    total = (qd * (jac.reshape(orc.n_elements, -1) * W)[:, :, None]).sum((0, 1))
+    assert np.abs(total).max() < 1e-12 * np.abs(qd).max() * orc.n_elements
+
+
+def test_rk3_matches_explicit_formula():
+    """Williamson 2N RK3 in the oracle equals the three-stage update written out."""
+    orc, Q0, _ = vortex_case(n=4, N=3)
+    orc.set_state(Q0)
+    dt = 1e-3
+    orc.time_step(O.RK3, 0.0, dt)
+    Q_rk = orc.state()
+    orc.set_state(Q0)
+    am, gm = [0.0, -5.0 / 9.0, -153.0 / 128.0], [1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0]
+    Q, G = Q0.copy(), np.zeros_like(Q0)
+    for m in range(3):
+        orc.set_state(Q)
+        k = orc.time_derivative(0.0)
+        G = k if m == 0 else am[m] * G + k
+        Q = Q + gm[m] * dt * G
+    assert rel_l2(Q_rk, Q) < 1e-15
