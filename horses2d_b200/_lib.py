@@ -42,7 +42,7 @@ class MeshDesc(C.Structure):
 _lib = None
 EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_state", "hg_ndof",
             "hg_time_derivative", "hg_time_step", "hg_time_steps", "hg_residuals", "hg_estimate_dt",
-            "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count")
+            "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info")
 
 
 def load():
@@ -76,5 +76,16 @@ def load():
     L.hg_device_state.argtypes = [vp]
     L.hg_launch_count.restype = C.c_int64
     L.hg_launch_count.argtypes = [vp]
+    L.hg_nodes.argtypes = [C.c_int32, C.c_int32, F64P, F64P]
+    L.hg_info.argtypes = [vp, I32P]
     _lib = L
     return L
+
+
+def nodes(N, node_type):
+    """The library's interpolation nodes and weights on [0,1] for order N."""
+    import numpy as np
+    xi, w = np.zeros(N + 1), np.zeros(N + 1)
+    if load().hg_nodes(N, node_type, xi.ctypes.data_as(F64P), w.ctypes.data_as(F64P)) != 0:
+        raise RuntimeError(load().hg_last_error(None).decode())
+    return xi, w

@@ -40,6 +40,7 @@ struct hg_ctx {
   unsigned long long* d_resid = nullptr;
   double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
   int cur = 0;                    // which trace buffer holds the current traces
+  bool affine = false;            // per-element constant metrics and per-side constant normals
   bool state_set = false;
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
@@ -83,7 +84,8 @@ template <int P, typename real>
 static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   constexpr int EPB = epb_for(P);
   dim3 block(P * P, EPB), grid((a.n_el + EPB - 1) / EPB);
-  stage_kernel<P, EPB, real><<<grid, block, 0, c->stream>>>(a);
+  if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block, 0, c->stream>>>(a);
+  else stage_kernel<P, EPB, real, false><<<grid, block, 0, c->stream>>>(a);
   ++c->launches;
 }
 
@@ -286,6 +288,39 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   for (size_t s = 0; s < side.size(); ++s)
     if (side[s].x == -2) throw std::runtime_error("element side not covered by any edge");
 
+  // Affine detection: every node of an element carries the same metrics and every
+  // side the same normal and dS (to 1e-14 relative); then the kernel reads one
+  // value per element / side instead of one per node.
+  {
+    auto close = [](double a, double b, double scale) { return std::fabs(a - b) <= 1e-14 * scale; };
+    bool aff = true;
+    for (int e = 0; e < E && aff; ++e) {
+      const double* g0 = &vg[size_t(e) * NP * 5];
+      double sc = 0.0;
+      for (int k = 0; k < 4; ++k) sc = std::fmax(sc, std::fabs(g0[k]));
+      for (int n = 1; n < NP && aff; ++n)
+        for (int k = 0; k < 5; ++k)
+          if (!close(g0[n * 5 + k], g0[k], k < 4 ? sc : std::fabs(g0[4]))) { aff = false; break; }
+      for (int s = 0; s < 4 && aff; ++s) {
+        const double* s0 = &sg[(size_t(e) * 4 + s) * P * 3];
+        for (int k = 1; k < P && aff; ++k)
+          for (int q = 0; q < 3; ++q)
+            if (!close(s0[k * 3 + q], s0[q], q < 2 ? 1.0 : std::fabs(s0[2]))) { aff = false; break; }
+      }
+    }
+    c->affine = aff;
+    if (aff) {
+      std::vector<double> vg1(size_t(E) * 5), sg1(size_t(E) * 4 * 3);
+      for (int e = 0; e < E; ++e) {
+        for (int k = 0; k < 5; ++k) vg1[size_t(e) * 5 + k] = vg[size_t(e) * NP * 5 + k];
+        for (int s = 0; s < 4; ++s)
+          for (int q = 0; q < 3; ++q) sg1[(size_t(e) * 4 + s) * 3 + q] = sg[(size_t(e) * 4 + s) * P * 3 + q];
+      }
+      vg.swap(vg1);
+      sg.swap(sg1);
+    }
+  }
+
   // dt support: corner distances
   c->dx.assign(E, 0.0);
   if (m->vertices) {
@@ -462,4 +497,21 @@ extern "C" int hg_synchronize(hg_ctx* c) {
     HG_CUDA(cudaGetLastError());
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_info(const hg_ctx* c, int32_t out[4]) {
+  if (!c || !out) return 1;
+  out[0] = c->N; out[1] = c->n_el; out[2] = c->affine ? 1 : 0; out[3] = c->precision;
+  return 0;
+}
+
+extern "C" int hg_nodes(int32_t N, int32_t node_type, double* xi, double* w) {
+  try {
+    NodalOps o = make_nodal_ops(N, node_type);
+    for (int i = 0; i <= N; ++i) { xi[i] = o.xi[i]; w[i] = o.w[i]; }
+    return 0;
+  } catch (const std::exception& ex) {
+    g_create_err = ex.what();
+    return 1;
+  }
 }

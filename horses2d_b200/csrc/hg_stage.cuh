@@ -60,7 +60,9 @@ struct Layout {
   static constexpr int FT = 4 * P;   // face-node tasks per element
 };
 
-template <int P, int EPB, typename real>
+// AFFINE: metrics constant per element (vol_geo [n_el][5]) and normals/dS constant
+// per side (side_geo [n_el*4][3]), as for parallelogram elements with straight edges.
+template <int P, int EPB, typename real, bool AFFINE>
 __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
   constexpr int NP = P * P;
   constexpr int FT = 4 * P;
@@ -86,7 +88,7 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
     q[0] = real(q01.x); q[1] = real(q01.y); q[2] = real(q23.x); q[3] = real(q23.y);
-    const double* gp = a.vol_geo + (size_t(e) * NP + tid) * 5;
+    const double* gp = AFFINE ? a.vol_geo + size_t(e) * 5 : a.vol_geo + (size_t(e) * NP + tid) * 5;
 #pragma unroll
     for (int k = 0; k < 5; ++k) geo[k] = real(gp[k]);
     real f[4], g[4];
@@ -119,7 +121,7 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) qo[k] += s_Q[le][node][k] * lbv[l];
       }
-      const double* g3 = a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
+      const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + s) * 3 : a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
       real F[4];
       if (kind == SIDE_WALL) {

@@ -153,3 +153,9 @@ class GpuDGSEM:
 
     def launch_count(self):
         return self._lib.hg_launch_count(self._h)
+
+    def info(self):
+        """{N, n_elements, affine, precision} of the context."""
+        out = (C.c_int32 * 4)()
+        self._check(self._lib.hg_info(self._h, out))
+        return dict(N=out[0], n_elements=out[1], affine=bool(out[2]), precision=out[3])

@@ -120,6 +120,11 @@ int  hg_synchronize(hg_ctx* ctx);
 double* hg_device_state(hg_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t hg_launch_count(const hg_ctx* ctx);
+/* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
+int  hg_info(const hg_ctx* ctx, int32_t out[4]);
+/* Interpolation nodes and weights on [0,1] used by the kernels for order N
+ * (NodesAndWeightsClass.f90:251-332 computeNodesAndWeights).  xi, w: N+1 doubles. */
+int  hg_nodes(int32_t N, int32_t node_type, double* xi, double* w);
 
 #ifdef __cplusplus
 }

@@ -72,7 +72,8 @@ def test_curved_mesh_walls_and_dirichlet():
     mach = 0.3
     bcs = [dict(type=O.BC_DIRICHLET, mach=mach)] * 4 + [dict(type=O.BC_EULERWALL)]
     orc = O.Oracle(m, 4, nodes=O.LGL, riemann=O.LXF, mach=mach, bcs=bcs)
-    assert orc.edge_count(1) > 0 and orc.edge_count(2) == 0 and orc.edge_count(3) == 0
+    # curved boundary edges (kind 5) on the circle, no mortars (kinds 2, 3)
+    assert orc.edge_count(5) > 0 and orc.edge_count(2) == 0 and orc.edge_count(3) == 0
     q = dirichlet_state(orc, mach)
     Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=7)
     orc.set_state(Q)
@@ -91,3 +92,26 @@ def test_fp32_bulk_residual():
     g.set_state(Q0)
     out = g.compute_time_derivative(0.0).reshape(-1, 4)
     assert rel_l2(out[:, 0], ref.reshape(-1, 4)[:, 0]) <= 1e-5
+
+
+@pytest.mark.parametrize("nodes,N", [(O.LGL, 4), (O.LG, 6)])
+def test_affine_path_with_package_mesh_builder(nodes, N):
+    """The package's own box builder (affine kernel path) against the oracle's reference construction."""
+    from horses2d_b200 import mesh as hmesh, cases
+    nx, ny = 7, 5
+    m = hmesh.cartesian(nx, ny, -5.0, 5.0, -4.0, 4.0)
+    orc = O.Oracle(m, N, nodes=nodes, riemann=O.ROE, mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
+    X = orc.coords()
+    Q = perturbed(cases.isentropic_vortex(X[:, 0], X[:, 1]).ravel(), 0.01, seed=3)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g = hg.GpuDGSEM(hmesh.box_descriptor(nx, ny, -5.0, 5.0, -4.0, 4.0, N, nodes), mach=0.5, node_type=nodes,
+                    riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    assert g.info()["affine"]
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= TOL_STAGE
+    dt = orc.estimate_dt(0.4, 1.0)
+    for s in range(10):
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, 10, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_100

@@ -1,0 +1,57 @@
+"""Host-side mesh builders of the package against the oracle's reference-faithful construction (CPU)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from horses2d_b200 import mesh as hmesh, lib
+
+
+def side_table(d):
+    """Per element-side view of an edge-centric descriptor: neighbour, orientation, normals, dS."""
+    E = len(d["N"])
+    P = int(d["N"][0]) + 1
+    F = len(d["edge_marker"])
+    tab = {}
+    n = d["edge_n"].reshape(F, P, 2)
+    dS = d["edge_dS"].reshape(F, P)
+    for f in range(F):
+        L, R = d["edge_elem"][2 * f], d["edge_elem"][2 * f + 1]
+        sL, sR = d["edge_side"][2 * f], d["edge_side"][2 * f + 1]
+        inv = bool(d["edge_inverse"][f])
+        if d["edge_marker"][f] == 0:
+            tab[(L, sL)] = ("L", R, sR, inv, n[f], dS[f])
+            tab[(R, sR)] = ("R", L, sL, inv, n[f][::-1] if inv else n[f], dS[f][::-1] if inv else dS[f])
+        else:
+            p = d["periodic_partner"][f]
+            tab[(L, sL)] = ("B", d["edge_elem"][2 * p] if p >= 0 else -1, d["edge_side"][2 * p] if p >= 0 else 0,
+                            inv, n[f], dS[f])
+    assert len(tab) == 4 * E
+    return tab
+
+
+@pytest.mark.parametrize("nodes,N", [(O.LGL, 4), (O.LG, 3)])
+def test_box_descriptor_matches_reference_construction(nodes, N):
+    nx, ny = 5, 4
+    m = hmesh.cartesian(nx, ny, -5.0, 5.0, -2.0, 3.0)
+    orc = O.Oracle(m, N, nodes=nodes, bcs=hmesh.periodic_bcs_cartesian())
+    ref = orc.export_mesh()
+    ours = hmesh.box_descriptor(nx, ny, -5.0, 5.0, -2.0, 3.0, N, nodes)
+    for k in ("Ja", "jac", "x", "volume", "vertices"):
+        np.testing.assert_allclose(ours[k], ref[k], rtol=1e-13, atol=1e-13)
+    ta, tb = side_table(ours), side_table(ref)
+    for key, va in ta.items():
+        vb = tb[key]
+        assert va[:4] == vb[:4], key
+        np.testing.assert_allclose(va[4], vb[4], atol=1e-15)
+        np.testing.assert_allclose(va[5], vb[5], rtol=1e-14)
+
+
+def test_library_nodes_match_oracle():
+    for nodes in (O.LG, O.LGL):
+        for N in range(1, 9):
+            xi, w = lib.nodes(N, nodes)
+            orc = O.Oracle(hmesh.cartesian(1, 1, 0.0, 1.0, 0.0, 1.0), N, nodes=nodes,
+                           bcs=hmesh.periodic_bcs_cartesian())
+            X = orc.coords()[:N + 1, 0]
+            np.testing.assert_allclose(xi, X, rtol=0, atol=1e-15)
+            assert abs(w.sum() - 1.0) < 1e-15
