@@ -37,7 +37,8 @@ struct hg_ctx {
   void* d_G = nullptr;
   void* d_T[2] = {nullptr, nullptr};
   double* d_QDot = nullptr;
-  unsigned long long* d_resid = nullptr;
+  double* d_resid = nullptr;      // per-CTA partial maxima of |QDot| of the last stage [grid][4]
+  double* d_resid_out = nullptr;  // reduced maxima [4]
   double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
   int cur = 0;                    // which trace buffer holds the current traces
   bool affine = false;            // per-element constant metrics and per-side constant normals
@@ -70,30 +71,32 @@ static T* dalloc(size_t n) {
 static void free_ctx(hg_ctx* c) {
   if (!c) return;
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
-                  c->d_QDot, c->d_resid, c->d_elmax};
+                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
 // ------------------------------------------------------------------ launches
-constexpr int epb_for(int P) {
-  return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : 3;
+static int grid_for(int P, int n_el) {
+  const int epb = epb_for(P);
+  return (n_el + epb - 1) / epb;
 }
 
 template <int P, typename real>
 static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   constexpr int EPB = epb_for(P);
-  dim3 block(P * P, EPB), grid((a.n_el + EPB - 1) / EPB);
-  if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block, 0, c->stream>>>(a);
-  else stage_kernel<P, EPB, real, false><<<grid, block, 0, c->stream>>>(a);
+  const int grid = (a.n_el + EPB - 1) / EPB;
+  if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
+  else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
   ++c->launches;
 }
 
 template <int P, typename real>
 static void launch_trace_P(hg_ctx* c) {
   constexpr int EPB = epb_for(P);
-  dim3 block(P * P, EPB), grid((c->n_el + EPB - 1) / EPB);
-  trace_kernel<P, EPB, real><<<grid, block, 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats, static_cast<real*>(c->d_T[c->cur]));
+  const int grid = (c->n_el + EPB - 1) / EPB;
+  trace_kernel<P, EPB, real><<<grid, block_for(P), 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats,
+                                                                   static_cast<real*>(c->d_T[c->cur]));
   ++c->launches;
 }
 
@@ -151,20 +154,17 @@ static void traces(hg_ctx* c) {
 static void one_step(hg_ctx* c, int scheme, double t, double dt) {
   (void)t;
   if (scheme == HG_SCHEME_EULER) {
-    HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
     stage(c, 0.0, dt, 1.0, true, true, nullptr, true);
   } else if (scheme == HG_SCHEME_RK3) {
     const double am[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
     const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
     for (int m = 0; m < 3; ++m) {
-      if (m == 2) HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
       stage(c, am[m], 1.0, gm[m] * dt, m == 0, true, nullptr, m == 2);
     }
   } else if (scheme == HG_SCHEME_RK5) {
     const double am[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
     const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
     for (int m = 0; m < 5; ++m) {
-      if (m == 4) HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
       stage(c, am[m], dt, gm[m], m == 0, true, nullptr, m == 4);
     }
   } else {
@@ -344,14 +344,15 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->d_T[0] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_T[1] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_QDot = dalloc<double>(c->ndof);
-  c->d_resid = dalloc<unsigned long long>(4);
+  c->d_resid = dalloc<double>(size_t(grid_for(P, E)) * 4);
+  c->d_resid_out = dalloc<double>(4);
   c->d_elmax = dalloc<double>(size_t(E) * 2);
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_side_geo, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_vol_geo, vg.data(), vg.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
-  HG_CUDA(cudaMemset(c->d_resid, 0, 4 * sizeof(unsigned long long)));
+  HG_CUDA(cudaMemset(c->d_resid, 0, size_t(grid_for(P, E)) * 4 * sizeof(double)));
 }
 
 extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, const hg_bc_desc* bcs, int32_t n_bcs,
@@ -419,7 +420,6 @@ extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
   try {
     require_state(c);
     (void)t;
-    HG_CUDA(cudaMemsetAsync(c->d_resid, 0, 4 * sizeof(unsigned long long), c->stream));
     stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, true);
     HG_CUDA(cudaGetLastError());
     if (QDot) {
@@ -450,10 +450,11 @@ extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double 
 
 extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
   try {
-    unsigned long long r[4];
-    HG_CUDA(cudaMemcpyAsync(r, c->d_resid, sizeof(r), cudaMemcpyDeviceToHost, c->stream));
+    residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c->P, c->n_el), c->d_resid, c->d_resid_out);
+    ++c->launches;
+    HG_CUDA(cudaGetLastError());
+    HG_CUDA(cudaMemcpyAsync(out, c->d_resid_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
-    for (int k = 0; k < 4; ++k) { double v; std::memcpy(&v, &r[k], 8); out[k] = v; }
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }

@@ -19,6 +19,11 @@
 // The Riemann flux of an interior face is evaluated by both of its elements with
 // identical arguments (LEFT trace, RIGHT trace, LEFT's normal), so both see the
 // same value and the face needs no separate launch or flux buffer.
+//
+// CTAs are one-dimensional, padded to whole warps (threads past EPB*(N+1)^2 only
+// take part in barriers and reductions).  Shared tiles are variable-major
+// ([var][element][node]) so that a warp reading one row or column of a tile
+// touches consecutive words.
 #pragma once
 #include "hg_physics.cuh"
 
@@ -37,8 +42,8 @@ template <typename real>
 struct StageArgs {
   int n_el;
   const int4* side;        // [n_el*4] {neighbour trace slot, flags, zone, 0}
-  const double* side_geo;  // [n_el*4][P][3]  nx, ny, dS in this element's side order
-  const double* vol_geo;   // [n_el][P*P][5]  Ja00 Ja01 Ja10 Ja11 1/J
+  const double* side_geo;  // [n_el*4][P][3] (or [n_el*4][3] affine)  nx, ny, dS in this element's side order
+  const double* vol_geo;   // [n_el][P*P][5] (or [n_el][5] affine)  Ja00 Ja01 Ja10 Ja11 1/J
   const double* mats;      // hatD[P*P], lb0[P], lb1[P], lbw0[P], lbw1[P]
   const Zone* zones;
   double* Q;               // [n_el][P*P][4]
@@ -46,7 +51,7 @@ struct StageArgs {
   const real* T_in;        // [n_el*4][P][4]
   real* T_out;
   double* QDot;            // optional output (time derivative only)
-  unsigned long long* resid;   // optional max |QDot| per variable (bit patterns of non-negative doubles)
+  double* resid;           // optional per-CTA max |QDot| per variable: [gridDim.x][4]
   double a, b, c;          // G = a G + b QDot ; Q += c G
   int first;               // a == 0: do not read G
   int update;              // 1: RK update, 0: only QDot (and traces of the unchanged Q)
@@ -54,40 +59,43 @@ struct StageArgs {
   PhysConst pc;
 };
 
-template <int P>
-struct Layout {
-  static constexpr int NP = P * P;
-  static constexpr int FT = 4 * P;   // face-node tasks per element
-};
+__host__ __device__ constexpr int epb_for(int P) {
+  return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : 3;
+}
+__host__ __device__ constexpr int block_for(int P) { return ((P * P * epb_for(P) + 31) / 32) * 32; }
+
+// max that keeps NaN (a residual that is NaN must stay visible)
+__device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
 
 // AFFINE: metrics constant per element (vol_geo [n_el][5]) and normals/dS constant
 // per side (side_geo [n_el*4][3]), as for parallelogram elements with straight edges.
 template <int P, int EPB, typename real, bool AFFINE>
-__global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
+__global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) {
   constexpr int NP = P * P;
   constexpr int FT = 4 * P;
+  constexpr int NW = block_for(P) / 32;
   __shared__ real s_mat[NP + 4 * P];
-  __shared__ real s_Fc[EPB][NP][4];
-  __shared__ real s_Gc[EPB][NP][4];
-  __shared__ real s_Q[EPB][NP][4];
-  __shared__ real s_F[EPB][FT][4];
+  __shared__ real s_Fc[4][EPB][NP];
+  __shared__ real s_Gc[4][EPB][NP];
+  __shared__ real s_Q[4][EPB][NP];
+  __shared__ real s_F[4][EPB][FT];
+  __shared__ double s_red[NW][4];
 
-  const int tid = threadIdx.x;            // node in element
-  const int le = threadIdx.y;             // element in block
-  const int flat = le * NP + tid;
-  for (int k = flat; k < NP + 4 * P; k += NP * EPB) s_mat[k] = real(a.mats[k]);
+  const int flat = threadIdx.x;
+  const int le = flat / NP;               // element in block
+  const int tid = flat - le * NP;         // node in element
+  for (int k = flat; k < NP + 4 * P; k += blockDim.x) s_mat[k] = real(a.mats[k]);
   const int e = blockIdx.x * EPB + le;
-  const bool active = e < a.n_el;
+  const bool active = le < EPB && e < a.n_el;
   Phys<real> ph;
   ph.load(a.pc);
   const int i = tid % P, j = tid / P;
 
-  real q[4];
   real geo[5];
   if (active) {
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
-    q[0] = real(q01.x); q[1] = real(q01.y); q[2] = real(q23.x); q[3] = real(q23.y);
+    const real q[4] = {real(q01.x), real(q01.y), real(q23.x), real(q23.y)};
     const double* gp = AFFINE ? a.vol_geo + size_t(e) * 5 : a.vol_geo + (size_t(e) * NP + tid) * 5;
 #pragma unroll
     for (int k = 0; k < 5; ++k) geo[k] = real(gp[k]);
@@ -95,9 +103,9 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
     inviscid_flux(ph, q, f, g);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      s_Fc[le][tid][k] = f[k] * geo[0] + g[k] * geo[2];   // F Ja(1,IX) + G Ja(2,IX)
-      s_Gc[le][tid][k] = f[k] * geo[1] + g[k] * geo[3];   // F Ja(1,IY) + G Ja(2,IY)
-      s_Q[le][tid][k] = q[k];
+      s_Fc[k][le][tid] = f[k] * geo[0] + g[k] * geo[2];   // F Ja(1,IX) + G Ja(2,IX)
+      s_Gc[k][le][tid] = f[k] * geo[1] + g[k] * geo[3];   // F Ja(1,IY) + G Ja(2,IY)
+      s_Q[k][le][tid] = q[k];
     }
   }
   __syncthreads();
@@ -113,13 +121,13 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
       const int s = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + s];
       const int kind = sd.y & 15;
-      // own trace at side node kk
       const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
       real qo[4] = {real(0), real(0), real(0), real(0)};
+#pragma unroll
       for (int l = 0; l < P; ++l) {
         const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) qo[k] += s_Q[le][node][k] * lbv[l];
+        for (int k = 0; k < 4; ++k) qo[k] += s_Q[k][le][node] * lbv[l];
       }
       const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + s) * 3 : a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
         }
       }
 #pragma unroll
-      for (int k = 0; k < 4; ++k) s_F[le][t][k] = F[k];
+      for (int k = 0; k < 4; ++k) s_F[k][le][t] = F[k];
     }
   }
   __syncthreads();
@@ -163,23 +171,16 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
     for (int l = 0; l < P; ++l) {
       const real hi = hatD[i * P + l], hj = hatD[j * P + l];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s_Fc[le][j * P + l][k] + hj * s_Gc[le][l * P + i][k];
+      for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s_Fc[k][le][j * P + l] + hj * s_Gc[k][le][l * P + i];
     }
     // lift: bottom F(i) lbw0(j), right F(j) lbw1(i), top F(i) lbw1(j), left F(j) lbw0(i)
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      qd[k] = qd[k] - s_F[le][0 * P + i][k] * lbw0[j];
-      qd[k] = qd[k] - s_F[le][1 * P + j][k] * lbw1[i];
-      qd[k] = qd[k] - s_F[le][2 * P + i][k] * lbw1[j];
-      qd[k] = qd[k] - s_F[le][3 * P + j][k] * lbw0[i];
+      qd[k] = qd[k] - s_F[k][le][0 * P + i] * lbw0[j];
+      qd[k] = qd[k] - s_F[k][le][1 * P + j] * lbw1[i];
+      qd[k] = qd[k] - s_F[k][le][2 * P + i] * lbw1[j];
+      qd[k] = qd[k] - s_F[k][le][3 * P + j] * lbw0[i];
       qd[k] = qd[k] * geo[4];
-    }
-    if (a.resid) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double v = fabs(double(qd[k]));
-        atomicMax(&a.resid[k], (unsigned long long)__double_as_longlong(v));
-      }
     }
     const size_t off = (size_t(e) * NP + tid) * 4;
     if (a.QDot) {
@@ -205,21 +206,40 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
       q23.x = q23.x + a.c * double(gn[2]);
       q23.y = q23.y + a.c * double(gn[3]);
       qp[0] = q01; qp[1] = q23;
-      s_Q[le][tid][0] = real(q01.x); s_Q[le][tid][1] = real(q01.y);
-      s_Q[le][tid][2] = real(q23.x); s_Q[le][tid][3] = real(q23.y);
+      s_Q[0][le][tid] = real(q01.x); s_Q[1][le][tid] = real(q01.y);
+      s_Q[2][le][tid] = real(q23.x); s_Q[3][le][tid] = real(q23.y);
     }
   }
+  if (a.resid) {   // uniform over the grid: every thread of the CTA takes part
+    double m[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) m[k] = active ? fabs(double(qd[k])) : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) m[k] = nanmax(m[k], __shfl_xor_sync(0xffffffffu, m[k], off));
+    if ((flat & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s_red[flat >> 5][k] = m[k];
+  }
   __syncthreads();
+  if (a.resid && flat < 4) {
+    double mx = 0.0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) mx = nanmax(mx, s_red[w][flat]);
+    a.resid[size_t(blockIdx.x) * 4 + flat] = mx;
+  }
   // traces of the updated state for the next launch
   if (active && a.update) {
     for (int t = tid; t < FT; t += NP) {
       const int s = t / P, kk = t % P;
       const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
       real tr[4] = {real(0), real(0), real(0), real(0)};
+#pragma unroll
       for (int l = 0; l < P; ++l) {
         const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) tr[k] += s_Q[le][node][k] * lbv[l];
+        for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
       }
       real* tp = a.T_out + ((size_t(e) * 4 + s) * P + kk) * 4;
 #pragma unroll
@@ -230,19 +250,19 @@ __global__ void __launch_bounds__(P * P * EPB) stage_kernel(StageArgs<real> a) {
 
 // Traces of the resident state (after hg_set_state).
 template <int P, int EPB, typename real>
-__global__ void __launch_bounds__(P * P * EPB) trace_kernel(int n_el, const double* Q, const double* mats, real* T) {
+__global__ void __launch_bounds__(block_for(P)) trace_kernel(int n_el, const double* Q, const double* mats, real* T) {
   constexpr int NP = P * P;
   constexpr int FT = 4 * P;
   __shared__ real s_lb[2 * P];
-  __shared__ real s_Q[EPB][NP][4];
-  const int tid = threadIdx.x, le = threadIdx.y;
-  const int flat = le * NP + tid;
-  for (int k = flat; k < 2 * P; k += NP * EPB) s_lb[k] = real(mats[NP + k]);
+  __shared__ real s_Q[4][EPB][NP];
+  const int flat = threadIdx.x;
+  const int le = flat / NP, tid = flat - le * NP;
+  for (int k = flat; k < 2 * P; k += blockDim.x) s_lb[k] = real(mats[NP + k]);
   const int e = blockIdx.x * EPB + le;
-  const bool active = e < n_el;
+  const bool active = le < EPB && e < n_el;
   if (active)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) s_Q[le][tid][k] = real(Q[(size_t(e) * NP + tid) * 4 + k]);
+    for (int k = 0; k < 4; ++k) s_Q[k][le][tid] = real(Q[(size_t(e) * NP + tid) * 4 + k]);
   __syncthreads();
   if (!active) return;
   for (int t = tid; t < FT; t += NP) {
@@ -252,12 +272,31 @@ __global__ void __launch_bounds__(P * P * EPB) trace_kernel(int n_el, const doub
     for (int l = 0; l < P; ++l) {
       const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) tr[k] += s_Q[le][node][k] * lbv[l];
+      for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
     }
     real* tp = T + ((size_t(e) * 4 + s) * P + kk) * 4;
 #pragma unroll
     for (int k = 0; k < 4; ++k) tp[k] = tr[k];
   }
+}
+
+// Max over the per-CTA residual partials: out[k] = max_b part[b*4+k] (NaN kept).
+__global__ void residual_reduce_kernel(int nblocks, const double* part, double* out) {
+  __shared__ double s[4][256];
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) m[k] = nanmax(m[k], part[size_t(b) * 4 + k]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = m[k];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = nanmax(s[k][threadIdx.x], s[k][threadIdx.x + w]);
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = s[threadIdx.x][0];
 }
 
 }  // namespace hg

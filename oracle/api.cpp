@@ -242,3 +242,26 @@ extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* 
   }
   return 0;
 }
+
+extern "C" int or_zone_edge_nodes(void* h, int zone, double* X) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  if (zone < 1 || zone >= int(o.zones.size())) return -1;
+  int n = 0;
+  for (int id : o.zones[zone].edges) {
+    const Edge& f = o.ed[id];
+    const int P = f.P();
+    for (int p = 0; p < P; ++p, ++n)
+      if (X) { X[2 * n] = f.X[p]; X[2 * n + 1] = f.X[P + p]; }
+  }
+  return n;
+}
+
+extern "C" void or_set_zone_state(void* h, int zone, const double* uB) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  int n = 0;
+  for (int id : o.zones[zone].edges) {
+    Edge& f = o.ed[id];
+    for (int p = 0; p < f.P(); ++p, ++n)
+      for (int k = 0; k < 4; ++k) f.uB_own[4 * p + k] = uB[4 * n + k];
+  }
+}

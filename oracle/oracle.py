@@ -82,6 +82,9 @@ def lib():
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
         L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
+        L.or_zone_edge_nodes.restype = i
+        L.or_zone_edge_nodes.argtypes = [vp, i, dp]
+        L.or_set_zone_state.argtypes = [vp, i, dp]
         _lib = L
     return _lib
 
@@ -205,6 +208,16 @@ class Oracle:
 
     def edge_count(self, kind):
         return lib().or_edge_count_by_type(self.h, kind)
+
+    def zone_edge_nodes(self, zone):
+        n = lib().or_zone_edge_nodes(self.h, zone, None)
+        X = np.zeros((n, 2))
+        lib().or_zone_edge_nodes(self.h, zone, _p(X, C.c_double))
+        return X
+
+    def set_zone_state(self, zone, uB):
+        uB = np.ascontiguousarray(uB, dtype=np.float64)
+        lib().or_set_zone_state(self.h, zone, _p(uB, C.c_double))
 
     def export_mesh(self):
         """The constructed mesh flattened like include/horses_gpu.h hg_mesh_desc."""

@@ -42,7 +42,7 @@ typedef struct {
   double aoa_deg;           /* angle of attack, degrees */
   int    wall_type;         /* viscous wall: 1 isothermal, 2 adiabatic */
   double wall_T;            /* isothermal wall temperature, K */
-  double wall_v[2];         /* wall velocity, m/s */
+  double wall_v[2];         /* wall velocity, dimensionless: sqrt(gamma) * Mach * direction */
   int    outflow_type;      /* pressure outlet: 1 reflective, 2 partially non-reflective */
 } or_bc;
 
@@ -101,6 +101,12 @@ int     or_edge_count_by_type(void* h, int type);
  * volume[E], vertices[E*8], edge_elem[2F], edge_side[2F], edge_inverse[F],
  * edge_marker[F], edge_n[F*P*2], edge_dS[F*P], periodic_partner[F], edge_invh[F].
  * Returns 0, or -1 when the mesh has mortars or mixed orders. */
+/* Boundary states given by functions (the problem-file plugin's BoundaryConditionFunction,
+ * BoundaryConditions/BoundaryConditionFunctionDrivers.incf): or_zone_edge_nodes returns the
+ * number of edge nodes of a zone and (if X != NULL) their coordinates [n][2], edges in
+ * mesh order; or_set_zone_state sets the zone's boundary state uB [n][4] at those nodes. */
+int     or_zone_edge_nodes(void* h, int zone, double* X);
+void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                        int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
                        double* edge_dS, int* periodic_partner, double* edge_invh);
