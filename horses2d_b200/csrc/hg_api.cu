@@ -7,6 +7,7 @@
 // Runge-Kutta schemes (Approximation/DGTimeIntegrator.f90:263-365).
 #include "../../include/horses_gpu.h"
 #include "hg_stage.cuh"
+#include "hg_ns.cuh"
 #include "hg_spectral.h"
 
 #include <cuda_runtime.h>
@@ -42,6 +43,11 @@ struct hg_ctx {
   double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
   int cur = 0;                    // which trace buffer holds the current traces
   bool affine = false;            // per-element constant metrics and per-side constant normals
+  bool ns = false, ip = false, grad_faces = false;   // Navier-Stokes kernels; interior penalty; SIPG/NIPG faces
+  double sigma0 = 0.0, epsilon = 0.0, temperature_ref = 273.15;
+  double* d_side_invh = nullptr;  // [n_el*4] invh of each side's edge
+  double* d_jac = nullptr;        // [n_el][NP] J (curved meshes, gradient faces)
+  void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
   bool state_set = false;
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
@@ -71,15 +77,15 @@ static T* dalloc(size_t n) {
 static void free_ctx(hg_ctx* c) {
   if (!c) return;
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
-                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax};
+                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
 // ------------------------------------------------------------------ launches
-static int grid_for(int P, int n_el) {
-  const int epb = epb_for(P);
-  return (n_el + epb - 1) / epb;
+static int grid_for(const hg_ctx* c) {
+  const int epb = c->ns ? epb_ns(c->P) : epb_for(c->P);
+  return (c->n_el + epb - 1) / epb;
 }
 
 template <int P, typename real>
@@ -100,6 +106,21 @@ static void launch_trace_P(hg_ctx* c) {
   ++c->launches;
 }
 
+template <int P, typename real, bool AFFINE, bool IP>
+static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
+  constexpr int EPB = epb_ns(P);
+  const int grid = (a.n_el + EPB - 1) / EPB;
+  ns_gradient_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a);
+  ns_stage_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a);
+  c->launches += 2;
+}
+
+template <int P, typename real>
+static void launch_ns_P(hg_ctx* c, const NSArgs<real>& a) {
+  if (c->affine) { if (c->ip) launch_ns_PAI<P, real, true, true>(c, a); else launch_ns_PAI<P, real, true, false>(c, a); }
+  else { if (c->ip) launch_ns_PAI<P, real, false, true>(c, a); else launch_ns_PAI<P, real, false, false>(c, a); }
+}
+
 #define HG_DISPATCH_P(P_, FN, ...)                      \
   switch (P_) {                                         \
     case 2: FN<2, real>(__VA_ARGS__); break;            \
@@ -117,7 +138,39 @@ template <typename real>
 static void run_trace(hg_ctx* c) { HG_DISPATCH_P(c->P, launch_trace_P, c); }
 
 template <typename real>
+static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+  NSArgs<real> a{};
+  a.n_el = c->n_el;
+  a.side = c->d_side;
+  a.side_geo = c->d_side_geo;
+  a.side_invh = c->d_side_invh;
+  a.vol_geo = c->d_vol_geo;
+  a.jac = c->d_jac;
+  a.mats = c->d_mats;
+  a.zones = c->d_zones;
+  a.Q = c->d_Q;
+  a.G = static_cast<real*>(c->d_G);
+  a.T_in = static_cast<const real*>(c->d_T[c->cur]);
+  a.T_out = static_cast<real*>(c->d_T[c->cur ^ 1]);
+  a.GT = static_cast<real*>(c->d_GT);
+  a.QDot = qdot;
+  a.resid = resid ? c->d_resid : nullptr;
+  a.a = ca; a.b = cb; a.c = cc;
+  a.first = first ? 1 : 0;
+  a.update = update ? 1 : 0;
+  a.riemann = c->riemann;
+  a.ip = c->ip ? 1 : 0;
+  a.grad_faces = c->grad_faces ? 1 : 0;
+  a.sigma0 = c->sigma0;
+  a.epsilon = c->epsilon;
+  a.pc = c->pc;
+  HG_DISPATCH_P(c->P, launch_ns_P, c, a);
+  if (update) c->cur ^= 1;
+}
+
+template <typename real>
 static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+  if (c->ns) { run_ns_stage<real>(c, ca, cb, cc, first, update, qdot, resid); return; }
   StageArgs<real> a{};
   a.n_el = c->n_el;
   a.side = c->d_side;
@@ -202,9 +255,13 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   for (int e = 0; e < E; ++e)
     if (m->N[e] != N) throw std::runtime_error("mixed polynomial orders are not supported by this kernel set");
   if (N < 1 || N > 8) throw std::runtime_error("polynomial order must be in 1..8");
-  if (ph->navier_stokes && ph->reynolds != 0.0)
-    throw std::runtime_error("viscous terms are not available in this kernel set (Reynolds number must be 0)");
   const int P = N + 1, NP = P * P;
+  // the Navier-Stokes build with Re = 0 has mu = 0: its viscous terms vanish identically
+  c->ns = ph->navier_stokes != 0 && ph->reynolds != 0.0;
+  c->ip = ph->viscous == 1;
+  c->grad_faces = c->ip && ph->ip_method != 2;
+  c->sigma0 = ph->sigma0_ip;
+  c->epsilon = ph->ip_method == 0 ? -1.0 : (ph->ip_method == 1 ? 1.0 : 0.0);
   c->n_el = E; c->N = N; c->P = P; c->node_type = ph->node_type; c->riemann = ph->riemann;
   if (c->riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
   c->ndof = int64_t(E) * NP * 4;
@@ -215,6 +272,10 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->pc.cp = gamma / (gamma - 1.0);
   c->pc.cv = 1.0 / (gamma - 1.0);
   c->pc.invSqrtGammaMach = 1.0 / (std::sqrt(gamma) * ph->mach);
+  c->pc.mu = c->ns ? 1.0 / ph->reynolds : 0.0;
+  c->pc.cpPr = c->pc.cp / ph->prandtl;
+  c->pc.lambda = -2.0 / 3.0;
+  c->temperature_ref = ph->temperature_ref;
 
   // nodal operators
   NodalOps ops = make_nodal_ops(N, ph->node_type);
@@ -224,6 +285,9 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   mats.insert(mats.end(), ops.lb1.begin(), ops.lb1.end());
   mats.insert(mats.end(), ops.lbw0.begin(), ops.lbw0.end());
   mats.insert(mats.end(), ops.lbw1.begin(), ops.lbw1.end());
+  mats.insert(mats.end(), ops.D.begin(), ops.D.end());
+  mats.insert(mats.end(), ops.dlbw0.begin(), ops.dlbw0.end());
+  mats.insert(mats.end(), ops.dlbw1.begin(), ops.dlbw1.end());
 
   // volume metrics
   std::vector<double> vg(size_t(E) * NP * 5);
@@ -239,11 +303,17 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
     zones[z].type = bcs[z].type;
     zones[z].riemann = bcs[z].riemann;
     for (int k = 0; k < 4; ++k) zones[z].q[k] = bcs[z].state[k];
+    zones[z].Tw = bcs[z].wall_T;
+    zones[z].vw[0] = bcs[z].wall_v[0];
+    zones[z].vw[1] = bcs[z].wall_v[1];
+    zones[z].wall_type = bcs[z].wall_type;
+    zones[z].outflow_type = bcs[z].outflow_type;
     if (bcs[z].riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
   }
 
   // side tables
   std::vector<int4> side(size_t(E) * 4, make_int4(-2, 0, -1, 0));
+  std::vector<double> sinvh(size_t(E) * 4, 0.0);
   std::vector<double> sg(size_t(E) * 4 * P * 3, 0.0);
   auto set_geo = [&](int e, int s, int edge, bool rev) {
     for (int k = 0; k < P; ++k) {
@@ -266,6 +336,7 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
       side[size_t(R) * 4 + sR] = make_int4(L * 4 + sL, SIDE_RIGHT | (inv ? SIDE_REVERSED : 0), -1, 0);
       set_geo(L, sL, f, false);
       set_geo(R, sR, f, inv);
+      if (m->edge_invh) sinvh[size_t(L) * 4 + sL] = sinvh[size_t(R) * 4 + sR] = m->edge_invh[f];
     } else {
       if (marker < 1 || marker > n_bcs) throw std::runtime_error("boundary edge with unknown marker");
       const hg_bc_desc& b = bcs[marker - 1];
@@ -279,10 +350,14 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
           break;
         }
         case HG_BC_EULERWALL: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_WALL, z, 0); break;
-        case HG_BC_DIRICHLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
-        default: throw std::runtime_error("boundary condition kind not available on the device in this kernel set");
+        case HG_BC_DIRICHLET:
+        case HG_BC_VISCOUSWALL:
+        case HG_BC_FARFIELD:
+        case HG_BC_PRESSUREOUTLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
+        default: throw std::runtime_error("unknown boundary condition kind");
       }
       set_geo(L, sL, f, false);
+      if (m->edge_invh) sinvh[size_t(L) * 4 + sL] = m->edge_invh[f];
     }
   }
   for (size_t s = 0; s < side.size(); ++s)
@@ -344,15 +419,25 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->d_T[0] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_T[1] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_QDot = dalloc<double>(c->ndof);
-  c->d_resid = dalloc<double>(size_t(grid_for(P, E)) * 4);
+  c->d_resid = dalloc<double>(size_t(grid_for(c)) * 4);
   c->d_resid_out = dalloc<double>(4);
   c->d_elmax = dalloc<double>(size_t(E) * 2);
+  if (c->ns) {
+    if (c->ip && !m->edge_invh) throw std::runtime_error("interior penalty needs edge_invh");
+    c->d_side_invh = dalloc<double>(sinvh.size());
+    c->d_GT = dalloc<char>(size_t(E) * 4 * P * 8 * rs);
+    HG_CUDA(cudaMemcpy(c->d_side_invh, sinvh.data(), sinvh.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (!c->affine) {
+      c->d_jac = dalloc<double>(size_t(E) * NP);
+      HG_CUDA(cudaMemcpy(c->d_jac, m->jac, size_t(E) * NP * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  }
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_side_geo, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_vol_geo, vg.data(), vg.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
-  HG_CUDA(cudaMemset(c->d_resid, 0, size_t(grid_for(P, E)) * 4 * sizeof(double)));
+  HG_CUDA(cudaMemset(c->d_resid, 0, size_t(grid_for(c)) * 4 * sizeof(double)));
 }
 
 extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, const hg_bc_desc* bcs, int32_t n_bcs,
@@ -450,7 +535,7 @@ extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double 
 
 extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
   try {
-    residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c->P, c->n_el), c->d_resid, c->d_resid_out);
+    residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c), c->d_resid, c->d_resid_out);
     ++c->launches;
     HG_CUDA(cudaGetLastError());
     HG_CUDA(cudaMemcpyAsync(out, c->d_resid_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

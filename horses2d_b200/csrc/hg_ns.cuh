@@ -1,0 +1,464 @@
+// hg_ns.cuh -- Navier-Stokes stage kernels (BR1 and interior penalty) for sm_100a.
+//
+// Per Runge-Kutta stage two launches:
+//   ns_gradient_kernel  the element gradient dQ -- BR1 lifting
+//        dQ = [ -VolGreen(Q Ja) + sum_faces lift(u* dS n) ] / J,  u* = (QL + QR)/2 or the
+//        boundary's viscous state (BR1_ComputeGradient, Approximation/DGViscous_BR1.f90:48-111;
+//        ComputeSolutionRiemann_*, DGViscousMethods.f90:538-917), or the interior-penalty local
+//        gradient (ComputeInteriorGradient, Mesh/QuadElement_QuadProcedures.incf:42-88) -- and
+//        writes only its traces on the four sides (interpolateGradientsToBoundaries,
+//        DGSpatialDiscretizationMethods.f90:1577-1631);
+//   ns_stage_kernel     recomputes dQ in shared memory (the full gradient never goes to HBM),
+//        F = Fi - Fv at the nodes (QDotVolumeLoop :243-268), face fluxes
+//        F* = (Fi* - Fv*) dS with the neighbours' Q and dQ traces (BR1: (FvL+FvR)/2 . n; IP adds
+//        sigma0 mu N^2 invh (uL - uR), DGViscous_IP.f90:45-130), boundary viscous fluxes by
+//        condition (Dirichlet / adiabatic / Neumann, :1142-1511), the interior-penalty gradient-face
+//        terms lifted by Scalar_StdGradientFace (DGWeakIntegrals.f90:268-495), 1/J, the RK update
+//        and the new Q traces.
+// Artificial viscosity enters as an element viscosity mu_a (Physical type) when given.
+#pragma once
+#include "hg_stage.cuh"
+
+namespace hg {
+
+template <typename real>
+struct NSArgs {
+  int n_el;
+  const int4* side;         // [n_el*4] {neighbour trace slot, flags, zone, 0}
+  const double* side_geo;   // normals / dS (per node, or per side when AFFINE)
+  const double* side_invh;  // [n_el*4] invh of the side's edge
+  const double* vol_geo;    // Ja00 Ja01 Ja10 Ja11 1/J (per node, or per element when AFFINE)
+  const double* jac;        // [n_el][NP] J per node (curved gradient faces)
+  const double* mats;       // hatD[NP] lb0 lb1 lbw0 lbw1 [P each] D[NP] dlbw0 dlbw1 [P each]
+  const Zone* zones;
+  double* Q;
+  real* G;
+  const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
+  real* T_out;
+  real* GT;                 // dQ traces                      [n_el*4][P][2][4]
+  double* QDot;
+  double* resid;
+  double a, b, c;
+  int first, update, riemann;
+  int ip, grad_faces;       // interior penalty (else BR1); gradient-face terms (SIPG/NIPG)
+  double sigma0, epsilon;
+  PhysConst pc;
+};
+
+__host__ __device__ constexpr int epb_ns(int P) {
+  return P == 2 ? 16 : P == 3 ? 7 : P == 4 ? 8 : P == 5 ? 5 : P == 6 ? 4 : P == 7 ? 3 : 2;
+}
+__host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) + 31) / 32) * 32; }
+
+// Shared tiles of one CTA.
+template <int P, int EPB, typename real, bool AFFINE>
+struct NSTiles {
+  static constexpr int NP = P * P, FT = 4 * P;
+  real mat[2 * NP + 6 * P];
+  real Q[4][EPB][NP];
+  real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : NP];   // Ja00 Ja01 Ja10 Ja11 J
+  real dQ[2][4][EPB][NP];
+  real Fc[4][EPB][NP];
+  real Gc[4][EPB][NP];
+  real face[12][EPB][FT];   // BR1 u* dS n (8) / F* (4) + gradient-face contravariant fluxes (8)
+  double red[32][4];
+};
+
+template <int P, int EPB, typename real, bool AFFINE>
+__device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE>& s, const real (*src)[EPB][P * P], int k,
+                                         int le, int side, int kk, const real* lbv) {
+  real t = real(0);
+#pragma unroll
+  for (int l = 0; l < P; ++l) {
+    const int node = (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
+    t += src[k][le][node] * lbv[l];
+  }
+  return t;
+}
+
+// Element gradient into s.dQ (both kernels).  Requires s.Q (and s.Ja) filled and synchronized.
+template <int P, int EPB, typename real, bool AFFINE, bool IP>
+__device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+                                                 const Phys<real>& ph, int le, int tid, int e, bool active,
+                                                 const real* geoE) {
+  constexpr int NP = P * P, FT = 4 * P;
+  const real* hatD = s.mat;
+  const real* lb0 = s.mat + NP;
+  const real* lb1 = lb0 + P;
+  const real* lbw0 = lb1 + P;
+  const real* lbw1 = lbw0 + P;
+  const real* D = lbw1 + P;
+  const int i = tid % P, j = tid / P;
+  if (!IP) {
+    // BR1 face terms u* dS n (outward normal of this element)
+    if (active) {
+      for (int t = tid; t < FT; t += NP) {
+        const int sd_ = t / P, kk = t % P;
+        const int4 sd = a.side[size_t(e) * 4 + sd_];
+        const int kind = sd.y & 15;
+        const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+        real qo[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+        const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
+        const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
+        real us[4];
+        if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
+          const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+          const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) us[k] = kind == SIDE_RIGHT ? real(0.5) * (tp[k] + qo[k]) : real(0.5) * (qo[k] + tp[k]);
+        } else {
+          real uB[4];
+          bc_states(ph, a.zones[sd.z], qo, nx, ny, uB, us);
+        }
+        const real sg = kind == SIDE_RIGHT ? real(-1) : real(1);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          s.face[k][le][t] = (sg * us[k]) * dS * nx;
+          s.face[4 + k][le][t] = (sg * us[k]) * dS * ny;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (active) {
+    real Ja00, Ja01, Ja10, Ja11, iJ;
+    if constexpr (AFFINE) { Ja00 = geoE[0]; Ja01 = geoE[1]; Ja10 = geoE[2]; Ja11 = geoE[3]; iJ = geoE[4]; }
+    else { Ja00 = s.Ja[0][le][tid]; Ja01 = s.Ja[1][le][tid]; Ja10 = s.Ja[2][le][tid]; Ja11 = s.Ja[3][le][tid];
+           iJ = real(1) / s.Ja[4][le][tid]; }
+    if (IP) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        real dxi = real(0), deta = real(0);
+#pragma unroll
+        for (int l = 0; l < P; ++l) {
+          dxi += D[i * P + l] * s.Q[k][le][j * P + l];
+          deta += D[j * P + l] * s.Q[k][le][l * P + i];
+        }
+        s.dQ[0][k][le][tid] = (dxi * Ja00 + deta * Ja01) * iJ;
+        s.dQ[1][k][le][tid] = (dxi * Ja10 + deta * Ja11) * iJ;
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        real v0 = real(0), v1 = real(0);
+        if constexpr (AFFINE) {
+          real axi = real(0), aeta = real(0);
+#pragma unroll
+          for (int l = 0; l < P; ++l) {
+            axi += hatD[i * P + l] * s.Q[k][le][j * P + l];
+            aeta += hatD[j * P + l] * s.Q[k][le][l * P + i];
+          }
+          v0 = axi * Ja00 + aeta * Ja01;
+          v1 = axi * Ja10 + aeta * Ja11;
+        } else {
+#pragma unroll
+          for (int l = 0; l < P; ++l) {
+            const int nx_ = j * P + l, ny_ = l * P + i;
+            const real qx = s.Q[k][le][nx_] * hatD[i * P + l], qy = s.Q[k][le][ny_] * hatD[j * P + l];
+            v0 += qx * s.Ja[0][le][nx_] + qy * s.Ja[1][le][ny_];
+            v1 += qx * s.Ja[2][le][nx_] + qy * s.Ja[3][le][ny_];
+          }
+        }
+        const real l0 = s.face[k][le][0 * P + i] * lbw0[j] + s.face[k][le][1 * P + j] * lbw1[i] +
+                        s.face[k][le][2 * P + i] * lbw1[j] + s.face[k][le][3 * P + j] * lbw0[i];
+        const real l1 = s.face[4 + k][le][0 * P + i] * lbw0[j] + s.face[4 + k][le][1 * P + j] * lbw1[i] +
+                        s.face[4 + k][le][2 * P + i] * lbw1[j] + s.face[4 + k][le][3 * P + j] * lbw0[i];
+        s.dQ[0][k][le][tid] = (-v0 + l0) * iJ;
+        s.dQ[1][k][le][tid] = (-v1 + l1) * iJ;
+      }
+    }
+  }
+}
+
+template <int P, int EPB, typename real, bool AFFINE>
+__device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s, int flat, int le,
+                                           int tid, int e, bool active, real* geoE) {
+  constexpr int NP = P * P;
+  for (int k = flat; k < 2 * NP + 6 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
+  if (active) {
+    const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
+    const double2 q01 = qp[0], q23 = qp[1];
+    s.Q[0][le][tid] = real(q01.x); s.Q[1][le][tid] = real(q01.y);
+    s.Q[2][le][tid] = real(q23.x); s.Q[3][le][tid] = real(q23.y);
+    if constexpr (AFFINE) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) geoE[k] = real(a.vol_geo[size_t(e) * 5 + k]);
+    } else {
+      const double* gp = a.vol_geo + (size_t(e) * NP + tid) * 5;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s.Ja[k][le][tid] = real(gp[k]);
+      s.Ja[4][le][tid] = real(a.jac[size_t(e) * NP + tid]);
+      geoE[4] = real(gp[4]);
+    }
+  }
+}
+
+template <int P, int EPB, typename real, bool AFFINE, bool IP>
+__global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a) {
+  constexpr int NP = P * P, FT = 4 * P;
+  __shared__ NSTiles<P, EPB, real, AFFINE> s;
+  const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
+  const int e = blockIdx.x * EPB + le;
+  const bool active = le < EPB && e < a.n_el;
+  Phys<real> ph;
+  ph.load(a.pc);
+  real geoE[5];
+  load_tiles(a, s, flat, le, tid, e, active, geoE);
+  __syncthreads();
+  element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+  __syncthreads();
+  if (!active) return;
+  const real* lb0 = s.mat + NP;
+  const real* lb1 = lb0 + P;
+  for (int t = tid; t < FT; t += NP) {
+    const int sd_ = t / P, kk = t % P;
+    const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+    real* gp = a.GT + ((size_t(e) * 4 + sd_) * P + kk) * 8;
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gp[d * 4 + k] = trace_of(s, s.dQ[d], k, le, sd_, kk, lbv);
+  }
+}
+
+template <int P, int EPB, typename real, bool AFFINE, bool IP>
+__global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
+  constexpr int NP = P * P, FT = 4 * P;
+  constexpr int NW = block_ns(P) / 32;
+  __shared__ NSTiles<P, EPB, real, AFFINE> s;
+  const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
+  const int e = blockIdx.x * EPB + le;
+  const bool active = le < EPB && e < a.n_el;
+  Phys<real> ph;
+  ph.load(a.pc);
+  const real mu = ph.mu;
+  real geoE[5];
+  load_tiles(a, s, flat, le, tid, e, active, geoE);
+  __syncthreads();
+  element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+  const int i = tid % P, j = tid / P;
+  const real* hatD = s.mat;
+  const real* lb0 = s.mat + NP;
+  const real* lb1 = lb0 + P;
+  const real* lbw0 = lb1 + P;
+  const real* lbw1 = lbw0 + P;
+  const real* dlbw0 = lbw1 + P + NP;
+  const real* dlbw1 = dlbw0 + P;
+  // volume flux F = Fi - mu Fv at this node, contravariant
+  real Ja00, Ja01, Ja10, Ja11, iJ;
+  if (active) {
+    if constexpr (AFFINE) { Ja00 = geoE[0]; Ja01 = geoE[1]; Ja10 = geoE[2]; Ja11 = geoE[3]; iJ = geoE[4]; }
+    else { Ja00 = s.Ja[0][le][tid]; Ja01 = s.Ja[1][le][tid]; Ja10 = s.Ja[2][le][tid]; Ja11 = s.Ja[3][le][tid]; iJ = geoE[4]; }
+    real q[4], gx[4], gy[4], fi[4], gi[4], fv[4], gv[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { q[k] = s.Q[k][le][tid]; gx[k] = s.dQ[0][k][le][tid]; gy[k] = s.dQ[1][k][le][tid]; }
+    inviscid_flux(ph, q, fi, gi);
+    viscous_flux(ph, q, gx, gy, fv, gv);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const real f = fi[k] - mu * fv[k], g = gi[k] - mu * gv[k];
+      s.Fc[k][le][tid] = f * Ja00 + g * Ja10;
+      s.Gc[k][le][tid] = f * Ja01 + g * Ja11;
+    }
+  }
+  __syncthreads();
+  // face fluxes
+  if (active) {
+    for (int t = tid; t < FT; t += NP) {
+      const int sd_ = t / P, kk = t % P;
+      const int4 sd = a.side[size_t(e) * 4 + sd_];
+      const int kind = sd.y & 15;
+      const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+      real qo[4], gox[4], goy[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+        gox[k] = trace_of(s, s.dQ[0], k, le, sd_, kk, lbv);
+        goy[k] = trace_of(s, s.dQ[1], k, le, sd_, kk, lbv);
+      }
+      const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
+      const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
+      const real invh = real(a.side_invh[size_t(e) * 4 + sd_]);
+      const real penalty = IP ? real(a.sigma0) * mu * real(P - 1) * real(P - 1) * invh : real(0);
+      real F[4], Gx[4] = {real(0), real(0), real(0), real(0)}, Gy[4] = {real(0), real(0), real(0), real(0)};
+      if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
+        const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+        const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+        const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
+        real qn[4], gnx[4], gny[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { qn[k] = tp[k]; gnx[k] = gp[k]; gny[k] = gp[4 + k]; }
+        const bool right = kind == SIDE_RIGHT;
+        const real* QL = right ? qn : qo;
+        const real* QR = right ? qo : qn;
+        int solver = a.riemann;
+        if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
+        real Fi[4], FLx[4], FLy[4], FRx[4], FRy[4];
+        riemann(solver, ph, QL, QR, nx, ny, Fi);
+        viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
+        viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          real fv = real(0.5) * (mu * FLx[k] + mu * FRx[k]) * nx + real(0.5) * (mu * FLy[k] + mu * FRy[k]) * ny;
+          if (IP) fv = fv - penalty * (QL[k] - QR[k]);
+          F[k] = (Fi[k] - fv) * dS;
+          if (right) F[k] = -F[k];
+        }
+        if (IP && a.grad_faces) {
+          real fgx[4], fgy[4], Ax[4], Ay[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) { fgx[k] = (QL[k] - QR[k]) * nx; fgy[k] = (QL[k] - QR[k]) * ny; }
+          viscous_flux(ph, right ? QR : QL, fgx, fgy, Ax, Ay);
+          const real cf = (right ? real(-0.5) : real(0.5)) * real(a.epsilon) * mu;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) { Gx[k] = cf * Ax[k] * dS; Gy[k] = cf * Ay[k] * dS; }
+        }
+      } else {
+        const Zone& z = a.zones[sd.z];
+        real uB[4], uSB[4];
+        const int vbc = bc_states(ph, z, qo, nx, ny, uB, uSB);
+        real Fi[4];
+        if (kind == SIDE_WALL) {
+          euler_wall_flux(ph, qo, nx, ny, dS, Fi);
+        } else {
+          const int solver = z.riemann >= 0 ? z.riemann : a.riemann;
+          riemann(solver, ph, qo, uB, nx, ny, Fi);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) Fi[k] = Fi[k] * dS;
+        }
+        real fv[4] = {real(0), real(0), real(0), real(0)};
+        if (vbc != VBC_NEUMANN) {
+          real Fx[4], Fy[4];
+          if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, gox, goy, Fx, Fy);
+          else viscous_flux(ph, qo, gox, goy, Fx, Fy);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            fv[k] = (mu * Fx[k]) * nx + (mu * Fy[k]) * ny;
+            if (IP) fv[k] = fv[k] - penalty * (qo[k] - uSB[k]);
+            fv[k] = fv[k] * dS;
+          }
+          if (IP && a.grad_faces) {
+            real fgx[4], fgy[4], Ax[4], Ay[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { fgx[k] = (qo[k] - uSB[k]) * nx; fgy[k] = (qo[k] - uSB[k]) * ny; }
+            if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, fgx, fgy, Ax, Ay);
+            else viscous_flux(ph, qo, fgx, fgy, Ax, Ay);
+            const real cf = real(a.epsilon) * mu;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { Gx[k] = (cf * Ax[k]) * dS; Gy[k] = (cf * Ay[k]) * dS; }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) F[k] = Fi[k] - fv[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];
+      if (IP && a.grad_faces) {
+        // metrics at the face node (interpolated along the other direction) and contravariant G
+        real fJa00, fJa01, fJa10, fJa11, fJ;
+        if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+        else {
+          fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
+          fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
+          fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
+          fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
+          fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          s.face[4 + k][le][t] = (Gx[k] * fJa00 + Gy[k] * fJa10) / fJ;
+          s.face[8 + k][le][t] = (Gx[k] * fJa01 + Gy[k] * fJa11) / fJ;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  real qd[4] = {real(0), real(0), real(0), real(0)};
+  if (active) {
+#pragma unroll
+    for (int l = 0; l < P; ++l) {
+      const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s.Fc[k][le][j * P + l] + hj * s.Gc[k][le][l * P + i];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      qd[k] = qd[k] - s.face[k][le][0 * P + i] * lbw0[j];
+      qd[k] = qd[k] - s.face[k][le][1 * P + j] * lbw1[i];
+      qd[k] = qd[k] - s.face[k][le][2 * P + i] * lbw1[j];
+      qd[k] = qd[k] - s.face[k][le][3 * P + j] * lbw0[i];
+    }
+    if (IP && a.grad_faces) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        real dFb = real(0), dGr = real(0), dFt = real(0), dGl = real(0);
+#pragma unroll
+        for (int l = 0; l < P; ++l) {
+          dFb += hatD[i * P + l] * s.face[4 + k][le][0 * P + l];
+          dGr += hatD[j * P + l] * s.face[8 + k][le][1 * P + l];
+          dFt += hatD[i * P + l] * s.face[4 + k][le][2 * P + l];
+          dGl += hatD[j * P + l] * s.face[8 + k][le][3 * P + l];
+        }
+        qd[k] = qd[k] - (dFb * lbw0[j] + s.face[8 + k][le][0 * P + i] * dlbw0[j]);
+        qd[k] = qd[k] - (s.face[4 + k][le][1 * P + j] * dlbw1[i] + dGr * lbw1[i]);
+        qd[k] = qd[k] - (dFt * lbw1[j] + s.face[8 + k][le][2 * P + i] * dlbw1[j]);
+        qd[k] = qd[k] - (s.face[4 + k][le][3 * P + j] * dlbw0[i] + dGl * lbw0[i]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) qd[k] = qd[k] * iJ;
+    const size_t off = (size_t(e) * NP + tid) * 4;
+    if (a.QDot) {
+      double2* dp = reinterpret_cast<double2*>(a.QDot + off);
+      dp[0] = make_double2(double(qd[0]), double(qd[1]));
+      dp[1] = make_double2(double(qd[2]), double(qd[3]));
+    }
+    if (a.update) {
+      real gn[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) gn[k] = a.first ? real(a.b) * qd[k] : real(a.a) * a.G[off + k] + real(a.b) * qd[k];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) a.G[off + k] = gn[k];
+      double2* qp = reinterpret_cast<double2*>(a.Q + off);
+      double2 q01 = qp[0], q23 = qp[1];
+      q01.x = q01.x + a.c * double(gn[0]);
+      q01.y = q01.y + a.c * double(gn[1]);
+      q23.x = q23.x + a.c * double(gn[2]);
+      q23.y = q23.y + a.c * double(gn[3]);
+      qp[0] = q01; qp[1] = q23;
+      s.Q[0][le][tid] = real(q01.x); s.Q[1][le][tid] = real(q01.y);
+      s.Q[2][le][tid] = real(q23.x); s.Q[3][le][tid] = real(q23.y);
+    }
+  }
+  if (a.resid) {
+    double m[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) m[k] = active ? fabs(double(qd[k])) : 0.0;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) m[k] = nanmax(m[k], __shfl_xor_sync(0xffffffffu, m[k], off));
+    if ((flat & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s.red[flat >> 5][k] = m[k];
+  }
+  __syncthreads();
+  if (a.resid && flat < 4) {
+    double mx = 0.0;
+    for (int w = 0; w < NW; ++w) mx = nanmax(mx, s.red[w][flat]);
+    a.resid[size_t(blockIdx.x) * 4 + flat] = mx;
+  }
+  if (active && a.update) {
+    for (int t = tid; t < FT; t += NP) {
+      const int sd_ = t / P, kk = t % P;
+      const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+      real* tp = a.T_out + ((size_t(e) * 4 + sd_) * P + kk) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tp[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+    }
+  }
+}
+
+}  // namespace hg

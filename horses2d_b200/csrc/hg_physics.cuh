@@ -19,19 +19,21 @@ enum { RIEMANN_ROE = 0, RIEMANN_HLL = 1, RIEMANN_EXACT = 2, RIEMANN_LXF = 3 };
 
 struct PhysConst {
   double gamma, gm1, cp, cv, invSqrtGammaMach;
+  double mu, cpPr, lambda;   // dimensionless viscosity, cp/Pr, second viscosity (-2/3)
 };
 
 template <typename real>
 struct Phys {
-  real gamma, gm1, cp, cv, isgm;
+  real gamma, gm1, cp, cv, isgm, mu, cpPr, lambda;
   __device__ __forceinline__ void load(const PhysConst& c) {
     gamma = real(c.gamma); gm1 = real(c.gm1); cp = real(c.cp); cv = real(c.cv); isgm = real(c.invSqrtGammaMach);
+    mu = real(c.mu); cpPr = real(c.cpPr); lambda = real(c.lambda);
   }
 };
 
-template <typename real> __device__ __forceinline__ real rsqrt_(real x);
-template <> __device__ __forceinline__ double rsqrt_(double x) { return sqrt(x); }
-template <> __device__ __forceinline__ float rsqrt_(float x) { return sqrtf(x); }
+template <typename real> __device__ __forceinline__ real sqrt_r(real x);
+template <> __device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+template <> __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
 
 template <typename real>
 __device__ __forceinline__ void inviscid_flux(const Phys<real>& ph, const real* u, real* f, real* g) {
@@ -60,11 +62,11 @@ __device__ __forceinline__ void rotate_back_scale(const Phys<real>& ph, real* F,
 
 template <typename real>
 __device__ __forceinline__ void roe(const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny, real* F) {
-  const real rhoL = qL[0], invRhoL = real(1) / rhoL, sqrtRhoL = rsqrt_(rhoL);
+  const real rhoL = qL[0], invRhoL = real(1) / rhoL, sqrtRhoL = sqrt_r(rhoL);
   const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
   const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
   const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
-  const real rhoR = qR[0], invRhoR = real(1) / rhoR, sqrtRhoR = rsqrt_(rhoR);
+  const real rhoR = qR[0], invRhoR = real(1) / rhoR, sqrtRhoR = sqrt_r(rhoR);
   const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
   const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
   const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
@@ -72,7 +74,7 @@ __device__ __forceinline__ void roe(const Phys<real>& ph, const real* qL, const 
   const real u = (sqrtRhoL * uL + sqrtRhoR * uR) * invrho;
   const real v = (sqrtRhoL * vL + sqrtRhoR * vR) * invrho;
   const real H = (sqrtRhoL * HL + sqrtRhoR * HR) * invrho;
-  const real a = rsqrt_(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
+  const real a = sqrt_r(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
   const real dq0 = rhoR - rhoL, dq1 = rhoR * uR - rhoL * uL, dq2 = rhoR * vR - rhoL * vL, dq3 = qR[3] - qL[3];
   const real al2 = dq2 - v * dq0;
   const real al1 = ph.gm1 * (dq0 * (H - u * u) + u * dq1 - dq3 + (dq2 - v * dq0) * v) / (a * a);
@@ -103,18 +105,18 @@ __device__ __forceinline__ void hll(const Phys<real>& ph, const real* qL, const 
   const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
   const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
   const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
-  const real aL = rsqrt_(ph.gamma * pL * invRhoL), rhoeL = qL[3];
+  const real aL = sqrt_r(ph.gamma * pL * invRhoL), rhoeL = qL[3];
   const real rhoR = qR[0], invRhoR = real(1) / rhoR;
   const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
   const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
   const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
-  const real aR = rsqrt_(ph.gamma * pR * invRhoR), rhoeR = qR[3];
-  const real sqrtRhoL = rsqrt_(rhoL), sqrtRhoR = rsqrt_(rhoR);
+  const real aR = sqrt_r(ph.gamma * pR * invRhoR), rhoeR = qR[3];
+  const real sqrtRhoL = sqrt_r(rhoL), sqrtRhoR = sqrt_r(rhoR);
   const real invrho = real(1) / (sqrtRhoL + sqrtRhoR);
   const real u = (sqrtRhoL * uL + sqrtRhoR * uR) * invrho;
   const real v = (sqrtRhoL * vL + sqrtRhoR * vR) * invrho;
   const real H = (sqrtRhoL * HL + sqrtRhoR * HR) * invrho;
-  const real a = rsqrt_(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
+  const real a = sqrt_r(ph.gm1 * (H - real(0.5) * (u * u + v * v)));
   const real SL = fmin(uL - aL, u - a), SR = fmax(uR + aR, u + a);
   if (SL >= real(0)) flux_normal(rhoL, uL, vL, pL, HL, F);
   else if (SR <= real(0)) flux_normal(rhoR, uR, vR, pR, HR, F);
@@ -134,12 +136,12 @@ __device__ __forceinline__ void lxf(const Phys<real>& ph, const real* qL, const 
   const real uL = (qL[1] * nx + qL[2] * ny) * invRhoL, vL = (-qL[1] * ny + qL[2] * nx) * invRhoL;
   const real pL = ph.gm1 * (qL[3] - real(0.5) * rhoL * (uL * uL + vL * vL));
   const real HL = ph.cp * pL * invRhoL + real(0.5) * (uL * uL + vL * vL);
-  const real aL = rsqrt_(ph.gamma * pL * invRhoL);
+  const real aL = sqrt_r(ph.gamma * pL * invRhoL);
   const real rhoR = qR[0], invRhoR = real(1) / rhoR;
   const real uR = (qR[1] * nx + qR[2] * ny) * invRhoR, vR = (-qR[1] * ny + qR[2] * nx) * invRhoR;
   const real pR = ph.gm1 * (qR[3] - real(0.5) * rhoR * (uR * uR + vR * vR));
   const real HR = ph.cp * pR * invRhoR + real(0.5) * (uR * uR + vR * vR);
-  const real aR = rsqrt_(ph.gamma * pR * invRhoR);
+  const real aR = sqrt_r(ph.gamma * pR * invRhoR);
   const real lam = fmax(fabs(uL) + aL, fabs(uR) + aR);
   real FL[4], FR[4];
   flux_normal(rhoL, uL, vL, pL, HL, FL);
@@ -169,6 +171,44 @@ __device__ __forceinline__ void euler_wall_flux(const Phys<real>& ph, const real
   inviscid_flux(ph, q, f, g);
 #pragma unroll
   for (int k = 0; k < 4; ++k) F[k] = f[k] * nx * dS + g[k] * ny * dS;
+}
+
+// viscousFlux (Physics/ViscousFluxes.f90:39-164): Fx, Fy from q and its gradient (dqx, dqy)
+template <typename real>
+__device__ __forceinline__ void viscous_flux(const Phys<real>& ph, const real* q, const real* dqx, const real* dqy,
+                                             real* Fx, real* Fy) {
+  const real invRho = real(1) / q[0];
+  const real u = q[1] * invRho, v = q[2] * invRho;
+  const real uDivRho = u * invRho, vDivRho = v * invRho;
+  const real divV = -uDivRho * dqx[0] + invRho * dqx[1] - vDivRho * dqy[0] + invRho * dqy[2];
+  const real dxT = ph.gm1 * invRho * (-q[3] * invRho * dqx[0] + dqx[3] + u * (u * dqx[0] - dqx[1]) + v * (v * dqx[0] - dqx[2]));
+  const real dyT = ph.gm1 * invRho * (-q[3] * invRho * dqy[0] + dqy[3] + u * (u * dqy[0] - dqy[1]) + v * (v * dqy[0] - dqy[2]));
+  Fx[0] = real(0);
+  Fx[1] = real(2) * (-uDivRho * dqx[0] + invRho * dqx[1]) + ph.lambda * divV;
+  Fx[2] = -vDivRho * dqx[0] - uDivRho * dqy[0] + invRho * dqy[1] + invRho * dqx[2];
+  Fx[3] = u * Fx[1] + v * Fx[2] + ph.cpPr * dxT;
+  Fy[0] = real(0);
+  Fy[1] = Fx[2];
+  Fy[2] = real(2) * (-vDivRho * dqy[0] + invRho * dqy[2]) + ph.lambda * divV;
+  Fy[3] = u * Fy[1] + v * Fy[2] + ph.cpPr * dyT;
+}
+
+// AdiabaticViscousFlux1D/2D (ViscousFluxes.f90:230-330): no heat flux, work term with qB's velocity
+template <typename real>
+__device__ __forceinline__ void viscous_flux_adiabatic(const Phys<real>& ph, const real* q, const real* qB,
+                                                       const real* dqx, const real* dqy, real* Fx, real* Fy) {
+  const real invRho = real(1) / q[0];
+  const real u = q[1] * invRho, v = q[2] * invRho;
+  const real uDivRho = u * invRho, vDivRho = v * invRho;
+  const real divV = -uDivRho * dqx[0] + invRho * dqx[1] - vDivRho * dqy[0] + invRho * dqy[2];
+  Fx[0] = real(0);
+  Fx[1] = real(2) * (-uDivRho * dqx[0] + invRho * dqx[1]) + ph.lambda * divV;
+  Fx[2] = -vDivRho * dqx[0] - uDivRho * dqy[0] + invRho * dqy[1] + invRho * dqx[2];
+  Fx[3] = (qB[1] * Fx[1] + qB[2] * Fx[2]) / qB[0];
+  Fy[0] = real(0);
+  Fy[1] = Fx[2];
+  Fy[2] = real(2) * (-vDivRho * dqy[0] + invRho * dqy[2]) + ph.lambda * divV;
+  Fy[3] = (qB[1] * Fy[1] + qB[2] * Fy[2]) / qB[0];
 }
 
 }  // namespace hg

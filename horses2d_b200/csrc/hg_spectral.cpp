@@ -122,6 +122,14 @@ NodalOps make_nodal_ops(int N, int node_type) {
   o.lb1 = lagrange_basis(o, 1.0);
   o.lbw0.resize(P); o.lbw1.resize(P);
   for (int i = 0; i < P; ++i) { o.lbw0[i] = o.lb0[i] / o.w[i]; o.lbw1[i] = o.lb1[i] / o.w[i]; }
+  // dlb = D^T lb (derivative of the boundary interpolant), dlbw = dlb / w
+  o.dlbw0.assign(P, 0.0); o.dlbw1.assign(P, 0.0);
+  for (int i = 0; i < P; ++i) {
+    double s0 = 0.0, s1 = 0.0;
+    for (int j = 0; j < P; ++j) { s0 += o.D[j * P + i] * o.lb0[j]; s1 += o.D[j * P + i] * o.lb1[j]; }
+    o.dlbw0[i] = s0 / o.w[i];
+    o.dlbw1[i] = s1 / o.w[i];
+  }
   return o;
 }
 

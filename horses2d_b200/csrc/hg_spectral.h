@@ -14,7 +14,7 @@ namespace hg {
 
 struct NodalOps {
   int N = 0, P = 0;
-  std::vector<double> xi, w, wb, D, hatD, lb0, lb1, lbw0, lbw1;
+  std::vector<double> xi, w, wb, D, hatD, lb0, lb1, lbw0, lbw1, dlbw0, dlbw1;
 };
 
 NodalOps make_nodal_ops(int N, int node_type);   // node_type: 1 LG, 2 LGL

@@ -26,17 +26,13 @@
 // touches consecutive words.
 #pragma once
 #include "hg_physics.cuh"
+#include "hg_bc.cuh"
 
 namespace hg {
 
 // side kinds
 enum { SIDE_LEFT = 0, SIDE_RIGHT = 1, SIDE_STATE = 2, SIDE_WALL = 3 };
 constexpr int SIDE_REVERSED = 16;
-
-struct Zone {
-  int type, riemann;
-  double q[4];
-};
 
 template <typename real>
 struct StageArgs {
@@ -139,8 +135,8 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
         int solver = a.riemann;
         if (kind == SIDE_STATE) {
           const Zone& z = a.zones[sd.z];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) qn[k] = real(z.q[k]);
+          real us[4];
+          bc_states(ph, z, qo, nx, ny, qn, us);
           if (z.riemann >= 0) solver = z.riemann;
         } else {
           const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;

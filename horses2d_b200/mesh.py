@@ -102,6 +102,215 @@ def box_descriptor(nx, ny, x0, x1, y0, y1, N, node_type, *, elem_offset=0, edge_
                 edge_invh=np.full(F, 0.0))
 
 
+def _same(a, b):
+    """Spectral_Auxiliars almostEqual: |a-b| <= 2 eps max(|a|,|b|) (absolute 2 eps at zero)."""
+    eps = np.finfo(float).eps
+    if a == 0.0 or b == 0.0:
+        return abs(a - b) <= 2.0 * eps
+    return abs(b - a) <= 2.0 * eps * max(abs(a), abs(b))
+
+
+def _bary(x):
+    w = np.ones_like(x)
+    for j in range(len(x)):
+        for k in range(len(x)):
+            if k != j:
+                w[j] *= x[j] - x[k]
+    return 1.0 / w
+
+
+def _interp(old, new):
+    """Barycentric interpolation matrix T[new, old] (exact rows where nodes coincide)."""
+    wb = _bary(old)
+    T = np.zeros((len(new), len(old)))
+    for k, x in enumerate(new):
+        d = x - old
+        hit = np.abs(d) <= 2.0 * np.finfo(float).eps * np.maximum(np.abs(x), np.abs(old))
+        if np.any(hit):
+            T[k, np.argmax(hit)] = 1.0
+        else:
+            t = wb / d
+            T[k] = t / t.sum()
+    return T
+
+
+def build_descriptor(m, N, node_type, *, reynolds_length=1.0, periodic_pairs=()):
+    """Constructed-mesh descriptor (include/horses_gpu.h hg_mesh_desc) from .HiOMesh arrays.
+
+    Conforming meshes with one polynomial order.  Restates the reference's
+    construction (Mesh/MeshFile.f90 computeFaces / computeElementOfEdges,
+    Mesh/QuadMesh_Construct.incf, Mesh/QuadElement_EdgeMappings.incf,
+    Mesh/QuadElement_EdgeProcedures.incf Edge_LinkWithElements / Edge_Invert,
+    Mesh/QuadElement_QuadMappings.incf QuadElement_SetMappings) with hash-based
+    connectivity:
+      * edges numbered by first appearance over elements and their faces
+        (p1p2, p2p3, p3p4, p4p1); LEFT = first owner, RIGHT = second;
+      * curved edges re-interpolated from their Chebyshev-Gauss-Lobatto samples at
+        order N/2 (interior) or N (boundary), then at the edge nodes;
+      * normals and dS per edge node, outward from LEFT, in LEFT's local order;
+        ``inverse`` when RIGHT runs the other way;
+      * transfinite element mappings, Ja = [[y_eta, -y_xi], [-x_eta, x_xi]].
+    ``periodic_pairs``: [(marker_a, marker_b, coord)] boundary zones linked as the
+    reference's Zone_LinkPeriodicZones does (coord 0: match x, 1: match y).
+    """
+    from ._lib import nodes as lib_nodes
+    P = N + 1
+    xi, w = lib_nodes(N, node_type)
+    D = np.zeros((P, P))
+    wb = _bary(xi)
+    for i in range(P):
+        for j in range(P):
+            if j != i:
+                D[i, j] = wb[j] / (wb[i] * (xi[i] - xi[j]))
+        D[i, i] = -D[i].sum() + D[i, i]
+    X = np.asarray(m["points"], float) / reynolds_length
+    quads = np.asarray(m["quads"], np.int64) - 1
+    E = quads.shape[0]
+    # ---- connectivity
+    edge_of, enodes, left, lside, right, rside = {}, [], [], [], [], []
+    for e in range(E):
+        for f in range(4):
+            a, b = quads[e, f], quads[e, (f + 1) % 4]
+            key = (min(a, b), max(a, b))
+            if key not in edge_of:
+                edge_of[key] = len(enodes)
+                enodes.append((a, b))
+                left.append(e); lside.append(f + 1); right.append(-1); rside.append(0)
+            else:
+                k = edge_of[key]
+                if right[k] != -1:
+                    raise ValueError("edge shared by more than two elements (non-conforming mesh)")
+                right[k] = e; rside[k] = f + 1
+    F = len(enodes)
+    marker = np.zeros(F, np.int32)
+    for (a, b), mk in zip(np.asarray(m["bdry_edges"], np.int64) - 1, np.asarray(m["bdry_marker"])):
+        marker[edge_of[(min(a, b), max(a, b))]] = mk
+    for k in range(F):
+        if (right[k] < 0) != (marker[k] != 0):
+            raise ValueError("boundary edges and element connectivity disagree (hanging nodes are not supported)")
+    curve = {}
+    if "curved_edges" in m and len(m["curved_edges"]):
+        ce = np.asarray(m["curved_edges"], np.int64) - 1
+        for c, (a, b) in enumerate(ce):
+            k = edge_of[(min(a, b), max(a, b))]
+            if k in curve:
+                continue
+            cx = np.asarray(m["curve_x"][c], float) / reynolds_length
+            cy = np.asarray(m["curve_y"][c], float) / reynolds_length
+            if (a, b) != tuple(enodes[k]):
+                cx, cy = cx[::-1], cy[::-1]
+            curve[k] = (cx, cy)
+    # ---- edge geometry in stored order, then oriented to LEFT
+    eX = np.zeros((F, P, 2)); edX = np.zeros((F, P, 2)); en = np.zeros((F, P, 2)); edS = np.zeros((F, P))
+    straight = np.ones(F, bool)
+    for k, (a, b) in enumerate(enodes):
+        if k in curve:
+            straight[k] = False
+            cx, cy = curve[k]
+            order = len(cx) - 1
+            nc = N if marker[k] != 0 else (N // 2 if N > 1 else N)
+            cgl = 0.5 + 0.5 * np.cos(np.pi * (order - np.arange(order + 1)) / order)
+            cgli = 0.5 + 0.5 * np.cos(np.pi * (nc - np.arange(nc + 1)) / nc)
+            T1 = _interp(cgl, cgli)
+            T2 = _interp(cgli, xi)
+            pts = T2 @ (T1 @ np.stack([cx, cy], 1))
+            dX = D @ pts
+            eX[k], edX[k] = pts, dX
+            edS[k] = np.sqrt((dX ** 2).sum(1))
+            en[k] = np.stack([dX[:, 1], -dX[:, 0]], 1) / edS[k][:, None]
+        else:
+            na, nb = X[a], X[b]
+            eX[k] = na[None] * (1.0 - xi)[:, None] + nb[None] * xi[:, None]
+            d = nb - na
+            edX[k] = d
+            L = np.sqrt(d[1] ** 2 + d[0] ** 2)
+            edS[k] = L
+            en[k] = np.array([d[1], -d[0]]) / L
+    nodes_lp = [tuple(enodes[k]) for k in range(F)]
+    for k in range(F):                         # LEFT side TOP/LEFT runs against the local coordinate
+        if lside[k] in (3, 4):
+            eX[k] = eX[k][::-1]; edX[k] = -edX[k][::-1]; edS[k] = edS[k][::-1]; en[k] = en[k][::-1]
+            nodes_lp[k] = nodes_lp[k][::-1]
+    inverse = np.zeros(F, np.int32)
+    for k in range(F):
+        if right[k] >= 0:
+            e, s = right[k], rside[k] - 1
+            p0, p1 = quads[e, s], quads[e, (s + 1) % 4]
+            rp = (p0, p1) if s in (0, 1) else (p1, p0)
+            inverse[k] = int(rp != nodes_lp[k])
+    # ---- periodic partners (Zone_LinkPeriodicZones)
+    partner = np.full(F, -1, np.int32)
+    for ma, mb, coord in periodic_pairs:
+        ea = [k for k in range(F) if marker[k] == ma]
+        eb = [k for k in range(F) if marker[k] == mb]
+        used = set()
+        for k1 in ea:
+            a1, b1 = X[nodes_lp[k1][0], coord], X[nodes_lp[k1][1], coord]
+            for k2 in eb:
+                if k2 in used:
+                    continue
+                a2, b2 = X[nodes_lp[k2][0], coord], X[nodes_lp[k2][1], coord]
+                if (_same(a1, a2) and _same(b1, b2)) or (_same(a1, b2) and _same(b1, a2)):
+                    used.add(k2)
+                    partner[k1], partner[k2] = k2, k1
+                    inv = int(np.dot(edX[k1][0], edX[k2][0]) < 0.0)
+                    inverse[k1] = inverse[k2] = inv
+                    break
+    # ---- element mappings (transfinite)
+    elem_edges = {}
+    for k in range(F):
+        elem_edges[(left[k], lside[k])] = (k, 1)
+        if right[k] >= 0:
+            elem_edges[(right[k], rside[k])] = (k, -1 if inverse[k] else 1)
+    Ja = np.zeros((E, P, P, 4)); jac = np.zeros((E, P, P)); xn = np.zeros((E, P, P, 2))
+    XI, ETA = np.meshgrid(xi, xi)            # [j][i]
+    for e in range(E):
+        Xe = np.zeros((4, P, P, 2)); dXe = np.zeros((4, P, P, 2))
+        for side in range(1, 5):
+            k, dr = elem_edges[(e, side)]
+            cx = xi if dr == 1 else 1.0 - xi
+            if marker[k] != 0:
+                idx = np.arange(P) if dr == 1 else np.arange(P)[::-1]
+                Xs, dXs = eX[k][idx], dr * (edX[k][idx] if not straight[k] else np.tile(edX[k][0], (P, 1)))
+            elif straight[k]:
+                na, nb = X[nodes_lp[k][0]], X[nodes_lp[k][1]]
+                Xs = na[None] * (1.0 - cx)[:, None] + nb[None] * cx[:, None]
+                dXs = np.tile(dr * (nb - na), (P, 1))
+            else:
+                T = _interp(xi, cx)
+                Xs, dXs = T @ eX[k], dr * (T @ edX[k])
+            if side in (1, 3):                    # along xi: value depends on i
+                Xe[side - 1] = Xs[None, :, :].repeat(P, 0)
+                dXe[side - 1] = dXs[None, :, :].repeat(P, 0)
+            else:                                 # along eta: value depends on j
+                Xe[side - 1] = Xs[:, None, :].repeat(P, 1)
+                dXe[side - 1] = dXs[:, None, :].repeat(P, 1)
+        n1, n2, n3, n4 = (X[quads[e, q]] for q in range(4))
+        x_, y_ = XI[..., None], ETA[..., None]
+        Xm = ((1 - y_) * Xe[0] + x_ * Xe[1] + y_ * Xe[2] + (1 - x_) * Xe[3]
+              - n1 * (1 - x_) * (1 - y_) - n2 * x_ * (1 - y_) - n3 * x_ * y_ - n4 * (1 - x_) * y_)
+        dxi = ((1 - y_) * dXe[0] + Xe[1] + y_ * dXe[2] - Xe[3] + n1 * (1 - y_) - n2 * (1 - y_) - n3 * y_ + n4 * y_)
+        deta = (-Xe[0] + x_ * dXe[1] + Xe[2] + (1 - x_) * dXe[3] + n1 * (1 - x_) + n2 * x_ - n3 * x_ - n4 * (1 - x_))
+        jac[e] = dxi[..., 0] * deta[..., 1] - deta[..., 0] * dxi[..., 1]
+        Ja[e, ..., 0] = deta[..., 1]
+        Ja[e, ..., 1] = -dxi[..., 1]
+        Ja[e, ..., 2] = -deta[..., 0]
+        Ja[e, ..., 3] = dxi[..., 0]
+        xn[e] = Xm
+    vol = np.einsum("eji,j,i->e", jac, w, w)
+    area = (edS * w[None, :]).sum(1)
+    invh = np.zeros(F)
+    for k in range(F):
+        vmin = vol[left[k]] if right[k] < 0 else min(vol[left[k]], vol[right[k]])
+        invh[k] = area[k] / vmin
+    return dict(N=np.full(E, N, np.int32), Ja=Ja.reshape(-1), jac=jac.reshape(-1), x=xn.reshape(-1),
+                volume=vol, vertices=X[quads].reshape(-1),
+                edge_elem=np.stack([left, right], 1).reshape(-1).astype(np.int32),
+                edge_side=np.stack([lside, rside], 1).reshape(-1).astype(np.int32),
+                edge_inverse=inverse, edge_marker=marker, edge_n=en.reshape(-1), edge_dS=edS.reshape(-1),
+                periodic_partner=partner, edge_invh=invh)
+
+
 def concat_descriptors(descs):
     """Pack independent meshes into one element list (disjoint union, ensemble runs)."""
     out = {}

@@ -39,8 +39,8 @@ class GpuDGSEM:
     """One mesh + physics + resident state on the GPU."""
 
     def __init__(self, mesh, *, mach, node_type=L.NODES_LGL, riemann=L.ROE, bcs=(), precision=L.PREC_FP64,
-                 reynolds=0.0, prandtl=0.72, navier_stokes=0, viscous=0, pressure_ref=101325.0,
-                 temperature_ref=273.15, reynolds_length=1.0, gamma=1.4):
+                 reynolds=0.0, prandtl=0.72, navier_stokes=0, viscous=L.BR1, ip_method=L.SIPG, sigma0_ip=1.0,
+                 pressure_ref=101325.0, temperature_ref=273.15, reynolds_length=1.0, gamma=1.4):
         lib = L.load()
         self._keep = []
         md = L.MeshDesc()
@@ -72,8 +72,8 @@ class GpuDGSEM:
         put("periodic_partner", "periodic_partner", np.int32, C.c_int32, True)
         put("edge_invh", "edge_invh", np.float64, C.c_double, True)
         ph = L.PhysicsDesc(node_type=node_type, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous,
-                           mach=mach, reynolds=reynolds, prandtl=prandtl, pressure_ref=pressure_ref,
-                           temperature_ref=temperature_ref, reynolds_length=reynolds_length, gamma=gamma,
+                           ip_method=ip_method, sigma0_ip=sigma0_ip, mach=mach, reynolds=reynolds,
+                           prandtl=prandtl, pressure_ref=pressure_ref, temperature_ref=temperature_ref, reynolds_length=reynolds_length, gamma=gamma,
                            gas_R=287.15)
         barr = (L.BCDesc * max(1, len(bcs)))()
         for k, b in enumerate(bcs):
@@ -83,6 +83,8 @@ class GpuDGSEM:
             for i in range(4):
                 barr[k].state[i] = st[i]
             barr[k].wall_T = b.get("wall_T", 1.0)
+            wv = b.get("wall_v", (0.0, 0.0))
+            barr[k].wall_v[0], barr[k].wall_v[1] = wv[0], wv[1]
             barr[k].wall_type = b.get("wall_type", 2)
             barr[k].outflow_type = b.get("outflow_type", 1)
         self._keep.append(barr)

@@ -48,6 +48,8 @@ typedef struct {
   int32_t riemann;         /* interior inviscid Riemann solver */
   int32_t navier_stokes;   /* 0: Euler build, 1: Navier-Stokes build */
   int32_t viscous;         /* 0: BR1, 1: interior penalty */
+  int32_t ip_method;       /* interior penalty: 0 SIPG, 1 NIPG, 2 IIPG (DGViscousMethods.f90:355-380) */
+  double  sigma0_ip;       /* "Jumps penalty parameter" */
   double  mach, reynolds, prandtl;
   double  pressure_ref, temperature_ref, reynolds_length;
   double  gamma;           /* 1.4 for the reference's "Air" */
@@ -61,10 +63,11 @@ typedef struct {
 typedef struct {
   int32_t type;            /* HG_BC_* */
   int32_t riemann;         /* zone Riemann solver, HG_RIEMANN_INTERIOR = interior one */
-  double  state[4];
-  double  wall_T;          /* viscous wall temperature (dimensionless), isothermal walls */
+  double  state[4];        /* Dirichlet / Farfield / Pressure-outlet state */
+  double  wall_T;          /* viscous wall temperature / reference temperature (isothermal walls) */
+  double  wall_v[2];       /* viscous wall velocity, dimensionless: sqrt(gamma) * Mach * direction */
   int32_t wall_type;       /* 1 isothermal, 2 adiabatic */
-  int32_t outflow_type;
+  int32_t outflow_type;    /* pressure outlet: 1 reflective, 2 partially non-reflective (default) */
 } hg_bc_desc;
 
 /* The mesh after the reference's construction (QuadMesh_t after

@@ -406,7 +406,10 @@ static void update_zones(Oracle& o, double t) {
 
 // ---------------------------------------------------------------- traces
 static void interpolate_to_boundaries(Oracle& o, bool gradient) {
-  for (auto& e : o.el) {
+  // each element writes only its own storage slots: element-parallel
+#pragma omp parallel for schedule(static)
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    Element& e = o.el[ei];
     const int P = e.P;
     const Spectral& s = *e.sp;
     const double* Q = gradient ? &o.dQ[2 * e.offset] : &o.Q[e.offset];
@@ -611,7 +614,11 @@ void time_derivative(Oracle& o, double t) {
     compute_gradient(o, vw);
     interpolate_to_boundaries(o, true);
   }
-  for (auto& e : o.el) volume_loop(o, e, vw);
+#pragma omp parallel for schedule(static)
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    ViscousWork w;
+    volume_loop(o, o.el[ei], w);
+  }
   for (auto& f : o.ed) {
     switch (f.kind) {
       case E_STRAIGHT: case E_CURVED: face_interior(o, f, vw); break;
@@ -619,7 +626,9 @@ void time_derivative(Oracle& o, double t) {
       default: face_boundary(o, f, vw); break;
     }
   }
-  for (auto& e : o.el) {
+#pragma omp parallel for schedule(static)
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    Element& e = o.el[ei];
     double* QD = &o.QDot[e.offset];
     for (int q = 0; q < e.P * e.P; ++q)
       for (int k = 0; k < 4; ++k) QD[4 * q + k] = QD[4 * q + k] / e.jac[q];

@@ -563,12 +563,16 @@ static void br1_face(Oracle& o, Edge& f) {
 void compute_gradient(Oracle& o, ViscousWork& vw) {
   (void)vw;
   if (is_ip(o)) {
-    for (auto& e : o.el) interior_gradient(o, e, &o.dQ[2 * e.offset]);
+#pragma omp parallel for schedule(static)
+    for (size_t ei = 0; ei < o.el.size(); ++ei) interior_gradient(o, o.el[ei], &o.dQ[2 * o.el[ei].offset]);
     return;
   }
-  for (auto& e : o.el) vector_volume_green(o, e, &o.dQ[2 * e.offset]);
+#pragma omp parallel for schedule(static)
+  for (size_t ei = 0; ei < o.el.size(); ++ei) vector_volume_green(o, o.el[ei], &o.dQ[2 * o.el[ei].offset]);
   for (auto& f : o.ed) br1_face(o, f);
-  for (auto& e : o.el) {
+#pragma omp parallel for schedule(static)
+  for (size_t ei = 0; ei < o.el.size(); ++ei) {
+    Element& e = o.el[ei];
     double* dQ = &o.dQ[2 * e.offset];
     const int NP = e.P * e.P;
     for (int d = 0; d < 2; ++d)

@@ -55,3 +55,29 @@ def test_library_nodes_match_oracle():
             X = orc.coords()[:N + 1, 0]
             np.testing.assert_allclose(xi, X, rtol=0, atol=1e-15)
             assert abs(w.sum() - 1.0) < 1e-15
+
+
+@pytest.mark.parametrize("case", ["cylinder", "ogrid", "periodic"])
+def test_general_builder_matches_reference_construction(case):
+    """build_descriptor (curved edges, LEFT/RIGHT orientation, periodic pairing) vs the oracle's mesh export."""
+    from cases_util import load_mesh
+    if case == "cylinder":
+        m, N, nodes, pp = load_mesh("CylinderBench"), 5, O.LGL, ()
+        bcs = [dict(type=O.BC_DIRICHLET)] * 4 + [dict(type=O.BC_EULERWALL)]
+    elif case == "ogrid":
+        m, N, nodes, pp = hmesh.ogrid(6, 12, 0.5, 10.0, 1.2), 3, O.LG, ()
+        bcs = [dict(type=O.BC_EULERWALL), dict(type=O.BC_DIRICHLET)]
+    else:
+        m, N, nodes, pp = load_mesh("VortexTransportCase"), 4, O.LGL, [(1, 2, 0), (3, 4, 1)]
+        bcs = hmesh.periodic_bcs_cartesian()
+    ref = O.Oracle(m, N, nodes=nodes, bcs=bcs, mach=0.3).export_mesh()
+    ours = hmesh.build_descriptor(m, N, nodes, periodic_pairs=pp)
+    for k in ("Ja", "jac", "x", "volume", "vertices", "edge_invh"):
+        scale = max(1.0, float(np.max(np.abs(ref[k]))))
+        np.testing.assert_allclose(ours[k], ref[k], rtol=0, atol=1e-13 * scale, err_msg=k)
+    ta, tb = side_table(ours), side_table(ref)
+    for key, va in ta.items():
+        vb = tb[key]
+        assert va[:4] == vb[:4], key
+        np.testing.assert_allclose(va[4], vb[4], atol=1e-13)
+        np.testing.assert_allclose(va[5], vb[5], rtol=1e-13)

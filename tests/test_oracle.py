@@ -7,6 +7,12 @@
   mortars and periodic zones, Legendre-Gauss nodes and the Roe flux (the case
   file's "Inviscid Riemann Flux" key is not the one Setup.f90:280 reads, so the
   default Roe applies).
+* Couette benchmark (TestCases/Benchmark/Simulations/Couette): Navier-Stokes
+  with BR1, isothermal walls (one moving), a Dirichlet zone fed by the
+  plugin's boundary-condition function and a partially non-reflective
+  pressure outlet, on a p-refined (N = 5/7/10/7) curved mesh with mortars.
+  The reference asserts iteration 19585 of the steady RK5 run (CFL 0.4,
+  residual 1e-4) and the four final residuals to 1e-12.
 * Spectral building blocks: exactness of the nodal derivative and quadrature.
 * Free-stream preservation on curved meshes, conservation on periodic meshes.
 """
@@ -106,3 +112,48 @@ def test_rk3_matches_explicit_formula():
         G = k if m == 0 else am[m] * G + k
         Q = Q + gm[m] * dt * G
     assert rel_l2(Q_rk, Q) < 1e-15
+
+
+def couette_state(x, y, ref):
+    """Couette profile of the Couette plugin's initial and boundary-condition functions (dimensional)."""
+    R = 287.15
+    cp, cv = R * 3.5, R * 2.5
+    T = ref["T"] - ref["V"] ** 2 * 0.72 / (8.0 * cp) * (y + 1.0) * (y - 1.0)
+    rho = 101325.0 / (R * T)
+    rhou = rho * ref["V"] * 0.5 * (y + 1.0)
+    return np.stack([rho, rhou, 0.0 * y, cv * rho * T + 0.5 * rhou * rhou / rho], 1)
+
+
+def test_couette_benchmark_golden():
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["Couette"]
+    m = load_mesh("CouetteBench")
+    porder = np.array([5, 7, 10, 7])[m["p_zones"]]
+    bcs = [dict(type=O.BC_VISCOUSWALL, wall_type=1),
+           dict(type=O.BC_VISCOUSWALL, wall_type=1, wall_v=(np.sqrt(1.4) * 0.8, 0.0)),
+           dict(type=O.BC_DIRICHLET),
+           dict(type=O.BC_PRESSUREOUTLET, outflow_type=2)]
+    orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.ROE, mach=0.8, reynolds=2000.0, prandtl=0.72,
+                   navier_stokes=1, viscous=O.BR1, bcs=bcs)
+    ref = orc.ref
+    scale = np.array([ref["rho"], ref["rho"] * ref["a"], ref["rho"] * ref["a"], ref["p"]])
+    X = orc.coords()
+    q0 = couette_state(X[:, 0], X[:, 1], ref)
+    q0[X[:, 0] ** 2 + X[:, 1] ** 2 < 0.005, 1] *= 1.005
+    orc.set_state((q0 / scale).ravel())
+    Xb = orc.zone_edge_nodes(3)
+    orc.set_zone_state(3, (couette_state(Xb[:, 0], Xb[:, 1], ref) / scale).ravel())
+    it, _ = orc.integrate(O.RK5, transient=False, t0=0.0, t_end=1.0, max_iter=100000, cfl=0.4, dt_cap=1.0,
+                          residual_target=1e-4)
+    assert it == golden["expected_iter"]
+    assert np.max(np.abs(orc.residuals() - np.array(golden["expectedResiduals"]))) <= 1e-12
+
+
+def test_ns_freestream_preservation_curved():
+    """Uniform flow is a discrete steady state of the NS residual on curved meshes (BR1 and IP)."""
+    m = load_mesh("CylinderBench")
+    for viscous in (O.BR1, O.IP):
+        orc = O.Oracle(m, 4, nodes=O.LG, riemann=O.ROE, mach=0.3, reynolds=100.0, navier_stokes=1, viscous=viscous,
+                       bcs=[dict(type=O.BC_DIRICHLET)] * 5)
+        q = np.array([1.0, 0.3 * np.sqrt(1.4), 0.0, 2.5 + 0.5 * 0.09 * 1.4])
+        orc.set_state(np.tile(q, orc.ndof // 4))
+        assert np.abs(orc.time_derivative(0.0)).max() <= 1e-8
