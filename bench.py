@@ -8,11 +8,20 @@ over the whole workload.  DOF-stage updates/s = NDOF * 3 * K / time, NDOF =
 size(Storage%Q) = 4 x nodes (the reference's DOF count, DGSEM_class.f90:337-340).
 
 Workloads (synthetic inputs with the configurations' shapes; seeds fixed):
+  cylinder : (default) Navier-Stokes past a circular cylinder, Re 100, M 0.2, Pr 0.72,
+             O-grid 64 radial x 128 azimuthal curved quads, r 0.5 -> 30, radial
+             stretching 1.05, N = 5, Legendre-Gauss nodes, BR1, Roe, adiabatic viscous
+             wall, far-field zone; uniform free stream + 1e-3 N(0,1) per DOF (seed
+             20261203); NDOF 1,179,648; CFL 0.05 (the reference's time-step estimate is
+             inviscid only; with the near-wall elements at Re 100, N = 5 the viscous limit
+             makes CFL 0.2 unstable, for the oracle as for the kernels).  FP64 plain; the
+             FP32-bulk path is timed in the same run and its density error after the K
+             steps is reported.
+  vortex16 : the reference-runnable case: 16 x 16 periodic vortex, N = 4, LGL, Roe, FP64.
   ensemble : 512 periodic isentropic-vortex instances on [-5,5]^2, n x n elements with
              n ~ U{8..48}, N ~ U{3..7}, vortex centre ~ U[-2,2]^2, beta ~ U[2,6],
              M 0.5 at 45 deg, LGL nodes, Roe, packed by polynomial order into one
              element list per order; FP32 bulk with FP64 state accumulator by default.
-  vortex16 : the reference-runnable case: 16 x 16 periodic vortex, N = 4, LGL, Roe, FP64.
   box512   : one 512 x 512 periodic vortex box, N = 4, LGL, Roe, FP64 (profiling case).
 Multi-GPU: independent replicas (the workload does not exchange data), weak scaling.
 """
@@ -32,6 +41,7 @@ sys.path.insert(0, ROOT)
 
 SEED = 20261203
 L2_BYTES = 126 * 2 ** 20
+CONFIGS = ("cylinder", "vortex16", "ensemble", "box512")
 
 
 def peaks():
@@ -55,9 +65,34 @@ def ensemble_spec(seed=SEED, n_inst=512):
     return inst
 
 
-def build_buckets(config, precision):
-    """[(descriptor, Q0, N, n_instances)] per polynomial order."""
-    from horses2d_b200 import mesh as hmesh, cases, NODES_LGL
+def cylinder_mesh():
+    from horses2d_b200 import mesh as hmesh
+    return hmesh.ogrid(64, 128, 0.5, 30.0, 1.05)
+
+
+def freestream(mach, gamma=1.4):
+    """Dimensionless uniform state (rho = p = 1, u = sqrt(gamma) M)."""
+    u = np.sqrt(gamma) * mach
+    return np.array([1.0, u, 0.0, 1.0 / (gamma - 1.0) + 0.5 * u * u])
+
+
+def cylinder_state(n_nodes, seed=SEED):
+    rng = np.random.default_rng(seed)
+    return (np.tile(freestream(0.2), n_nodes) + 1e-3 * rng.standard_normal(4 * n_nodes))
+
+
+def build_parts(config):
+    """[(descriptor, Q0, N, n_instances, solver kwargs, cfl)] -- one GPU context each."""
+    from horses2d_b200 import mesh as hmesh, cases
+    import horses2d_b200 as hg
+    if config == "cylinder":
+        N = 5
+        desc = hmesh.build_descriptor(cylinder_mesh(), N, hg.NODES_LG)
+        q = freestream(0.2)
+        kw = dict(mach=0.2, reynolds=100.0, prandtl=0.72, navier_stokes=1, viscous=hg.BR1, node_type=hg.NODES_LG,
+                  riemann=hg.ROE, bcs=[dict(type=hg.BC_VISCOUSWALL, wall_type=2),
+                                       dict(type=hg.BC_FARFIELD, state=q)])
+        return [(desc, cylinder_state(len(desc["N"]) * (N + 1) ** 2), N, 1, kw, 0.05)]
     if config == "vortex16":
         inst = [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
     elif config == "box512":
@@ -66,20 +101,37 @@ def build_buckets(config, precision):
         inst = ensemble_spec()
     else:
         raise SystemExit(f"unknown config {config}")
-    buckets = []
+    kw = dict(mach=0.5, node_type=hg.NODES_LGL, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    parts = []
     for N in sorted({i["N"] for i in inst}):
         descs, qs = [], []
         eo = fo = 0
         for it in (i for i in inst if i["N"] == N):
-            d = hmesh.box_descriptor(it["n"], it["n"], -5.0, 5.0, -5.0, 5.0, N, NODES_LGL, elem_offset=eo, edge_offset=fo)
+            d = hmesh.box_descriptor(it["n"], it["n"], -5.0, 5.0, -5.0, 5.0, N, hg.NODES_LGL,
+                                     elem_offset=eo, edge_offset=fo)
             x = d["x"].reshape(-1, 2)
             qs.append(cases.isentropic_vortex(x[:, 0], x[:, 1], mach=0.5, beta=it["beta"], xc=it["xc"], yc=it["yc"]))
             eo += len(d["N"])
             fo += len(d["edge_marker"])
             descs.append(d)
-        buckets.append((hmesh.concat_descriptors(descs), np.concatenate(qs).ravel(), N,
-                        sum(1 for i in inst if i["N"] == N)))
-    return buckets
+        parts.append((hmesh.concat_descriptors(descs), np.concatenate(qs).ravel(), N,
+                      sum(1 for i in inst if i["N"] == N), kw, 0.4))
+    return parts
+
+
+def stage_bytes_per_dof(config, prec_fp32, affine):
+    """Algorithmic DRAM bytes per DOF of one launch of the fused stage kernel (RK3 average).
+
+    State Q read + written in FP64 (16 B), RK register G written every stage and read in
+    stages 2-3 (sG = 4 or 8 B), volume metrics (Ja, 1/J: 5 FP64 per node = 10 B/DOF) on
+    curved meshes, 0 on affine ones.  Face traces and nodal matrices are cache-resident."""
+    sg = 4 if prec_fp32 else 8
+    return 16.0 + sg * (1.0 + 2.0 / 3.0) + (0.0 if affine else 10.0)
+
+
+def gradient_bytes_per_dof(affine):
+    """Navier-Stokes gradient pass: Q read (8 B) + volume metrics (10 B/DOF when curved)."""
+    return 8.0 + (0.0 if affine else 10.0)
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -136,53 +188,80 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-# ----------------------------------------------------------------------------- reference arm (CPU)
-def cpu_rate(config, budget_s=12.0, threads=None):
+# ----------------------------------------------------------------------------- CPU (oracle) timing
+class CpuArm:
     """Oracle restatement timed on the host cores on a bounded sample of the workload.
 
-    Instances of the workload are stepped concurrently (one oracle per thread; the
-    ctypes calls release the GIL).  Returns (DOF-stage/s, cores, sample text)."""
-    from concurrent.futures import ThreadPoolExecutor
-    from oracle import oracle as O
-    from horses2d_b200 import mesh as hmesh, cases
-    threads = threads or os.cpu_count() or 1
-    inst = ensemble_spec() if config == "ensemble" else [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
-    if config == "box512":
-        inst = [dict(n=64, N=4, xc=0.0, yc=0.0, beta=5.0)]
-    sample = inst[:threads] if config == "ensemble" else inst * threads
-    orcs = []
-    for it in sample:
-        o = O.Oracle(hmesh.cartesian(it["n"], it["n"], -5.0, 5.0, -5.0, 5.0), it["N"], nodes=O.LGL, riemann=O.ROE,
-                     mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
-        X = o.coords()
-        o.set_state(cases.isentropic_vortex(X[:, 0], X[:, 1], beta=it["beta"], xc=it["xc"], yc=it["yc"]).ravel())
-        orcs.append((o, o.estimate_dt(0.4, 1.0)))
+    cylinder: the full workload on one oracle whose element loops run on all host
+    threads (OpenMP, face loops serial, as the reference's own parallel build).
+    Vortex workloads: instances stepped concurrently, one single-threaded oracle per
+    host thread (the ctypes calls release the GIL)."""
 
-    def run(arg):
+    def __init__(self, config, threads=None):
+        from oracle import oracle as O
+        from horses2d_b200 import mesh as hmesh, cases
+        self.O = O
+        self.config = config
+        self.threads = threads or os.cpu_count() or 1
+        self.steps_done = []
+        if config == "cylinder":
+            O.lib().or_set_threads(self.threads)
+            o = O.Oracle(cylinder_mesh(), 5, nodes=O.LG, riemann=O.ROE, mach=0.2, reynolds=100.0, prandtl=0.72,
+                         navier_stokes=1, viscous=O.BR1,
+                         bcs=[dict(type=O.BC_VISCOUSWALL, wall_type=2), dict(type=O.BC_FARFIELD)])
+            o.set_state(cylinder_state(o.ndof // 4))
+            self.orcs = [(o, o.estimate_dt(0.05, 1.0))]
+            return
+        inst = ensemble_spec() if config == "ensemble" else [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
+        if config == "box512":
+            inst = [dict(n=64, N=4, xc=0.0, yc=0.0, beta=5.0)]
+        self.inst = inst[:self.threads] if config == "ensemble" else inst * self.threads
+        self.orcs = []
+        for it in self.inst:
+            o = O.Oracle(hmesh.cartesian(it["n"], it["n"], -5.0, 5.0, -5.0, 5.0), it["N"], nodes=O.LGL,
+                         riemann=O.ROE, mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
+            X = o.coords()
+            o.set_state(cases.isentropic_vortex(X[:, 0], X[:, 1], beta=it["beta"], xc=it["xc"],
+                                                yc=it["yc"]).ravel())
+            self.orcs.append((o, o.estimate_dt(0.4, 1.0)))
+
+    def _run(self, arg, budget_s, single):
+        O = self.O
+        if single:
+            O.lib().or_set_threads(1)
         o, dt = arg
         t0 = time.perf_counter()
         steps = 0
-        while time.perf_counter() - t0 < budget_s:
+        while time.perf_counter() - t0 < budget_s or steps == 0:
             o.time_step(O.RK3, steps * dt, dt)
             steps += 1
-        return o.ndof * 3 * steps, time.perf_counter() - t0
+        return o.ndof * 3 * steps, time.perf_counter() - t0, steps
 
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        res = list(ex.map(run, orcs))
-    rate = sum(r[0] / r[1] for r in res)
-    txt = (f"{len(sample)} instance(s) ({', '.join(str(it['n']) + 'x' + str(it['n']) + ' N=' + str(it['N']) for it in sample[:4])}"
-           f"{', ...' if len(sample) > 4 else ''}), RK3 steps for ~{budget_s:.0f} s each, one oracle per host thread")
-    return rate, threads, txt
+    def sample(self, budget_s):
+        """(DOF-stage/s, cores, description) of ~budget_s seconds of RK3 steps."""
+        from concurrent.futures import ThreadPoolExecutor
+        if self.config == "cylinder":
+            n, el, steps = self._run(self.orcs[0], budget_s, False)
+            return (n / el, self.threads, f"full cylinder workload (NDOF {self.orcs[0][0].ndof}), {steps} RK3 steps "
+                    f"in {el:.1f} s, OpenMP element loops on {self.threads} threads")
+        with ThreadPoolExecutor(max_workers=self.threads) as ex:
+            res = list(ex.map(lambda a: self._run(a, budget_s, True), self.orcs))
+        rate = sum(r[0] / r[1] for r in res)
+        desc = ", ".join(f"{it['n']}x{it['n']} N={it['N']}" for it in self.inst[:4])
+        return rate, self.threads, (f"{len(self.inst)} instance(s) ({desc}{', ...' if len(self.inst) > 4 else ''}),"
+                                    f" RK3 steps for ~{budget_s:.0f} s each, one single-threaded oracle per host "
+                                    "thread")
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return
+    arm = CpuArm(args.config)
     per_step_rates = []
     cores = 0
     sample = ""
     for s in range(args.warmup + args.steps):
-        rate, cores, sample = cpu_rate(args.config, budget_s=3.0)
+        rate, cores, sample = arm.sample(3.0)
         if s >= args.warmup:
             per_step_rates.append(rate)
     value = float(np.mean(per_step_rates))
@@ -190,20 +269,100 @@ def run_reference(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.config},
-            "cpu_baseline": {"value": value, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
+                             "sample": f"each step: {sample}"},
             "e2e": {"value": value, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "reference Fortran needs gfortran + NetCDF-Fortran (absent); its C++ FP64 restatement is timed"}
     print(json.dumps(line), flush=True)
 
 
 # ----------------------------------------------------------------------------- GPU arm
+def make_contexts(parts, prec, stream):
+    import torch
+    import horses2d_b200 as hg
+    ctxs = []
+    for desc, Q0, N, ninst, kw, cfl in parts:
+        g = hg.GpuDGSEM(desc, precision=prec, **kw)
+        g.set_stream(stream.cuda_stream)
+        Qh = torch.from_numpy(Q0).pin_memory()
+        g.set_state(Qh.numpy())
+        ctxs.append(dict(g=g, Qh=Qh, N=N, ninst=ninst, cfl=cfl))
+    return ctxs
+
+
+class L2Flush:
+    """Writes a 256 MB device buffer (twice the 126 MB L2) between timed steps."""
+
+    def __init__(self, enabled):
+        import torch
+        self.buf = torch.empty(256 * 2 ** 20, dtype=torch.uint8, device="cuda") if enabled else None
+        self.val = 0
+
+    def __call__(self, stream):
+        import torch
+        if self.buf is not None:
+            self.val ^= 1
+            with torch.cuda.stream(stream):
+                self.buf.fill_(self.val)
+
+
+def device_timed(ctxs, steps, warmup, dt, stream, world, dist, flush):
+    """Warm-up, then K steps, each between its own events on the launching stream with the
+    L2 flush (if any) outside the events; barrier + sync on both sides.  Returns (ms, launches)."""
+    import torch
+    import horses2d_b200 as hg
+
+    def step(s):
+        for c in ctxs:
+            c["g"].time_step(hg.SCHEME_RK3, s * dt, dt)
+
+    for s in range(warmup):
+        step(s)
+    torch.cuda.synchronize()
+    launches0 = sum(c["g"].launch_count() for c in ctxs)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for s in range(steps):
+        flush(stream)
+        evs[s][0].record(stream)
+        step(warmup + s)
+        evs[s][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    return sum(a.elapsed_time(b) for a, b in evs), sum(c["g"].launch_count() for c in ctxs) - launches0
+
+
+def kernel_split(ctxs, steps, dt, stream, flush):
+    """Per-kernel CUDA-event times over `steps` further steps (library timing mode)."""
+    import torch
+    import horses2d_b200 as hg
+    for c in ctxs:
+        c["g"].profile(True)
+    for s in range(steps):
+        flush(stream)
+        for c in ctxs:
+            c["g"].time_step(hg.SCHEME_RK3, s * dt, dt)
+    tot = {}
+    for c in ctxs:
+        for k, (ms, n) in c["g"].kernel_times().items():
+            a = tot.setdefault(k, [0.0, 0])
+            a[0] += ms
+            a[1] += n
+        c["g"].profile(False)
+    torch.cuda.synchronize()
+    return tot
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="ensemble", choices=["ensemble", "vortex16", "box512"])
+    ap.add_argument("--config", default="cylinder", choices=CONFIGS)
     ap.add_argument("--precision", default=None, choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -221,61 +380,38 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     precision = args.precision or ("fp32" if args.config == "ensemble" else "fp64")
     prec = hg.PREC_FP32 if precision == "fp32" else hg.PREC_FP64
-    buckets = build_buckets(args.config, prec)
+    parts = build_parts(args.config)
     stream = torch.cuda.Stream()
-    ctxs = []
-    for desc, Q0, N, ninst in buckets:
-        g = hg.GpuDGSEM(desc, mach=0.5, node_type=hg.NODES_LGL, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4,
-                        precision=prec)
-        g.set_stream(stream.cuda_stream)
-        Qh = torch.from_numpy(Q0).pin_memory()
-        ctxs.append((g, Qh, N, ninst))
-    ndof = sum(g.ndof for g, _, _, _ in ctxs)
-    for g, Qh, _, _ in ctxs:
-        g.set_state(Qh.numpy())
-    dt = min(g.estimate_time_step(0.4, 1.0) for g, _, _, _ in ctxs)
+    ctxs = make_contexts(parts, prec, stream)
+    ndof = sum(c["g"].ndof for c in ctxs)
+    dt = min(c["g"].estimate_time_step(c["cfl"], 1.0) for c in ctxs)
+    affine = all(c["g"].info()["affine"] for c in ctxs)
+    ns = any(p[4].get("navier_stokes") for p in parts)
+    flush = L2Flush(ndof * 8 * 3 < 2 * L2_BYTES)
     torch.cuda.synchronize()
 
-    def step(s):
-        for g, _, _, _ in ctxs:
-            g.time_step(hg.SCHEME_RK3, s * dt, dt)
-
-    for s in range(args.warmup):
-        step(s)
-    torch.cuda.synchronize()
     # ---- device-resident timed region
     clocks = ClockSampler(local)
     clocks.start()
-    launches0 = sum(g.launch_count() for g, _, _, _ in ctxs)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for s in range(args.steps):
-        step(args.warmup + s)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    launches = sum(g.launch_count() for g, _, _, _ in ctxs) - launches0
+    ms, launches = device_timed(ctxs, args.steps, args.warmup, dt, stream, world, dist, flush)
     clk = clocks.stop()
+    # ---- per-kernel split (library CUDA-event timing, separate loop)
+    split = kernel_split(ctxs, max(3, min(args.steps, 10)), dt, stream, flush)
     # ---- end to end through the public API with host buffers
     res_host = np.zeros(4)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for g, Qh, _, _ in ctxs:
-        g.set_state(Qh.numpy())
+    for c in ctxs:
+        c["g"].set_state(c["Qh"].numpy())
     for s in range(args.steps):
-        step(s)
-        for g, _, _, _ in ctxs:
-            res_host = np.maximum(res_host, g.residuals())
-    Qout = [np.empty(g.ndof) for g, _, _, _ in ctxs]
-    for (g, _, _, _), q in zip(ctxs, Qout):
-        q[:] = g.state()
+        for c in ctxs:
+            c["g"].time_step(hg.SCHEME_RK3, s * dt, dt)
+            res_host = np.maximum(res_host, c["g"].residuals())
+    Qout = [np.empty(c["g"].ndof) for c in ctxs]
+    for c, q in zip(ctxs, Qout):
+        q[:] = c["g"].state()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
@@ -287,46 +423,73 @@ def main():
     ms, e2e_ms = float(t_max[0]), float(t_max[1])
     value = ndof * 3 * args.steps * world / (ms * 1e-3)
     e2e = ndof * 3 * args.steps * world / (e2e_ms * 1e-3)
-    # roofline of the dominant kernel (the fused stage kernel is every launch of the timed region)
-    sq, sg = 8, (4 if prec == hg.PREC_FP32 else 8)
-    bytes_step = ndof * (3 * (sq + sq + sg) + 2 * sg)           # Q r/w + G w every stage, G r in stages 2-3
-    n_stage_launches = 3 * args.steps * len(ctxs)
-    avg_launch_s = ms * 1e-3 / n_stage_launches
-    bytes_per_launch = bytes_step * args.steps / n_stage_launches
-    achieved = bytes_per_launch / avg_launch_s / 1e9
+
+    # ---- roofline of the dominant kernel (fused stage kernel), from its own event times
+    bpd = stage_bytes_per_dof(args.config, prec == hg.PREC_FP32, affine)
+    st_ms, st_n = split["stage"]
+    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
+    stage_launch_bytes = bpd * ndof / len(ctxs)
+    achieved = stage_launch_bytes / avg_stage_s / 1e9
     peak, peak_kind = peaks()
     traffic = None
     tpath = os.path.join(ROOT, "profiles", f"stage_kernel_{args.config}_{precision}.traffic.json")
     if os.path.exists(tpath):
         try:
-            t = json.load(open(tpath))
-            traffic = t["bytes_per_dof_stage"] * ndof / len(ctxs)
+            traffic = json.load(open(tpath))["bytes_per_dof"] * ndof / len(ctxs)
         except Exception:
             traffic = None
+    step_bytes_per_dof_stage = bpd + (gradient_bytes_per_dof(affine) if ns else 0.0)
+    step_achieved = step_bytes_per_dof_stage * ndof * 3 * args.steps / (ms * 1e-3) / 1e9
+    total_split = sum(v[0] for v in split.values()) or 1.0
     line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc" if prec == hg.PREC_FP32 else "f64",
             "data": "synthetic",
             "config": {"workload": args.config, "ndof": ndof, "precision": precision,
-                       "orders": [c[2] for c in ctxs], "instances": sum(c[3] for c in ctxs),
-                       "scheme": "Williamson RK3", "l2": "inputs larger than L2" if ndof * 8 > L2_BYTES
-                       else "working set fits L2 (no flush)", "parallelism": f"replicas x{world}"},
+                       "orders": [c["N"] for c in ctxs], "instances": sum(c["ninst"] for c in ctxs),
+                       "scheme": "Williamson RK3",
+                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
+                              if flush.buf is not None else "inputs larger than L2"),
+                       "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": ndof * 8 / args.steps,
                     "d2h_bytes_per_step": 32 * len(ctxs) + ndof * 8 / args.steps,
-                    "note": "hg_set_state from pinned host, K x (hg_time_step + hg_residuals), hg_get_state"},
+                    "note": "hg_set_state from pinned host, K x (hg_time_step + hg_residuals), hg_get_state; "
+                            "consecutive steps, no L2 flush"},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_dof_stage": bytes_step / ndof / 3},
+            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel" if ns else "stage_kernel",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
+            "step_roofline": {"algorithmic_bytes_per_dof_stage": step_bytes_per_dof_stage,
+                              "achieved": step_achieved, "frac": step_achieved / peak},
+            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
             "clocks": clk}
+
+    # ---- FP32-bulk companion on the same workload (FP64 runs): speed and density error after K steps
+    if prec == hg.PREC_FP64 and args.config == "cylinder":
+        c32 = make_contexts(parts, hg.PREC_FP32, stream)
+        ms32, _ = device_timed(c32, args.steps, args.warmup, dt, stream, 1, dist, flush)
+        for c in ctxs + c32:
+            c["g"].set_state(c["Qh"].numpy())
+        for s in range(args.steps):
+            for c in ctxs + c32:
+                c["g"].time_step(hg.SCHEME_RK3, s * dt, dt)
+        r64 = np.concatenate([c["g"].state().reshape(-1, 4)[:, 0] for c in ctxs])
+        r32 = np.concatenate([c["g"].state().reshape(-1, 4)[:, 0] for c in c32])
+        line["fp32_bulk"] = {"value": ndof * 3 * args.steps / (ms32 * 1e-3), "ms_per_step": ms32 / args.steps,
+                             "speedup_vs_fp64": ms / ms32,
+                             "rel_l2_density_vs_fp64_after_K_steps": float(np.linalg.norm(r32 - r64)
+                                                                           / np.linalg.norm(r64))}
+        for c in c32:
+            c["g"].close()
     if rank == 0 and not args.no_cpu_baseline:
-        rate, cores, sample = cpu_rate(args.config)
+        rate, cores, sample = CpuArm(args.config).sample(12.0)
         line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
                                 "sample": sample}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    for g, _, _, _ in ctxs:
-        g.close()
+    for c in ctxs:
+        c["g"].close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -45,7 +45,9 @@ class MeshDesc(C.Structure):
 _lib = None
 EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_state", "hg_ndof",
             "hg_time_derivative", "hg_time_step", "hg_time_steps", "hg_residuals", "hg_estimate_dt",
-            "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info")
+            "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info",
+            "hg_profile", "hg_kernel_times")
+KERNEL_KINDS = ("stage", "gradient", "trace", "reduce", "speed")
 
 
 def load():
@@ -81,6 +83,8 @@ def load():
     L.hg_launch_count.argtypes = [vp]
     L.hg_nodes.argtypes = [C.c_int32, C.c_int32, F64P, F64P]
     L.hg_info.argtypes = [vp, I32P]
+    L.hg_profile.argtypes = [vp, C.c_int32]
+    L.hg_kernel_times.argtypes = [vp, F64P, C.POINTER(C.c_int64), C.c_int32]
     _lib = L
     return L
 

@@ -52,6 +52,13 @@ struct hg_ctx {
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
   double save_umax = 0.0, save_amax = 0.0;
+  // per-kernel timing (hg_profile): event pairs recorded around each launch
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_pool;
+  size_t prof_used = 0;
+  std::vector<int> prof_kind;
+  double prof_ms[HG_KERNEL_KINDS] = {};
+  int64_t prof_n[HG_KERNEL_KINDS] = {};
 };
 
 static std::string g_create_err;
@@ -76,10 +83,46 @@ static T* dalloc(size_t n) {
 
 static void free_ctx(hg_ctx* c) {
   if (!c) return;
+  for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+// ------------------------------------------------------------------ per-kernel timing
+static void prof_collect(hg_ctx* c) {
+  if (c->prof_used == 0) return;
+  HG_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t k = 0; k < c->prof_kind.size(); ++k) {
+    float ms = 0.f;
+    HG_CUDA(cudaEventElapsedTime(&ms, c->prof_pool[2 * k], c->prof_pool[2 * k + 1]));
+    c->prof_ms[c->prof_kind[k]] += ms;
+    c->prof_n[c->prof_kind[k]] += 1;
+  }
+  c->prof_kind.clear();
+  c->prof_used = 0;
+}
+
+static cudaEvent_t prof_event(hg_ctx* c) {
+  if (c->prof_used == c->prof_pool.size()) {
+    cudaEvent_t e;
+    HG_CUDA(cudaEventCreate(&e));
+    c->prof_pool.push_back(e);
+  }
+  return c->prof_pool[c->prof_used++];
+}
+
+// Launch f() on the context's stream; with timing on, bracket it by an event pair of kernel class `kind`.
+template <class F>
+static void timed(hg_ctx* c, int kind, F&& f) {
+  if (!c->prof) { f(); return; }
+  if (c->prof_used >= 8192) prof_collect(c);
+  cudaEvent_t a = prof_event(c), b = prof_event(c);
+  HG_CUDA(cudaEventRecord(a, c->stream));
+  f();
+  HG_CUDA(cudaEventRecord(b, c->stream));
+  c->prof_kind.push_back(kind);
 }
 
 // ------------------------------------------------------------------ launches
@@ -92,8 +135,10 @@ template <int P, typename real>
 static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   constexpr int EPB = epb_for(P);
   const int grid = (a.n_el + EPB - 1) / EPB;
-  if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
-  else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
+  timed(c, HG_KERNEL_STAGE, [&] {
+    if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
+    else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
+  });
   ++c->launches;
 }
 
@@ -101,8 +146,10 @@ template <int P, typename real>
 static void launch_trace_P(hg_ctx* c) {
   constexpr int EPB = epb_for(P);
   const int grid = (c->n_el + EPB - 1) / EPB;
-  trace_kernel<P, EPB, real><<<grid, block_for(P), 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats,
-                                                                   static_cast<real*>(c->d_T[c->cur]));
+  timed(c, HG_KERNEL_TRACE, [&] {
+    trace_kernel<P, EPB, real><<<grid, block_for(P), 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats,
+                                                                     static_cast<real*>(c->d_T[c->cur]));
+  });
   ++c->launches;
 }
 
@@ -110,8 +157,9 @@ template <int P, typename real, bool AFFINE, bool IP>
 static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
   constexpr int EPB = epb_ns(P);
   const int grid = (a.n_el + EPB - 1) / EPB;
-  ns_gradient_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a);
-  ns_stage_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a);
+  timed(c, HG_KERNEL_GRADIENT,
+        [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });
+  timed(c, HG_KERNEL_STAGE, [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });
   c->launches += 2;
 }
 
@@ -535,7 +583,8 @@ extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double 
 
 extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
   try {
-    residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c), c->d_resid, c->d_resid_out);
+    timed(c, HG_KERNEL_REDUCE,
+          [&] { residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c), c->d_resid, c->d_resid_out); });
     ++c->launches;
     HG_CUDA(cudaGetLastError());
     HG_CUDA(cudaMemcpyAsync(out, c->d_resid_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -548,8 +597,10 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
   try {
     require_state(c);
     const int threads = 256;
-    element_speed_kernel<<<(c->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
-        c->n_el, c->P * c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
+    timed(c, HG_KERNEL_SPEED, [&] {
+      element_speed_kernel<<<(c->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
+          c->n_el, c->P * c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
+    });
     ++c->launches;
     HG_CUDA(cudaGetLastError());
     std::vector<double> em(size_t(c->n_el) * 2);
@@ -581,6 +632,28 @@ extern "C" int hg_synchronize(hg_ctx* c) {
   try {
     HG_CUDA(cudaStreamSynchronize(c->stream));
     HG_CUDA(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_profile(hg_ctx* c, int32_t enable) {
+  try {
+    prof_collect(c);
+    if (enable) {
+      for (int k = 0; k < HG_KERNEL_KINDS; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
+    }
+    c->prof = enable != 0;
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_kernel_times(hg_ctx* c, double* ms, int64_t* launches, int32_t n) {
+  try {
+    prof_collect(c);
+    for (int k = 0; k < n && k < HG_KERNEL_KINDS; ++k) {
+      if (ms) ms[k] = c->prof_ms[k];
+      if (launches) launches[k] = c->prof_n[k];
+    }
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }

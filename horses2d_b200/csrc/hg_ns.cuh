@@ -15,7 +15,6 @@
 //        condition (Dirichlet / adiabatic / Neumann, :1142-1511), the interior-penalty gradient-face
 //        terms lifted by Scalar_StdGradientFace (DGWeakIntegrals.f90:268-495), 1/J, the RK update
 //        and the new Q traces.
-// Artificial viscosity enters as an element viscosity mu_a (Physical type) when given.
 #pragma once
 #include "hg_stage.cuh"
 

@@ -156,6 +156,17 @@ class GpuDGSEM:
     def launch_count(self):
         return self._lib.hg_launch_count(self._h)
 
+    def profile(self, enable=True):
+        """Start (clearing the totals) or stop per-kernel CUDA-event timing."""
+        self._check(self._lib.hg_profile(self._h, 1 if enable else 0))
+
+    def kernel_times(self):
+        """{kernel class: (total ms, launches)} since profile(True)."""
+        n = len(L.KERNEL_KINDS)
+        ms, cnt = (C.c_double * n)(), (C.c_int64 * n)()
+        self._check(self._lib.hg_kernel_times(self._h, ms, cnt, n))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(L.KERNEL_KINDS)}
+
     def info(self):
         """{N, n_elements, affine, precision} of the context."""
         out = (C.c_int32 * 4)()

@@ -123,6 +123,16 @@ int  hg_synchronize(hg_ctx* ctx);
 double* hg_device_state(hg_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t hg_launch_count(const hg_ctx* ctx);
+/* Per-kernel device time (no reference counterpart; the reference has only its
+ * whole-simulation stopwatch, DGTimeIntegrator.f90:173-242).  With timing on,
+ * every launch is bracketed by a CUDA event pair on the context's stream.
+ * hg_profile(ctx, 1) clears the totals and starts; hg_profile(ctx, 0) stops.
+ * hg_kernel_times synchronises and returns, per HG_KERNEL_* class (first n),
+ * the summed milliseconds and the launch count since timing started. */
+enum { HG_KERNEL_STAGE = 0, HG_KERNEL_GRADIENT = 1, HG_KERNEL_TRACE = 2, HG_KERNEL_REDUCE = 3,
+       HG_KERNEL_SPEED = 4, HG_KERNEL_KINDS = 5 };
+int  hg_profile(hg_ctx* ctx, int32_t enable);
+int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
 /* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
 int  hg_info(const hg_ctx* ctx, int32_t out[4]);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N

@@ -16,6 +16,9 @@
 #include <cstring>
 #include <cstdio>
 #include <exception>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 using namespace orc;
 
@@ -169,6 +172,16 @@ extern "C" int or_integrate(void* h, int scheme, int mode, double t0, double t_e
   if (t_out) *t_out = t;
   (void)o;
   return iter;
+}
+
+// OpenMP team size of the calling host thread's parallel regions (the reference runs
+// with OMP_NUM_THREADS threads; callers that step one oracle per host thread pass 1).
+extern "C" void or_set_threads(int n) {
+#ifdef _OPENMP
+  omp_set_num_threads(n > 0 ? n : 1);
+#else
+  (void)n;
+#endif
 }
 
 extern "C" void or_ref_values(void* h, double out[8]) {

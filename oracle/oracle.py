@@ -77,6 +77,7 @@ def lib():
         L.or_integrate.restype = i
         L.or_integrate.argtypes = [vp, i, i, d, d, i, d, d, d, dp]
         L.or_ref_values.argtypes = [vp, dp]
+        L.or_set_threads.argtypes = [C.c_int]
         L.or_element_geometry.argtypes = [vp, dp, dp, dp]
         L.or_edge_count_by_type.restype = i
         L.or_edge_count_by_type.argtypes = [vp, i]

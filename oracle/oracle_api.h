@@ -92,6 +92,7 @@ void    or_residuals(void* h, double out[4]);
 int     or_integrate(void* h, int scheme, int mode, double t0, double t_end, int max_iter,
                      double cfl, double dt_cap, double residual_target, double* t_out);
 /* Physics constants resolved by InitializePhysics (Physics/PhysicsNS.f90:405-481). */
+void    or_set_threads(int n);             /* OpenMP threads of the calling thread's regions */
 void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless, invSqrtGammaMach */
 /* Geometry export for cross-checking host-side mesh builders. */
 void    or_element_geometry(void* h, double* Ja, double* jac, double* volume); /* Ja [ndof/4][2][2], jac [ndof/4], volume [E] */
