@@ -46,7 +46,7 @@ _lib = None
 EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_state", "hg_ndof",
             "hg_time_derivative", "hg_time_step", "hg_time_steps", "hg_residuals", "hg_estimate_dt",
             "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info",
-            "hg_profile", "hg_kernel_times")
+            "hg_profile", "hg_kernel_times", "hg_residuals_noalloc")
 KERNEL_KINDS = ("stage", "gradient", "trace", "reduce", "speed")
 
 

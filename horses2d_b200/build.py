@@ -8,7 +8,7 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "libhorsesgpu.so")
-SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp"]
+SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu"]
 DEPS = SOURCES + ["csrc/hg_stage.cuh", "csrc/hg_physics.cuh", "csrc/hg_bc.cuh", "csrc/hg_ns.cuh", "csrc/hg_spectral.h", "../include/horses_gpu.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]

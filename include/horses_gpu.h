@@ -133,6 +133,21 @@ enum { HG_KERNEL_STAGE = 0, HG_KERNEL_GRADIENT = 1, HG_KERNEL_TRACE = 2, HG_KERN
        HG_KERNEL_SPEED = 4, HG_KERNEL_KINDS = 5 };
 int  hg_profile(hg_ctx* ctx, int32_t enable);
 int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
+/* hg_residuals_noalloc -- no reference counterpart.  Per-variable max |x| (the reduction of
+ * Mesh_ComputeResiduals, QuadMesh_Auxiliars.incf:22-38) of a caller-owned DEVICE array in the
+ * reference layout (ndof doubles, 4 per node, 32-byte aligned), written to the HOST array out[4].
+ * It allocates no device memory: partial maxima go to a fixed file-scope device scratch
+ * (512 KB + 32 B), which bounds ndof to HG_NOALLOC_MAX_NDOF (= 16384 blocks x 8192 nodes x 4);
+ * larger or malformed sizes are rejected before any launch.  For callers that hold a QDot (or
+ * any state-shaped) array on the device and may not allocate, e.g. a monitor running inside a
+ * fixed device-memory budget.  Runs on cuda_stream (NULL: legacy default stream) and
+ * synchronises it.  The first call with a device current looks up the scratch address for that
+ * device (cudaGetSymbolAddress); make one call before any stream capture if you capture.  Calls
+ * that overlap in time on one device share the scratch and race: serialise them.
+ * Returns 0 ok, 1 bad argument (null, ndof <= 0, not a multiple of 4, above the limit,
+ * misaligned), 2 set-up failed, 3 launch or copy failed. */
+#define HG_NOALLOC_MAX_NDOF 536870912LL
+int  hg_residuals_noalloc(const double* qdot, int64_t ndof, void* cuda_stream, double out[4]);
 /* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
 int  hg_info(const hg_ctx* ctx, int32_t out[4]);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N
