@@ -126,6 +126,13 @@ static void timed(hg_ctx* c, int kind, F&& f) {
 }
 
 // ------------------------------------------------------------------ launches
+// Prefer the largest shared-memory carve-out for a kernel (once per instantiation): the stage
+// kernels are latency-bound and their resident CTAs per SM are capped by shared memory otherwise.
+template <typename K>
+static void max_carveout(K kernel) {
+  HG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+}
 static int grid_for(const hg_ctx* c) {
   const int epb = c->ns ? epb_ns(c->P) : epb_for(c->P);
   return (c->n_el + epb - 1) / epb;
@@ -135,6 +142,12 @@ template <int P, typename real>
 static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   constexpr int EPB = epb_for(P);
   const int grid = (a.n_el + EPB - 1) / EPB;
+  static bool attr = false;
+  if (!attr) {
+    max_carveout(stage_kernel<P, EPB, real, true>);
+    max_carveout(stage_kernel<P, EPB, real, false>);
+    attr = true;
+  }
   timed(c, HG_KERNEL_STAGE, [&] {
     if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
     else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
@@ -157,6 +170,12 @@ template <int P, typename real, bool AFFINE, bool IP>
 static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
   constexpr int EPB = epb_ns(P);
   const int grid = (a.n_el + EPB - 1) / EPB;
+  static bool attr = false;
+  if (!attr) {
+    max_carveout(ns_gradient_kernel<P, EPB, real, AFFINE, IP>);
+    max_carveout(ns_stage_kernel<P, EPB, real, AFFINE, IP>);
+    attr = true;
+  }
   timed(c, HG_KERNEL_GRADIENT,
         [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });
   timed(c, HG_KERNEL_STAGE, [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });

@@ -14,16 +14,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
 BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL, BC_FARFIELD, BC_PRESSUREOUTLET = 1, 2, 3, 4, 5, 6
+BC_NEWDIRICHLET = 7
 ROE, HLL, EXACT, LXF, INTERIOR = 0, 1, 2, 3, -1
 LG, LGL = 1, 2
 EULER, RK3, RK5 = 0, 1, 2
 BR1, IP = 0, 1
+AV_NONE, AV_LAPLACIAN, AV_PHYSICAL = 0, 1, 2
 
 
 class OrBC(C.Structure):
     _fields_ = [("type", C.c_int), ("riemann", C.c_int), ("periodic_dir", C.c_int), ("connected_marker", C.c_int),
                 ("pressure", C.c_double), ("temperature", C.c_double), ("mach", C.c_double), ("aoa_deg", C.c_double),
-                ("wall_type", C.c_int), ("wall_T", C.c_double), ("wall_v", C.c_double * 2), ("outflow_type", C.c_int)]
+                ("wall_type", C.c_int), ("wall_T", C.c_double), ("wall_v", C.c_double * 2), ("outflow_type", C.c_int),
+                ("nd_mode", C.c_int), ("nd_outflow_total", C.c_int)]
 
 
 class OrCase(C.Structure):
@@ -31,7 +34,7 @@ class OrCase(C.Structure):
                 ("ip_method", C.c_int), ("sigma0_ip", C.c_double), ("sigma1_ip", C.c_double),
                 ("mach", C.c_double), ("reynolds", C.c_double), ("prandtl", C.c_double),
                 ("pressure_ref", C.c_double), ("temperature_ref", C.c_double), ("reynolds_length", C.c_double),
-                ("n_markers", C.c_int), ("bcs", C.POINTER(OrBC))]
+                ("n_markers", C.c_int), ("bcs", C.POINTER(OrBC)), ("av_type", C.c_int), ("av_intensity", C.c_double)]
 
 
 class OrMesh(C.Structure):
@@ -99,7 +102,7 @@ class Oracle:
 
     def __init__(self, mesh, poly_order, *, nodes=LGL, riemann=ROE, mach=0.5, reynolds=0.0, prandtl=0.72,
                  pressure_ref=101325.0, temperature_ref=273.15, reynolds_length=1.0, bcs=(), navier_stokes=0,
-                 viscous=BR1, ip_method=0, sigma0_ip=1.0, sigma1_ip=0.0):
+                 viscous=BR1, ip_method=0, sigma0_ip=1.0, sigma1_ip=0.0, av_type=0, av_intensity=1.0):
         self._keep = []
         m = OrMesh()
         pts = np.ascontiguousarray(mesh["points"], dtype=np.float64)
@@ -137,11 +140,14 @@ class Oracle:
             wv = b.get("wall_v", (0.0, 0.0))
             bb.wall_v[0], bb.wall_v[1] = wv[0], wv[1]
             bb.outflow_type = b.get("outflow_type", 1)
+            bb.nd_mode = b.get("mode", 0)
+            bb.nd_outflow_total = b.get("outflow_total", 0)
         self._keep.append(bc_arr)
         c = OrCase(nodes=nodes, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous, ip_method=ip_method,
                    sigma0_ip=sigma0_ip, sigma1_ip=sigma1_ip, mach=mach, reynolds=reynolds, prandtl=prandtl,
                    pressure_ref=pressure_ref, temperature_ref=temperature_ref, reynolds_length=reynolds_length,
-                   n_markers=len(bcs), bcs=C.cast(bc_arr, C.POINTER(OrBC)))
+                   n_markers=len(bcs), bcs=C.cast(bc_arr, C.POINTER(OrBC)), av_type=av_type,
+                   av_intensity=av_intensity)
         err = C.create_string_buffer(512)
         self.h = lib().or_create(C.byref(c), C.byref(m), err, 512)
         if not self.h:

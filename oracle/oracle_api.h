@@ -22,7 +22,7 @@ extern "C" {
 
 /* Boundary-condition kinds (Generic/Defines.h FACE_INTERIOR .. NEWDIRICHLET_BC). */
 enum { OR_BC_PERIODIC = 1, OR_BC_DIRICHLET = 2, OR_BC_EULERWALL = 3, OR_BC_VISCOUSWALL = 4,
-       OR_BC_FARFIELD = 5, OR_BC_PRESSUREOUTLET = 6 };
+       OR_BC_FARFIELD = 5, OR_BC_PRESSUREOUTLET = 6, OR_BC_NEWDIRICHLET = 7 };
 /* Riemann solvers (Physics/RiemannSolvers.f90); LXF is new (no reference). */
 enum { OR_RIEMANN_ROE = 0, OR_RIEMANN_HLL = 1, OR_RIEMANN_EXACT = 2, OR_RIEMANN_LXF = 3,
        OR_RIEMANN_INTERIOR = -1 };
@@ -30,6 +30,7 @@ enum { OR_NODES_LG = 1, OR_NODES_LGL = 2 };
 enum { OR_SCHEME_EULER = 0, OR_SCHEME_RK3 = 1, OR_SCHEME_RK5 = 2 };
 enum { OR_VISC_BR1 = 0, OR_VISC_IP = 1 };
 enum { OR_IP_SIPG = 0, OR_IP_NIPG = 1, OR_IP_IIPG = 2 };
+enum { OR_AV_NONE = 0, OR_AV_LAPLACIAN = 1, OR_AV_PHYSICAL = 2 };
 
 typedef struct {
   int    type;              /* OR_BC_* */
@@ -44,6 +45,8 @@ typedef struct {
   double wall_T;            /* isothermal wall temperature, K */
   double wall_v[2];         /* wall velocity, dimensionless: sqrt(gamma) * Mach * direction */
   int    outflow_type;      /* pressure outlet: 1 reflective, 2 partially non-reflective */
+  int    nd_mode;           /* newDirichlet "Mode": 0 specify speed (default), 1 specify total pressure */
+  int    nd_outflow_total;  /* newDirichlet "Outflow pressure": 0 static (default), 1 total */
 } or_bc;
 
 typedef struct {
@@ -58,6 +61,8 @@ typedef struct {
   double pressure_ref, temperature_ref, reynolds_length;
   int    n_markers;
   const or_bc* bcs;         /* [n_markers], zone k+1 */
+  int    av_type;           /* artificial dissipation: OR_AV_NONE / LAPLACIAN / PHYSICAL (jumps-based indicator) */
+  double av_intensity;      /* "Artificial dissipation intensity" (Ceps) */
 } or_case;
 
 typedef struct {
@@ -91,8 +96,8 @@ void    or_residuals(void* h, double out[4]);
  * mode 1 transient, 0 steady.  Returns the number of iterations run. */
 int     or_integrate(void* h, int scheme, int mode, double t0, double t_end, int max_iter,
                      double cfl, double dt_cap, double residual_target, double* t_out);
-/* Physics constants resolved by InitializePhysics (Physics/PhysicsNS.f90:405-481). */
 void    or_set_threads(int n);             /* OpenMP threads of the calling thread's regions */
+/* Physics constants resolved by InitializePhysics (Physics/PhysicsNS.f90:405-481). */
 void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless, invSqrtGammaMach */
 /* Geometry export for cross-checking host-side mesh builders. */
 void    or_element_geometry(void* h, double* Ja, double* jac, double* volume); /* Ja [ndof/4][2][2], jac [ndof/4], volume [E] */

@@ -321,6 +321,14 @@ void setup_zones(Oracle& o) {
         case OR_BC_VISCOUSWALL:
           viscous_wall_associate(o, Z, f);
           break;
+        case OR_BC_NEWDIRICHLET:   // newDirichletBC_Associate; uSB aliases uB (newDirichlet.incf)
+          Z.q = bc_state(o, Z.bc);
+          f.inviscidBCType = WEAK_RIEMANN;
+          f.uB_own.assign(4 * P, 0.0);
+          f.uB = &f.uB_own;
+          f.uSB = &f.uB_own;
+          f.viscousBCType.assign(P, VBC_DIRICHLET);
+          break;
         default: throw std::runtime_error("boundary condition not supported by the oracle");
       }
     }
@@ -386,6 +394,78 @@ static void euler_wall_update(const Oracle& o, Edge& f) {
   }
 }
 
+// newDirichletBC_UpdateSolution (BoundaryConditions/newDirichlet.incf): characteristic in/outflow
+// state per node from the zone state (no boundary-condition function).
+static double gf_norm2(double a, double b) {   // NORM2 of two values, scaled sum of squares
+  double scale = 0.0, ssq = 1.0;
+  for (double x : {a, b}) {
+    if (x != 0.0) {
+      const double ax = std::fabs(x);
+      if (scale < ax) { ssq = 1.0 + ssq * (scale / ax) * (scale / ax); scale = ax; }
+      else ssq = ssq + (ax / scale) * (ax / scale);
+    }
+  }
+  return scale * std::sqrt(ssq);
+}
+
+static void newdirichlet_update(Oracle& o, Zone& Z, Edge& f) {
+  const Physics& ph = o.ph;
+  const int P = f.P();
+  const double gamma = ph.gamma, gm1 = ph.gm1, cp = ph.cp, cv = ph.cv;
+  const double* q = Z.q.data();
+  const std::vector<double>& Q = f.storage[0].Q;
+  for (int i = 0; i < P; ++i) {
+    const double uExt = q[1] / q[0], vExt = q[2] / q[0];
+    const double nrm = gf_norm2(uExt, vExt);
+    const double nInf[2] = {uExt / nrm, vExt / nrm};
+    const double pExt = gm1 * (q[3] - 0.5 * (q[1] * uExt + q[2] * vExt));
+    const double MExtSq = (uExt * uExt + vExt * vExt) / (gamma * pExt) * q[0];
+    const double sExt = pExt / std::pow(q[0], gamma);
+    const double ptExt = pExt * std::pow(1.0 + 0.5 * gm1 * MExtSq, cp);
+    const double* qL = &Q[4 * i];
+    double* uB = &f.uB_own[4 * i];
+    const double rhoL = qL[0], uL = qL[1] / rhoL, vL = qL[2] / rhoL;
+    const double vnL = uL * f.nx(i) + vL * f.ny(i);
+    const double pL = gm1 * (qL[3] - 0.5 * (qL[1] * uL + qL[2] * vL));
+    const double aL = std::sqrt(gamma * pL / rhoL);
+    const double ML = std::sqrt(uL * uL + vL * vL) / aL;
+    int vbc;
+    if (vnL <= 0.0) {
+      if (ML > 1.0) {
+        for (int k = 0; k < 4; ++k) uB[k] = q[k];
+      } else {
+        const double pR = pL;
+        const double rhoR = std::pow(pR / sExt, 1.0 / gamma);
+        const double aR = std::sqrt(gamma * pR / rhoR);
+        if (Z.bc.nd_mode == 0) {
+          uB[0] = q[0]; uB[1] = q[1]; uB[2] = q[2];
+          uB[3] = cv * pR + 0.5 * (uB[1] * uB[1] + uB[2] * uB[2]) / uB[0];
+        } else {
+          double MR;
+          if (pR >= ptExt) MR = -std::sqrt(2.0 / gm1 * (std::pow(pR / ptExt, gm1 / gamma) - 1.0));
+          else MR = std::sqrt(2.0 / gm1 * (std::pow(ptExt / pR, gm1 / gamma) - 1.0));
+          uB[0] = rhoR;
+          uB[1] = rhoR * aR * MR * nInf[0];
+          uB[2] = rhoR * aR * MR * nInf[1];
+          uB[3] = cv * pR + 0.5 * rhoR * aR * aR * MR * MR;
+        }
+      }
+      vbc = VBC_DIRICHLET;
+    } else {
+      if (ML > 1.0) {
+        for (int k = 0; k < 4; ++k) uB[k] = qL[k];
+        vbc = VBC_NEUMANN;
+      } else {
+        uB[0] = qL[0]; uB[1] = qL[1]; uB[2] = qL[2];
+        const double pb = Z.bc.nd_outflow_total ? ptExt : pExt;
+        uB[3] = cv * (2.0 * pb - pL) + 0.5 * (uB[1] * uL + uB[2] * vL);
+        vbc = VBC_DIRICHLET;
+      }
+    }
+    if (o.cas.navier_stokes) f.viscousBCType[i] = vbc;
+  }
+}
+
 static void update_zones(Oracle& o, double t) {
   for (size_t z = 1; z < o.zones.size(); ++z) {
     Zone& Z = o.zones[z];
@@ -397,6 +477,7 @@ static void update_zones(Oracle& o, double t) {
         case OR_BC_FARFIELD: farfield_update(o, Z, f); break;
         case OR_BC_PRESSUREOUTLET: pressure_outlet_update(o, Z, f); break;
         case OR_BC_VISCOUSWALL: viscous_wall_update(o, Z, f); break;
+        case OR_BC_NEWDIRICHLET: newdirichlet_update(o, Z, f); break;
         default: break;
       }
     }
@@ -588,6 +669,7 @@ static void volume_loop(Oracle& o, Element& e, ViscousWork& vw) {
   std::vector<double> F(size_t(P) * P * 8);   // [(node)*8 + dim*4 + k]
   for (int q = 0; q < P * P; ++q) inviscid_flux(ph, &Q[4 * q], &F[q * 8], &F[q * 8 + 4]);
   if (o.cas.navier_stokes) viscous_volume_flux(o, e, F, vw);
+  if (o.cas.navier_stokes) av_volume_flux(o, e, F);
   std::vector<double> Fc(4 * P * P, 0.0), Gc(4 * P * P, 0.0);
   for (int d = 0; d < 2; ++d)
     for (int q = 0; q < P * P; ++q)
@@ -611,6 +693,8 @@ void time_derivative(Oracle& o, double t) {
   interpolate_to_boundaries(o, false);
   update_zones(o, t);
   if (o.cas.navier_stokes) {
+    compute_av_viscosity(o);
+    set_physical_av(o);
     compute_gradient(o, vw);
     interpolate_to_boundaries(o, true);
   }

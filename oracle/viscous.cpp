@@ -83,10 +83,11 @@ struct EdgeArrays {
 };
 
 // viscous Riemann flux at one point (BR1 / IP interior form), including mu: Fstar[k]
-static void visc_riemann(const Oracle& o, int N, double invh, const double* qL, const double* qR, const double* dqLx,
-                         const double* dqLy, const double* dqRx, const double* dqRy, double nx, double ny, double* Fs) {
+static void visc_riemann(const Oracle& o, double mu_a, int N, double invh, const double* qL, const double* qR,
+                         const double* dqLx, const double* dqLy, const double* dqRx, const double* dqRy, double nx,
+                         double ny, double* Fs) {
   const Physics& ph = o.ph;
-  const double mu = ph.mu + 0.0;
+  const double mu = ph.mu + mu_a;
   double FLx[4], FLy[4], FRx[4], FRy[4];
   vflux(ph, qL, dqLx, dqLy, FLx, FLy);
   vflux(ph, qR, dqRx, dqRy, FRx, FRy);
@@ -104,13 +105,13 @@ static void visc_riemann(const Oracle& o, int N, double invh, const double* qL, 
 }
 
 // IP_GradientRiemannSolver at one point: GL[d][k], GR[d][k]
-static void visc_gradient_riemann(const Oracle& o, const double* qL, const double* qR, double nx, double ny, double* GLx,
-                                  double* GLy, double* GRx, double* GRy) {
+static void visc_gradient_riemann(const Oracle& o, double mu_a, const double* qL, const double* qR, double nx, double ny,
+                                  double* GLx, double* GLy, double* GRx, double* GRy) {
   const Physics& ph = o.ph;
   double fgx[4], fgy[4];
   for (int k = 0; k < 4; ++k) { fgx[k] = (qL[k] - qR[k]) * nx; fgy[k] = (qL[k] - qR[k]) * ny; }
   const double eps = ip_epsilon(o);
-  const double cL = 0.5 * eps * (ph.mu + 0.0), cR = -0.5 * eps * (ph.mu + 0.0);
+  const double cL = 0.5 * eps * (ph.mu + mu_a), cR = -0.5 * eps * (ph.mu + mu_a);
   vflux(ph, qL, fgx, fgy, GLx, GLy);
   vflux(ph, qR, fgx, fgy, GRx, GRy);
   for (int k = 0; k < 4; ++k) { GLx[k] *= cL; GLy[k] *= cL; GRx[k] *= cR; GRy[k] *= cR; }
@@ -432,7 +433,7 @@ static void vector_volume_green(Oracle& o, Element& e, double* dQ) {
   for (size_t n = 0; n < vol.size(); ++n) dQ[n] = -vol[n];
 }
 
-static void interior_gradient(Oracle& o, Element& e, double* dQ) {
+void interior_gradient(Oracle& o, Element& e, double* dQ) {
   const int P = e.P;
   const Spectral& s = *e.sp;
   const double* Q = &o.Q[e.offset];
@@ -607,9 +608,11 @@ void viscous_interior_flux(Oracle& o, Edge& f, const std::vector<double>& QL, co
   std::vector<double> dQR = project_to_edge(f, SLOT_RIGHT, f.storage[SLOT_RIGHT].dQ, 2);
   for (int i = 0; i < P; ++i) {
     double Fv[4];
-    visc_riemann(o, f.N, f.invh, &QL[4 * i], &QR[4 * i], &dQL[4 * i], &dQL[(P + i) * 4], &dQR[4 * i], &dQR[(P + i) * 4],
-                 f.nx(i), f.ny(i), Fv);
-    for (int k = 0; k < 4; ++k) Fs[4 * i + k] = Fs[4 * i + k] - Fv[k] - 0.0;
+    visc_riemann(o, f.mu_a, f.N, f.invh, &QL[4 * i], &QR[4 * i], &dQL[4 * i], &dQL[(P + i) * 4], &dQR[4 * i],
+                 &dQR[(P + i) * 4], f.nx(i), f.ny(i), Fv);
+    double Fa[4];
+    av_face_flux(o, f, &QL[4 * i], &QR[4 * i], Fa);
+    for (int k = 0; k < 4; ++k) Fs[4 * i + k] = Fs[4 * i + k] - Fv[k] - Fa[k];
   }
 }
 
@@ -621,7 +624,7 @@ void viscous_interior_gradient_faces(Oracle& o, Edge& f, const std::vector<doubl
   std::vector<double> GL(8 * P), GR(8 * P);
   for (int i = 0; i < P; ++i) {
     double a[4], b[4], c[4], d[4];
-    visc_gradient_riemann(o, &QL[4 * i], &QR[4 * i], f.nx(i), f.ny(i), a, b, c, d);
+    visc_gradient_riemann(o, f.mu_a, &QL[4 * i], &QR[4 * i], f.nx(i), f.ny(i), a, b, c, d);
     for (int k = 0; k < 4; ++k) {
       GL[(0 * P + i) * 4 + k] = a[k]; GL[(P + i) * 4 + k] = b[k];
       GR[(0 * P + i) * 4 + k] = c[k]; GR[(P + i) * 4 + k] = d[k];
@@ -670,16 +673,20 @@ void viscous_mortar_fluxes(Oracle& o, Edge& f, const std::vector<double>& QLN, c
   for (int i = 0; i < PN; ++i) {
     const double nx = curved ? f.normal_N[i] : f.normal_N[0], ny = curved ? f.normal_N[PN + i] : f.normal_N[1];
     double Fv[4];
-    visc_riemann(o, f.N_N, f.invh, &QLN[4 * i], &QRN[4 * i], &dLN[4 * i], &dLN[(PN + i) * 4], &dRN[4 * i],
+    visc_riemann(o, f.mu_a, f.N_N, f.invh, &QLN[4 * i], &QRN[4 * i], &dLN[4 * i], &dLN[(PN + i) * 4], &dRN[4 * i],
                  &dRN[(PN + i) * 4], nx, ny, Fv);
-    for (int k = 0; k < 4; ++k) FN[4 * i + k] = FN[4 * i + k] - Fv[k] - 0.0;
+    double Fa[4];
+    av_face_flux(o, f, &QLN[4 * i], &QRN[4 * i], Fa);
+    for (int k = 0; k < 4; ++k) FN[4 * i + k] = FN[4 * i + k] - Fv[k] - Fa[k];
   }
   for (int i = 0; i < PS; ++i) {
     const double nx = curved ? f.normal_S[i] : f.normal_S[0], ny = curved ? f.normal_S[PS + i] : f.normal_S[1];
     double Fv[4];
-    visc_riemann(o, f.N_S, f.invh, &QLS[4 * i], &QRS[4 * i], &dLS[4 * i], &dLS[(PS + i) * 4], &dRS[4 * i],
+    visc_riemann(o, f.mu_a, f.N_S, f.invh, &QLS[4 * i], &QRS[4 * i], &dLS[4 * i], &dLS[(PS + i) * 4], &dRS[4 * i],
                  &dRS[(PS + i) * 4], nx, ny, Fv);
-    for (int k = 0; k < 4; ++k) FS[4 * i + k] = FS[4 * i + k] - Fv[k] - 0.0;
+    double Fa[4];
+    av_face_flux(o, f, &QLS[4 * i], &QRS[4 * i], Fa);
+    for (int k = 0; k < 4; ++k) FS[4 * i + k] = FS[4 * i + k] - Fv[k] - Fa[k];
   }
 }
 
@@ -697,7 +704,7 @@ void viscous_mortar_gradient_faces(Oracle& o, Edge& f, const std::vector<double>
       const double nx = curved ? nrm[i] : nrm[0], ny = curved ? nrm[Pm + i] : nrm[1];
       const double dS = curved ? dSm[i] : dSm[0];
       double a[4], b[4], c[4], d[4];
-      visc_gradient_riemann(o, &QL[4 * i], &QR[4 * i], nx, ny, a, b, c, d);
+      visc_gradient_riemann(o, f.mu_a, &QL[4 * i], &QR[4 * i], nx, ny, a, b, c, d);
       for (int k = 0; k < 4; ++k) {
         GL[(0 * Pm + i) * 4 + k] = a[k] * dS; GL[(Pm + i) * 4 + k] = b[k] * dS;
         GR[(0 * Pm + i) * 4 + k] = c[k] * dS; GR[(Pm + i) * 4 + k] = d[k] * dS;
@@ -732,9 +739,9 @@ void viscous_boundary_flux(Oracle& o, Edge& f, std::vector<double>& F, ViscousWo
   const int P = f.P();
   const std::vector<double>& Q = f.storage[0].Q;
   const std::vector<double>& dQ = f.storage[0].dQ;
-  std::vector<double> Fv(4 * P, 0.0);
+  std::vector<double> Fv(4 * P, 0.0), Fa(4 * P, 0.0);
   g_bdryG.assign(8 * P, 0.0);
-  const double mu = ph.mu + 0.0;
+  const double mu = ph.mu + f.mu_a;
   const bool ip = is_ip(o);
   const double penalty = ip ? o.cas.sigma0_ip * mu * f.N * f.N * f.invh : 0.0;
   const double eps = ip_epsilon(o);
@@ -747,17 +754,24 @@ void viscous_boundary_flux(Oracle& o, Edge& f, std::vector<double>& F, ViscousWo
       double qb[4], gbx[4], gby[4];
       for (int k = 0; k < 4; ++k) { qb[k] = uB[4 * r + k]; gbx[k] = gB[4 * r + k]; gby[k] = gB[(P + r) * 4 + k]; }
       double fv[4];
-      visc_riemann(o, f.N, f.invh, &Q[4 * i], qb, &dQ[4 * i], &dQ[(P + i) * 4], gbx, gby, f.nx(i), f.ny(i), fv);
+      visc_riemann(o, f.mu_a, f.N, f.invh, &Q[4 * i], qb, &dQ[4 * i], &dQ[(P + i) * 4], gbx, gby, f.nx(i), f.ny(i),
+                   fv);
       for (int k = 0; k < 4; ++k) Fv[4 * i + k] = fv[k] * f.dS[0];
+      double fa[4];
+      av_face_flux(o, f, &Q[4 * i], qb, fa);
+      for (int k = 0; k < 4; ++k) Fa[4 * i + k] = fa[k] * f.dS[0];
       if (gradient_faces(o)) {
         double a[4], b[4], c[4], d[4];
-        visc_gradient_riemann(o, &Q[4 * i], qb, f.nx(i), f.ny(i), a, b, c, d);
+        visc_gradient_riemann(o, f.mu_a, &Q[4 * i], qb, f.nx(i), f.ny(i), a, b, c, d);
         for (int k = 0; k < 4; ++k) { g_bdryG[(0 * P + i) * 4 + k] = a[k] * f.dS[0]; g_bdryG[(P + i) * 4 + k] = b[k] * f.dS[0]; }
       }
     }
   } else if (!f.viscousBCType.empty() && f.viscousBCType[0] == VBC_ADIABATIC) {
     const std::vector<double>& uS = *f.uSB;
     for (int i = 0; i < P; ++i) {
+      double fa[4];
+      av_face_flux(o, f, &Q[4 * i], &uS[4 * i], fa);
+      for (int k = 0; k < 4; ++k) Fa[4 * i + k] = fa[k] * dS_at(i);
       double Fx[4], Fy[4];
       vflux_adiabatic(ph, &Q[4 * i], &Q[4 * i], &dQ[4 * i], &dQ[(P + i) * 4], Fx, Fy);
       for (int k = 0; k < 4; ++k) {
@@ -780,6 +794,9 @@ void viscous_boundary_flux(Oracle& o, Edge& f, std::vector<double>& F, ViscousWo
   } else {
     const std::vector<double>& uS = *f.uSB;
     for (int i = 0; i < P; ++i) {
+      double fa[4];
+      av_face_flux(o, f, &Q[4 * i], &uS[4 * i], fa);
+      for (int k = 0; k < 4; ++k) Fa[4 * i + k] = fa[k] * dS_at(i);
       const int vbc = f.viscousBCType.empty() ? VBC_NEUMANN : f.viscousBCType[i];
       if (vbc == VBC_DIRICHLET) {
         double Fx[4], Fy[4];
@@ -802,7 +819,7 @@ void viscous_boundary_flux(Oracle& o, Edge& f, std::vector<double>& F, ViscousWo
       // Neumann (and the far field): zero viscous and gradient-face flux
     }
   }
-  for (int n = 0; n < 4 * P; ++n) F[n] = F[n] - Fv[n] - 0.0;
+  for (int n = 0; n < 4 * P; ++n) F[n] = F[n] - Fv[n] - Fa[n];
 }
 
 void viscous_boundary_gradient_face(Oracle& o, Edge& f, ViscousWork& vw) {

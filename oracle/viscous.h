@@ -34,5 +34,16 @@ void viscous_mortar_gradient_faces(Oracle& o, Edge& f, const std::vector<double>
                                    const std::vector<double>& QLS, const std::vector<double>& QRS, ViscousWork& vw);
 void viscous_boundary_flux(Oracle& o, Edge& f, std::vector<double>& F, ViscousWork& vw);
 void viscous_boundary_gradient_face(Oracle& o, Edge& f, ViscousWork& vw);
+void interior_gradient(Oracle& o, Element& e, double* dQ);   // dQ[(d*NP+q)*4+k]
+
+// dissipation.cpp
+double edge_jumps(const Oracle& o, const Edge& f, int var);
+double av_element_viscosity(const Oracle& o, const Element& e);
+double av_edge_viscosity(const Oracle& o, const Edge& f);
+void compute_av_viscosity(Oracle& o);
+void set_physical_av(Oracle& o);
+bool laplacian_av(const Oracle& o);
+void av_volume_flux(Oracle& o, Element& e, std::vector<double>& F);
+void av_face_flux(const Oracle& o, const Edge& f, const double* qL, const double* qR, double* Fa);
 
 }  // namespace orc

@@ -13,6 +13,11 @@
   pressure outlet, on a p-refined (N = 5/7/10/7) curved mesh with mortars.
   The reference asserts iteration 19585 of the steady RK5 run (CFL 0.4,
   residual 1e-4) and the four final residuals to 1e-12.
+* Ramp benchmark (TestCases/Benchmark/Simulations/Ramp): Navier-Stokes build at
+  Re = 0 with IIPG, the jumps-based Laplacian artificial dissipation (intensity
+  0.1), Euler walls and two newDirichlet zones, Mach 2, N = 3, Legendre-Gauss,
+  steady RK5 (CFL 0.1, dt cap 2, residual 1e-8); the reference asserts
+  iteration 9884 and the four final residuals to 1e-11.
 * Spectral building blocks: exactness of the nodal derivative and quadrature.
 * Free-stream preservation on curved meshes, conservation on periodic meshes.
 """
@@ -157,3 +162,22 @@ def test_ns_freestream_preservation_curved():
         q = np.array([1.0, 0.3 * np.sqrt(1.4), 0.0, 2.5 + 0.5 * 0.09 * 1.4])
         orc.set_state(np.tile(q, orc.ndof // 4))
         assert np.abs(orc.time_derivative(0.0)).max() <= 1e-8
+
+
+def test_ramp_benchmark_golden():
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["Ramp"]
+    bcs = [dict(type=O.BC_EULERWALL), dict(type=O.BC_EULERWALL), dict(type=O.BC_NEWDIRICHLET),
+           dict(type=O.BC_NEWDIRICHLET)]
+    orc = O.Oracle(load_mesh("RampBench"), 3, nodes=O.LG, riemann=O.ROE, mach=2.0, reynolds=0.0, prandtl=0.72,
+                   navier_stokes=1, viscous=O.IP, ip_method=2, sigma0_ip=1.0, bcs=bcs, av_type=O.AV_LAPLACIAN,
+                   av_intensity=0.1)
+    r = orc.ref
+    cv = 287.15 * 2.5   # UniformInitialCondition (Generic/InitialConditions.f90:154-170), dimensional
+    q = np.array([r["rho"], r["rho"] * r["V"], r["rho"] * r["V"] * np.sin(0.0),
+                  cv * r["rho"] * r["T"] + 0.5 * r["rho"] * r["V"] * r["V"]])
+    q = q / np.array([r["rho"], r["rho"] * r["a"], r["rho"] * r["a"], r["p"]])
+    orc.set_state(np.tile(q, orc.ndof // 4))
+    it, _ = orc.integrate(O.RK5, transient=False, t0=0.0, t_end=1.0, max_iter=20000, cfl=0.1, dt_cap=2.0,
+                          residual_target=1e-8)
+    assert it == golden["expected_iter"]
+    assert np.max(np.abs(orc.residuals() - np.array(golden["residuals"]))) <= 1e-11
