@@ -306,9 +306,11 @@ class L2Flush:
                 self.buf.fill_(self.val)
 
 
-def device_timed(ctxs, steps, warmup, dt, stream, world, dist, flush):
-    """Warm-up, then K steps, each between its own events on the launching stream with the
-    L2 flush (if any) outside the events; barrier + sync on both sides.  Returns (ms, launches)."""
+def device_timed(ctxs, steps, warmup, dt, stream, world, dist, flush, min_load_s=0.0):
+    """Warm-up (at least `warmup` steps and, when asked, at least `min_load_s` seconds of load so
+    that the clock sampler sees the GPU busy), then K steps, each between its own events on the
+    launching stream with the L2 flush (if any) outside the events; barrier + sync on both sides.
+    Returns (ms, launches)."""
     import torch
     import horses2d_b200 as hg
 
@@ -316,8 +318,14 @@ def device_timed(ctxs, steps, warmup, dt, stream, world, dist, flush):
         for c in ctxs:
             c["g"].time_step(hg.SCHEME_RK3, s * dt, dt)
 
-    for s in range(warmup):
+    t0 = time.perf_counter()
+    s = 0
+    while s < warmup or time.perf_counter() - t0 < min_load_s:
+        flush(stream)
         step(s)
+        s += 1
+        if s % 16 == 0:
+            torch.cuda.synchronize()
     torch.cuda.synchronize()
     launches0 = sum(c["g"].launch_count() for c in ctxs)
     if world > 1:
@@ -393,7 +401,7 @@ def main():
     # ---- device-resident timed region
     clocks = ClockSampler(local)
     clocks.start()
-    ms, launches = device_timed(ctxs, args.steps, args.warmup, dt, stream, world, dist, flush)
+    ms, launches = device_timed(ctxs, args.steps, args.warmup, dt, stream, world, dist, flush, min_load_s=2.0)
     clk = clocks.stop()
     # ---- per-kernel split (library CUDA-event timing, separate loop)
     split = kernel_split(ctxs, max(3, min(args.steps, 10)), dt, stream, flush)

@@ -10,4 +10,5 @@ from . import _lib as lib  # noqa: F401
 from .solver import GpuDGSEM, HorsesGpuError  # noqa: F401
 from ._lib import (NODES_LG, NODES_LGL, ROE, HLL, EXACT, LXF, INTERIOR, SCHEME_EULER, SCHEME_RK3,  # noqa: F401
                    SCHEME_RK5, PREC_FP64, PREC_FP32, BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL,
-                   BC_FARFIELD, BC_PRESSUREOUTLET, BR1, IP, SIPG, NIPG, IIPG)
+                   BC_FARFIELD, BC_PRESSUREOUTLET, BC_NEWDIRICHLET, BR1, IP, SIPG, NIPG, IIPG,
+                   AV_NONE, AV_LAPLACIAN, AV_PHYSICAL)

@@ -17,6 +17,8 @@ PREC_FP64, PREC_FP32 = 0, 1
 BR1, IP = 0, 1
 SIPG, NIPG, IIPG = 0, 1, 2
 BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL, BC_FARFIELD, BC_PRESSUREOUTLET = 1, 2, 3, 4, 5, 6
+BC_NEWDIRICHLET = 7
+AV_NONE, AV_LAPLACIAN, AV_PHYSICAL = 0, 1, 2
 
 I32P = C.POINTER(C.c_int32)
 F64P = C.POINTER(C.c_double)
@@ -27,12 +29,13 @@ class PhysicsDesc(C.Structure):
                 ("viscous", C.c_int32), ("ip_method", C.c_int32), ("sigma0_ip", C.c_double),
                 ("mach", C.c_double), ("reynolds", C.c_double), ("prandtl", C.c_double),
                 ("pressure_ref", C.c_double), ("temperature_ref", C.c_double), ("reynolds_length", C.c_double),
-                ("gamma", C.c_double), ("gas_R", C.c_double)]
+                ("gamma", C.c_double), ("gas_R", C.c_double), ("av_type", C.c_int32), ("av_intensity", C.c_double)]
 
 
 class BCDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("riemann", C.c_int32), ("state", C.c_double * 4), ("wall_T", C.c_double),
-                ("wall_v", C.c_double * 2), ("wall_type", C.c_int32), ("outflow_type", C.c_int32)]
+                ("wall_v", C.c_double * 2), ("wall_type", C.c_int32), ("outflow_type", C.c_int32),
+                ("nd_mode", C.c_int32), ("nd_outflow_total", C.c_int32)]
 
 
 class MeshDesc(C.Structure):

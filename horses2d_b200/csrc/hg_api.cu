@@ -5,69 +5,15 @@
 // Edge_LinkWithElements / Zone_LinkPeriodicZones) into per-element side tables,
 // upload everything once, and sequence the stage kernels of the low-storage
 // Runge-Kutta schemes (Approximation/DGTimeIntegrator.f90:263-365).
-#include "../../include/horses_gpu.h"
-#include "hg_stage.cuh"
-#include "hg_ns.cuh"
+#include "hg_ctx.h"
 #include "hg_spectral.h"
 
-#include <cuda_runtime.h>
 #include <cstring>
-#include <string>
-#include <vector>
-#include <stdexcept>
 #include <cmath>
 #include <algorithm>
 
-using namespace hg;
-
-struct hg_ctx {
-  std::string err;
-  int n_el = 0, N = 0, P = 0, node_type = 0, precision = 0, riemann = 0;
-  int64_t ndof = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  PhysConst pc{};
-  double mach = 0, gamma = 1.4;
-  // device buffers
-  int4* d_side = nullptr;
-  double* d_side_geo = nullptr;
-  double* d_vol_geo = nullptr;
-  double* d_mats = nullptr;
-  Zone* d_zones = nullptr;
-  double* d_Q = nullptr;
-  void* d_G = nullptr;
-  void* d_T[2] = {nullptr, nullptr};
-  double* d_QDot = nullptr;
-  double* d_resid = nullptr;      // per-CTA partial maxima of |QDot| of the last stage [grid][4]
-  double* d_resid_out = nullptr;  // reduced maxima [4]
-  double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
-  int cur = 0;                    // which trace buffer holds the current traces
-  bool affine = false;            // per-element constant metrics and per-side constant normals
-  bool ns = false, ip = false, grad_faces = false;   // Navier-Stokes kernels; interior penalty; SIPG/NIPG faces
-  double sigma0 = 0.0, epsilon = 0.0, temperature_ref = 273.15;
-  double* d_side_invh = nullptr;  // [n_el*4] invh of each side's edge
-  double* d_jac = nullptr;        // [n_el][NP] J (curved meshes, gradient faces)
-  void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
-  bool state_set = false;
-  int64_t launches = 0;
-  std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
-  double save_umax = 0.0, save_amax = 0.0;
-  // per-kernel timing (hg_profile): event pairs recorded around each launch
-  bool prof = false;
-  std::vector<cudaEvent_t> prof_pool;
-  size_t prof_used = 0;
-  std::vector<int> prof_kind;
-  double prof_ms[HG_KERNEL_KINDS] = {};
-  int64_t prof_n[HG_KERNEL_KINDS] = {};
-};
 
 static std::string g_create_err;
-
-#define HG_CUDA(call)                                                                           \
-  do {                                                                                          \
-    cudaError_t e_ = (call);                                                                    \
-    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
 
 static int fail(hg_ctx* c, const std::exception& ex) {
   if (c) c->err = ex.what();
@@ -85,107 +31,15 @@ static void free_ctx(hg_ctx* c) {
   if (!c) return;
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
-                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT};
+                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
+                  c->d_av_el, c->d_side_area, c->d_mu_av};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
-// ------------------------------------------------------------------ per-kernel timing
-static void prof_collect(hg_ctx* c) {
-  if (c->prof_used == 0) return;
-  HG_CUDA(cudaStreamSynchronize(c->stream));
-  for (size_t k = 0; k < c->prof_kind.size(); ++k) {
-    float ms = 0.f;
-    HG_CUDA(cudaEventElapsedTime(&ms, c->prof_pool[2 * k], c->prof_pool[2 * k + 1]));
-    c->prof_ms[c->prof_kind[k]] += ms;
-    c->prof_n[c->prof_kind[k]] += 1;
-  }
-  c->prof_kind.clear();
-  c->prof_used = 0;
-}
-
-static cudaEvent_t prof_event(hg_ctx* c) {
-  if (c->prof_used == c->prof_pool.size()) {
-    cudaEvent_t e;
-    HG_CUDA(cudaEventCreate(&e));
-    c->prof_pool.push_back(e);
-  }
-  return c->prof_pool[c->prof_used++];
-}
-
-// Launch f() on the context's stream; with timing on, bracket it by an event pair of kernel class `kind`.
-template <class F>
-static void timed(hg_ctx* c, int kind, F&& f) {
-  if (!c->prof) { f(); return; }
-  if (c->prof_used >= 8192) prof_collect(c);
-  cudaEvent_t a = prof_event(c), b = prof_event(c);
-  HG_CUDA(cudaEventRecord(a, c->stream));
-  f();
-  HG_CUDA(cudaEventRecord(b, c->stream));
-  c->prof_kind.push_back(kind);
-}
-
-// ------------------------------------------------------------------ launches
-// Prefer the largest shared-memory carve-out for a kernel (once per instantiation): the stage
-// kernels are latency-bound and their resident CTAs per SM are capped by shared memory otherwise.
-template <typename K>
-static void max_carveout(K kernel) {
-  HG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               int(cudaSharedmemCarveoutMaxShared)));
-}
 static int grid_for(const hg_ctx* c) {
   const int epb = c->ns ? epb_ns(c->P) : epb_for(c->P);
   return (c->n_el + epb - 1) / epb;
-}
-
-template <int P, typename real>
-static void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
-  constexpr int EPB = epb_for(P);
-  const int grid = (a.n_el + EPB - 1) / EPB;
-  static bool attr = false;
-  if (!attr) {
-    max_carveout(stage_kernel<P, EPB, real, true>);
-    max_carveout(stage_kernel<P, EPB, real, false>);
-    attr = true;
-  }
-  timed(c, HG_KERNEL_STAGE, [&] {
-    if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
-    else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
-  });
-  ++c->launches;
-}
-
-template <int P, typename real>
-static void launch_trace_P(hg_ctx* c) {
-  constexpr int EPB = epb_for(P);
-  const int grid = (c->n_el + EPB - 1) / EPB;
-  timed(c, HG_KERNEL_TRACE, [&] {
-    trace_kernel<P, EPB, real><<<grid, block_for(P), 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats,
-                                                                     static_cast<real*>(c->d_T[c->cur]));
-  });
-  ++c->launches;
-}
-
-template <int P, typename real, bool AFFINE, bool IP>
-static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
-  constexpr int EPB = epb_ns(P);
-  const int grid = (a.n_el + EPB - 1) / EPB;
-  static bool attr = false;
-  if (!attr) {
-    max_carveout(ns_gradient_kernel<P, EPB, real, AFFINE, IP>);
-    max_carveout(ns_stage_kernel<P, EPB, real, AFFINE, IP>);
-    attr = true;
-  }
-  timed(c, HG_KERNEL_GRADIENT,
-        [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });
-  timed(c, HG_KERNEL_STAGE, [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP><<<grid, block_ns(P), 0, c->stream>>>(a); });
-  c->launches += 2;
-}
-
-template <int P, typename real>
-static void launch_ns_P(hg_ctx* c, const NSArgs<real>& a) {
-  if (c->affine) { if (c->ip) launch_ns_PAI<P, real, true, true>(c, a); else launch_ns_PAI<P, real, true, false>(c, a); }
-  else { if (c->ip) launch_ns_PAI<P, real, false, true>(c, a); else launch_ns_PAI<P, real, false, false>(c, a); }
 }
 
 #define HG_DISPATCH_P(P_, FN, ...)                      \
@@ -231,6 +85,10 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.sigma0 = c->sigma0;
   a.epsilon = c->epsilon;
   a.pc = c->pc;
+  a.av = c->av;
+  a.av_el = c->d_av_el;
+  a.side_area = c->d_side_area;
+  a.mu_av = c->d_mu_av;
   HG_DISPATCH_P(c->P, launch_ns_P, c, a);
   if (update) c->cur ^= 1;
 }
@@ -324,7 +182,11 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   if (N < 1 || N > 8) throw std::runtime_error("polynomial order must be in 1..8");
   const int P = N + 1, NP = P * P;
   // the Navier-Stokes build with Re = 0 has mu = 0: its viscous terms vanish identically
-  c->ns = ph->navier_stokes != 0 && ph->reynolds != 0.0;
+  if (ph->av_type < HG_AV_NONE || ph->av_type > HG_AV_PHYSICAL) throw std::runtime_error("unknown artificial dissipation type");
+  c->av = ph->navier_stokes ? ph->av_type : HG_AV_NONE;   // artificial dissipation exists in the Navier-Stokes build
+  // the Navier-Stokes build with Re = 0 has mu = 0: its viscous terms vanish identically unless
+  // artificial dissipation is on
+  c->ns = ph->navier_stokes != 0 && (ph->reynolds != 0.0 || c->av != HG_AV_NONE);
   c->ip = ph->viscous == 1;
   c->grad_faces = c->ip && ph->ip_method != 2;
   c->sigma0 = ph->sigma0_ip;
@@ -339,7 +201,7 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->pc.cp = gamma / (gamma - 1.0);
   c->pc.cv = 1.0 / (gamma - 1.0);
   c->pc.invSqrtGammaMach = 1.0 / (std::sqrt(gamma) * ph->mach);
-  c->pc.mu = c->ns ? 1.0 / ph->reynolds : 0.0;
+  c->pc.mu = (ph->navier_stokes != 0 && ph->reynolds != 0.0) ? 1.0 / ph->reynolds : 0.0;
   c->pc.cpPr = c->pc.cp / ph->prandtl;
   c->pc.lambda = -2.0 / 3.0;
   c->temperature_ref = ph->temperature_ref;
@@ -355,6 +217,7 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   mats.insert(mats.end(), ops.D.begin(), ops.D.end());
   mats.insert(mats.end(), ops.dlbw0.begin(), ops.dlbw0.end());
   mats.insert(mats.end(), ops.dlbw1.begin(), ops.dlbw1.end());
+  mats.insert(mats.end(), ops.w.begin(), ops.w.end());
 
   // volume metrics
   std::vector<double> vg(size_t(E) * NP * 5);
@@ -375,6 +238,8 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
     zones[z].vw[1] = bcs[z].wall_v[1];
     zones[z].wall_type = bcs[z].wall_type;
     zones[z].outflow_type = bcs[z].outflow_type;
+    zones[z].nd_mode = bcs[z].nd_mode;
+    zones[z].nd_outflow_total = bcs[z].nd_outflow_total;
     if (bcs[z].riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
   }
 
@@ -420,7 +285,8 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
         case HG_BC_DIRICHLET:
         case HG_BC_VISCOUSWALL:
         case HG_BC_FARFIELD:
-        case HG_BC_PRESSUREOUTLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
+        case HG_BC_PRESSUREOUTLET:
+        case HG_BC_NEWDIRICHLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
         default: throw std::runtime_error("unknown boundary condition kind");
       }
       set_geo(L, sL, f, false);
@@ -489,6 +355,30 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->d_resid = dalloc<double>(size_t(grid_for(c)) * 4);
   c->d_resid_out = dalloc<double>(4);
   c->d_elmax = dalloc<double>(size_t(E) * 2);
+  if (c->av != HG_AV_NONE) {
+    // Edge_t%Area = sum_p dS(p) w(p) in the edge's node order (QuadMesh_Construct.incf:270-303), per side;
+    // per element Ceps sqrt(Volume)/(N+1) and the sum of the four areas (JumpsBasedElementViscosity)
+    if (!m->volume) throw std::runtime_error("artificial dissipation needs element volumes");
+    std::vector<double> area(size_t(E) * 4, 0.0), avel(size_t(E) * 2, 0.0);
+    for (int f = 0; f < m->n_edges; ++f) {
+      double A = 0.0;
+      for (int p = 0; p < P; ++p) A += m->edge_dS[size_t(f) * P + p] * ops.w[p];
+      const int L = m->edge_elem[2 * f], R = m->edge_elem[2 * f + 1];
+      area[size_t(L) * 4 + m->edge_side[2 * f] - 1] = A;
+      if (m->edge_marker[f] == 0) area[size_t(R) * 4 + m->edge_side[2 * f + 1] - 1] = A;
+    }
+    for (int e = 0; e < E; ++e) {
+      const double maxVisc = std::sqrt(m->volume[e]) / (N + 1);
+      avel[2 * size_t(e)] = ph->av_intensity * maxVisc;
+      const double* A = &area[size_t(e) * 4];
+      avel[2 * size_t(e) + 1] = A[0] + A[1] + A[2] + A[3];
+    }
+    c->d_av_el = dalloc<double>(avel.size());
+    c->d_side_area = dalloc<double>(area.size());
+    c->d_mu_av = dalloc<double>(size_t(E));
+    HG_CUDA(cudaMemcpy(c->d_av_el, avel.data(), avel.size() * sizeof(double), cudaMemcpyHostToDevice));
+    HG_CUDA(cudaMemcpy(c->d_side_area, area.data(), area.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   if (c->ns) {
     if (c->ip && !m->edge_invh) throw std::runtime_error("interior penalty needs edge_invh");
     c->d_side_invh = dalloc<double>(sinvh.size());

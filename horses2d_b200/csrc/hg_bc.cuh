@@ -12,6 +12,7 @@
 //   Dirichlet       Dirichlet.incf:155-300 (NAVIER_STOKES branch for uSB / vbc)
 //   Farfield        Farfield.incf:138-376
 //   PressureOutlet  PressureOutlet.incf:151-330
+//   newDirichlet    newDirichlet.incf (UpdateSolution; uSB aliases uB in the Navier-Stokes build)
 // Where the reference is undefined: far-field zones never set their viscous
 // condition (Farfield.incf), so the far field is Neumann here; the straight-edge
 // supersonic-outflow branch of the far field writes uB with swapped indices
@@ -22,7 +23,7 @@
 namespace hg {
 
 enum { BC_PERIODIC = 1, BC_DIRICHLET = 2, BC_EULERWALL = 3, BC_VISCOUSWALL = 4, BC_FARFIELD = 5,
-       BC_PRESSUREOUTLET = 6 };
+       BC_PRESSUREOUTLET = 6, BC_NEWDIRICHLET = 7 };
 enum { VBC_DIRICHLET = 1, VBC_NEUMANN = 2, VBC_ADIABATIC = 4 };
 
 struct Zone {
@@ -32,7 +33,81 @@ struct Zone {
   double vw[2];         // dimensionless wall velocity
   int wall_type;        // 1 isothermal, 2 adiabatic
   int outflow_type;     // 1 reflective, 2 partially non-reflective
+  int nd_mode;          // newDirichlet: 0 specify speed, 1 specify total pressure
+  int nd_outflow_total; // newDirichlet: outflow pressure 0 static, 1 total
 };
+
+// NORM2 of a 2-vector with a running scale (no overflow), as Fortran's intrinsic evaluates it
+template <typename real>
+__device__ __forceinline__ real norm2_scaled(real a, real b) {
+  real scale = real(0), ssq = real(1);
+  const real xs[2] = {a, b};
+#pragma unroll
+  for (int n = 0; n < 2; ++n) {
+    if (xs[n] != real(0)) {
+      const real ax = fabs(xs[n]);
+      if (scale < ax) { ssq = real(1) + ssq * (scale / ax) * (scale / ax); scale = ax; }
+      else ssq = ssq + (ax / scale) * (ax / scale);
+    }
+  }
+  return scale * sqrt_r(ssq);
+}
+
+// newDirichletBC_UpdateSolution at one node (out of line: pow would raise the register budget of
+// every kernel that inlines the zone switch).
+template <typename real>
+__device__ __noinline__ int new_dirichlet_state(const Phys<real>& ph, const Zone& z, const real* q, real nx, real ny,
+                                                real* uB, real* uSB) {
+  const real gm1 = ph.gm1, gamma = ph.gamma, cv = ph.cv;
+  const real cp = ph.cp;
+  const real zq[4] = {real(z.q[0]), real(z.q[1]), real(z.q[2]), real(z.q[3])};
+  const real uExt = zq[1] / zq[0], vExt = zq[2] / zq[0];
+  const real pExt = gm1 * (zq[3] - real(0.5) * (zq[1] * uExt + zq[2] * vExt));
+  const real MExtSq = (uExt * uExt + vExt * vExt) / (gamma * pExt) * zq[0];
+  const real sExt = pExt / pow_r(zq[0], gamma);
+  const real ptExt = pExt * pow_r(real(1) + real(0.5) * gm1 * MExtSq, cp);
+  const real rhoL = q[0], uL = q[1] / rhoL, vL = q[2] / rhoL;
+  const real vnL = uL * nx + vL * ny;
+  const real pL = gm1 * (q[3] - real(0.5) * (q[1] * uL + q[2] * vL));
+  const real aL = sqrt_r(gamma * pL / rhoL);
+  const real ML = sqrt_r(uL * uL + vL * vL) / aL;
+  int vbc;
+  if (vnL <= real(0)) {
+    if (ML > real(1)) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) uB[k] = zq[k];
+    } else {
+      const real pR = pL;
+      const real rhoR = pow_r(pR / sExt, real(1) / gamma);
+      const real aR = sqrt_r(gamma * pR / rhoR);
+      if (z.nd_mode == 0) {
+        uB[0] = zq[0]; uB[1] = zq[1]; uB[2] = zq[2];
+        uB[3] = cv * pR + real(0.5) * (uB[1] * uB[1] + uB[2] * uB[2]) / uB[0];
+      } else {
+        const real nrm = norm2_scaled(uExt, vExt);
+        const real MR = pR >= ptExt ? -sqrt_r(real(2) / gm1 * (pow_r(pR / ptExt, gm1 / gamma) - real(1)))
+                                    : sqrt_r(real(2) / gm1 * (pow_r(ptExt / pR, gm1 / gamma) - real(1)));
+        uB[0] = rhoR;
+        uB[1] = rhoR * aR * MR * (uExt / nrm);
+        uB[2] = rhoR * aR * MR * (vExt / nrm);
+        uB[3] = cv * pR + real(0.5) * rhoR * aR * aR * MR * MR;
+      }
+    }
+    vbc = VBC_DIRICHLET;
+  } else if (ML > real(1)) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) uB[k] = q[k];
+    vbc = VBC_NEUMANN;
+  } else {
+    uB[0] = q[0]; uB[1] = q[1]; uB[2] = q[2];
+    const real pb = z.nd_outflow_total ? ptExt : pExt;
+    uB[3] = cv * (real(2) * pb - pL) + real(0.5) * (uB[1] * uL + uB[2] * vL);
+    vbc = VBC_DIRICHLET;
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) uSB[k] = uB[k];
+  return vbc;
+}
 
 // Returns the inviscid ghost uB, the viscous state uSB and the viscous condition.
 template <typename real>
@@ -166,6 +241,8 @@ __device__ __forceinline__ int bc_states(const Phys<real>& ph, const Zone& z, co
       }
       return VBC_DIRICHLET;
     }
+    case BC_NEWDIRICHLET:
+      return new_dirichlet_state(ph, z, q, nx, ny, uB, uSB);
     default: {
 #pragma unroll
       for (int k = 0; k < 4; ++k) { uB[k] = q[k]; uSB[k] = q[k]; }

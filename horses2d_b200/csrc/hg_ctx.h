@@ -1,0 +1,112 @@
+// hg_ctx.h -- the library context and the launch helpers shared by the translation units of
+// libhorsesgpu.so (host API in hg_api.cu; kernel instantiations in hg_inst_*.cu, compiled in parallel).
+#pragma once
+#include "../../include/horses_gpu.h"
+#include "hg_stage.cuh"
+#include "hg_ns.cuh"
+
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include <stdexcept>
+
+using namespace hg;
+
+struct hg_ctx {
+  std::string err;
+  int n_el = 0, N = 0, P = 0, node_type = 0, precision = 0, riemann = 0;
+  int64_t ndof = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  PhysConst pc{};
+  double mach = 0, gamma = 1.4;
+  // device buffers
+  int4* d_side = nullptr;
+  double* d_side_geo = nullptr;
+  double* d_vol_geo = nullptr;
+  double* d_mats = nullptr;
+  Zone* d_zones = nullptr;
+  double* d_Q = nullptr;
+  void* d_G = nullptr;
+  void* d_T[2] = {nullptr, nullptr};
+  double* d_QDot = nullptr;
+  double* d_resid = nullptr;      // per-CTA partial maxima of |QDot| of the last stage [grid][4]
+  double* d_resid_out = nullptr;  // reduced maxima [4]
+  double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
+  int cur = 0;                    // which trace buffer holds the current traces
+  bool affine = false;            // per-element constant metrics and per-side constant normals
+  bool ns = false, ip = false, grad_faces = false;   // Navier-Stokes kernels; interior penalty; SIPG/NIPG faces
+  double sigma0 = 0.0, epsilon = 0.0, temperature_ref = 273.15;
+  double* d_side_invh = nullptr;  // [n_el*4] invh of each side's edge
+  int av = 0;                     // artificial dissipation HG_AV_*
+  double* d_av_el = nullptr;      // [n_el][2] Ceps sqrt(Volume)/(N+1), sum of edge areas
+  double* d_side_area = nullptr;  // [n_el*4] Area of each side's edge
+  double* d_mu_av = nullptr;      // [n_el] element artificial viscosity of the current stage
+  double* d_jac = nullptr;        // [n_el][NP] J (curved meshes, gradient faces)
+  void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
+  bool state_set = false;
+  int64_t launches = 0;
+  std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
+  double save_umax = 0.0, save_amax = 0.0;
+  // per-kernel timing (hg_profile): event pairs recorded around each launch
+  bool prof = false;
+  std::vector<cudaEvent_t> prof_pool;
+  size_t prof_used = 0;
+  std::vector<int> prof_kind;
+  double prof_ms[HG_KERNEL_KINDS] = {};
+  int64_t prof_n[HG_KERNEL_KINDS] = {};
+};
+
+#define HG_CUDA(call)                                                                           \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess) throw std::runtime_error(std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ------------------------------------------------------------------ per-kernel timing
+inline void prof_collect(hg_ctx* c) {
+  if (c->prof_used == 0) return;
+  HG_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t k = 0; k < c->prof_kind.size(); ++k) {
+    float ms = 0.f;
+    HG_CUDA(cudaEventElapsedTime(&ms, c->prof_pool[2 * k], c->prof_pool[2 * k + 1]));
+    c->prof_ms[c->prof_kind[k]] += ms;
+    c->prof_n[c->prof_kind[k]] += 1;
+  }
+  c->prof_kind.clear();
+  c->prof_used = 0;
+}
+
+inline cudaEvent_t prof_event(hg_ctx* c) {
+  if (c->prof_used == c->prof_pool.size()) {
+    cudaEvent_t e;
+    HG_CUDA(cudaEventCreate(&e));
+    c->prof_pool.push_back(e);
+  }
+  return c->prof_pool[c->prof_used++];
+}
+
+// Launch f() on the context's stream; with timing on, bracket it by an event pair of kernel class `kind`.
+template <class F>
+inline void timed(hg_ctx* c, int kind, F&& f) {
+  if (!c->prof) { f(); return; }
+  if (c->prof_used >= 8192) prof_collect(c);
+  cudaEvent_t a = prof_event(c), b = prof_event(c);
+  HG_CUDA(cudaEventRecord(a, c->stream));
+  f();
+  HG_CUDA(cudaEventRecord(b, c->stream));
+  c->prof_kind.push_back(kind);
+}
+
+// Prefer the largest shared-memory carve-out for a kernel (once per instantiation): the stage
+// kernels are latency-bound and their resident CTAs per SM are capped by shared memory otherwise.
+template <typename K>
+inline void max_carveout(K kernel) {
+  HG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               int(cudaSharedmemCarveoutMaxShared)));
+}
+
+// Per-order launches, explicitly instantiated in hg_inst_*.cu.
+template <int P, typename real> void launch_stage_P(hg_ctx* c, const StageArgs<real>& a);
+template <int P, typename real> void launch_trace_P(hg_ctx* c);
+template <int P, typename real> void launch_ns_P(hg_ctx* c, const NSArgs<real>& a);

@@ -1,0 +1,5 @@
+// hg_inst_ns64a.cu -- explicit instantiations: Navier-Stokes kernels, P = 2, 3, double.
+#include "hg_launch.cuh"
+
+template void launch_ns_P<2, double>(hg_ctx*, const NSArgs<double>&);
+template void launch_ns_P<3, double>(hg_ctx*, const NSArgs<double>&);

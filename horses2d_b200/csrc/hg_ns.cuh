@@ -42,6 +42,11 @@ struct NSArgs {
   int ip, grad_faces;       // interior penalty (else BR1); gradient-face terms (SIPG/NIPG)
   double sigma0, epsilon;
   PhysConst pc;
+  // artificial dissipation (jumps-based indicator)
+  int av;                   // 0 none, 1 Laplacian, 2 Physical
+  const double* av_el;      // [n_el][2] Ceps sqrt(Volume)/(N+1), sum of the 4 edge areas
+  const double* side_area;  // [n_el*4] Area of each side's edge
+  double* mu_av;            // [n_el] element viscosity of the current state (written by the gradient kernel)
 };
 
 __host__ __device__ constexpr int epb_ns(int P) {
@@ -53,7 +58,7 @@ __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) +
 template <int P, int EPB, typename real, bool AFFINE>
 struct NSTiles {
   static constexpr int NP = P * P, FT = 4 * P;
-  real mat[2 * NP + 6 * P];
+  real mat[2 * NP + 7 * P];   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w
   real Q[4][EPB][NP];
   real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : NP];   // Ja00 Ja01 Ja10 Ja11 J
   real dQ[2][4][EPB][NP];
@@ -175,7 +180,7 @@ template <int P, int EPB, typename real, bool AFFINE>
 __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s, int flat, int le,
                                            int tid, int e, bool active, real* geoE) {
   constexpr int NP = P * P;
-  for (int k = flat; k < 2 * NP + 6 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
+  for (int k = flat; k < 2 * NP + 7 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
   if (active) {
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
@@ -194,7 +199,79 @@ __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB
   }
 }
 
-template <int P, int EPB, typename real, bool AFFINE, bool IP>
+// JumpsBasedElementViscosity (Approximation/DGArtificialDissipation.f90:277-338) of each element of the
+// CTA into a.mu_av.  Edge jumps (Edge_ComputeJumps and the boundary/curved variants,
+// Mesh/QuadElement_EdgeProcedures.incf:1348-1619): sum over the edge nodes, in the edge's order, of
+// w (2 (QL-QR)/(QL+QR))^2 dS for rho and rhoE; boundary and periodic edges use the viscous boundary
+// state (uSB) and dS at their first node.  Uses s.face[0..1] as scratch; ends with a barrier.
+template <int P, int EPB, typename real, bool AFFINE>
+__device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+                                                  const Phys<real>& ph, int le, int tid, int e, bool active) {
+  constexpr int NP = P * P, FT = 4 * P;
+  const real* lb0 = s.mat + NP;
+  const real* lb1 = lb0 + P;
+  const real* wq = s.mat + 2 * NP + 6 * P;
+  if (active) {
+    for (int t = tid; t < FT; t += NP) {
+      const int sd_ = t / P, kk = t % P;
+      const int4 sd = a.side[size_t(e) * 4 + sd_];
+      const int kind = sd.y & 15;
+      const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+      real qo[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+      const size_t sbase = size_t(e) * 4 + sd_;
+      real qn0, qn3;
+      bool node0 = true;
+      if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
+        const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+        const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+        qn0 = tp[0];
+        qn3 = tp[3];
+        node0 = sd.z >= 0;   // periodic edges are boundary edges of the reference
+      } else {
+        const double* g3 = AFFINE ? a.side_geo + sbase * 3 : a.side_geo + (sbase * P + kk) * 3;
+        real uB[4], uS[4];
+        bc_states(ph, a.zones[sd.z], qo, real(g3[0]), real(g3[1]), uB, uS);
+        qn0 = uS[0];
+        qn3 = uS[3];
+      }
+      const real dSn = real(AFFINE ? a.side_geo[sbase * 3 + 2] : a.side_geo[(sbase * P + (node0 ? 0 : kk)) * 3 + 2]);
+      const real jr = real(2) * (qo[0] - qn0) / (qo[0] + qn0);
+      const real je = real(2) * (qo[3] - qn3) / (qo[3] + qn3);
+      s.face[0][le][t] = wq[kk] * jr * jr * dSn;
+      s.face[1][le][t] = wq[kk] * je * je * dSn;
+    }
+  }
+  __syncthreads();
+  if (active && tid == 0) {
+    real gr = real(0), ge = real(0);
+#pragma unroll
+    for (int sd_ = 0; sd_ < 4; ++sd_) {
+      const int fl = a.side[size_t(e) * 4 + sd_].y;
+      const bool rev = (fl & 15) == SIDE_RIGHT && (fl & SIDE_REVERSED);
+      real sr = real(0), se = real(0);
+      for (int n = 0; n < P; ++n) {
+        const int kk = rev ? (P - 1 - n) : n;
+        sr = sr + s.face[0][le][sd_ * P + kk];
+        se = se + s.face[1][le][sd_ * P + kk];
+      }
+      gr = gr + sr;
+      ge = ge + se;
+    }
+    double gk = double(gr > ge ? gr : ge) / a.av_el[2 * size_t(e) + 1];
+    gk = gk > 1.0e-8 ? log10(gk) : -1.7976931348623157e308;
+    const double k = 5.0;
+    const double s0 = log10(1.0 / ((P * P) * double(P * P))) + 1.0;
+    double G;
+    if (gk < s0 - k) G = 0.0;
+    else if (gk < s0 + k) G = 0.5 * sin(0.5 * 3.141592653589793238462643 * (gk - s0) / k) + 0.5;
+    else G = 1.0;
+    a.mu_av[e] = a.av_el[2 * size_t(e)] * G;
+  }
+}
+
+template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
 __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
   __shared__ NSTiles<P, EPB, real, AFFINE> s;
@@ -208,6 +285,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a
   __syncthreads();
   element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
   __syncthreads();
+  if (AV) element_viscosity<P, EPB, real, AFFINE>(a, s, ph, le, tid, e, active);
   if (!active) return;
   const real* lb0 = s.mat + NP;
   const real* lb1 = lb0 + P;
@@ -222,7 +300,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a
   }
 }
 
-template <int P, int EPB, typename real, bool AFFINE, bool IP>
+template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
 __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
   constexpr int NW = block_ns(P) / 32;
@@ -235,6 +313,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
   const real mu = ph.mu;
   real geoE[5];
   load_tiles(a, s, flat, le, tid, e, active, geoE);
+  const real mu_e = (AV && active) ? real(a.mu_av[e]) : real(0);
   __syncthreads();
   element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
   const int i = tid % P, j = tid / P;
@@ -255,9 +334,32 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
     for (int k = 0; k < 4; ++k) { q[k] = s.Q[k][le][tid]; gx[k] = s.dQ[0][k][le][tid]; gy[k] = s.dQ[1][k][le][tid]; }
     inviscid_flux(ph, q, fi, gi);
     viscous_flux(ph, q, gx, gy, fv, gv);
+    const real mu_v = (AV && a.av == 2) ? mu + mu_e : mu;
+    real ax[4] = {real(0), real(0), real(0), real(0)}, ay[4] = {real(0), real(0), real(0), real(0)};
+    if (AV && a.av == 1) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
+      if (IP) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { ax[k] = gx[k]; ay[k] = gy[k]; }
+      } else {
+        const real* D = s.mat + NP + 4 * P;   // D follows hatD, lb0, lb1, lbw0, lbw1
+        const real iJl = AFFINE ? geoE[4] : real(1) / s.Ja[4][le][tid];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          real dxi = real(0), deta = real(0);
+#pragma unroll
+          for (int l = 0; l < P; ++l) {
+            dxi += D[i * P + l] * s.Q[k][le][j * P + l];
+            deta += D[j * P + l] * s.Q[k][le][l * P + i];
+          }
+          ax[k] = (dxi * Ja00 + deta * Ja01) * iJl;
+          ay[k] = (dxi * Ja10 + deta * Ja11) * iJl;
+        }
+      }
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const real f = fi[k] - mu * fv[k], g = gi[k] - mu * gv[k];
+      real f = fi[k] - mu_v * fv[k], g = gi[k] - mu_v * gv[k];
+      if (AV && a.av == 1) { f = f - mu_e * ax[k]; g = g - mu_e * ay[k]; }
       s.Fc[k][le][tid] = f * Ja00 + g * Ja10;
       s.Gc[k][le][tid] = f * Ja01 + g * Ja11;
     }
@@ -280,7 +382,14 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
       const real invh = real(a.side_invh[size_t(e) * 4 + sd_]);
-      const real penalty = IP ? real(a.sigma0) * mu * real(P - 1) * real(P - 1) * invh : real(0);
+      // edge viscosity (JumpsBasedEdgeViscosity): mean over the edge's elements; boundary and
+      // periodic edges have one element
+      real mu_ed = mu_e;
+      if (AV && (kind == SIDE_LEFT || kind == SIDE_RIGHT) && sd.z < 0)
+        mu_ed = (real(a.mu_av[sd.x >> 2]) + mu_e) / real(2);
+      const real mu_f = (AV && a.av == 2) ? mu + mu_ed : mu;
+      const real lap = (AV && a.av == 1) ? mu_ed * real(a.side_area[size_t(e) * 4 + sd_]) : real(0);
+      const real penalty = IP ? real(a.sigma0) * mu_f * real(P - 1) * real(P - 1) * invh : real(0);
       real F[4], Gx[4] = {real(0), real(0), real(0), real(0)}, Gy[4] = {real(0), real(0), real(0), real(0)};
       if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
         const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
@@ -300,9 +409,14 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
         viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          real fv = real(0.5) * (mu * FLx[k] + mu * FRx[k]) * nx + real(0.5) * (mu * FLy[k] + mu * FRy[k]) * ny;
+          real fv = real(0.5) * (mu_f * FLx[k] + mu_f * FRx[k]) * nx + real(0.5) * (mu_f * FLy[k] + mu_f * FRy[k]) * ny;
           if (IP) fv = fv - penalty * (QL[k] - QR[k]);
-          F[k] = (Fi[k] - fv) * dS;
+          if (AV) {
+            const real fa = -(lap * (QL[k] - QR[k]));
+            F[k] = (Fi[k] - fv - fa) * dS;
+          } else {
+            F[k] = (Fi[k] - fv) * dS;
+          }
           if (right) F[k] = -F[k];
         }
         if (IP && a.grad_faces) {
@@ -310,7 +424,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
 #pragma unroll
           for (int k = 0; k < 4; ++k) { fgx[k] = (QL[k] - QR[k]) * nx; fgy[k] = (QL[k] - QR[k]) * ny; }
           viscous_flux(ph, right ? QR : QL, fgx, fgy, Ax, Ay);
-          const real cf = (right ? real(-0.5) : real(0.5)) * real(a.epsilon) * mu;
+          const real cf = (right ? real(-0.5) : real(0.5)) * real(a.epsilon) * mu_f;
 #pragma unroll
           for (int k = 0; k < 4; ++k) { Gx[k] = cf * Ax[k] * dS; Gy[k] = cf * Ay[k] * dS; }
         }
@@ -334,7 +448,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
           else viscous_flux(ph, qo, gox, goy, Fx, Fy);
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
-            fv[k] = (mu * Fx[k]) * nx + (mu * Fy[k]) * ny;
+            fv[k] = (mu_f * Fx[k]) * nx + (mu_f * Fy[k]) * ny;
             if (IP) fv[k] = fv[k] - penalty * (qo[k] - uSB[k]);
             fv[k] = fv[k] * dS;
           }
@@ -344,13 +458,13 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
             for (int k = 0; k < 4; ++k) { fgx[k] = (qo[k] - uSB[k]) * nx; fgy[k] = (qo[k] - uSB[k]) * ny; }
             if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, fgx, fgy, Ax, Ay);
             else viscous_flux(ph, qo, fgx, fgy, Ax, Ay);
-            const real cf = real(a.epsilon) * mu;
+            const real cf = real(a.epsilon) * mu_f;
 #pragma unroll
             for (int k = 0; k < 4; ++k) { Gx[k] = (cf * Ax[k]) * dS; Gy[k] = (cf * Ay[k]) * dS; }
           }
         }
 #pragma unroll
-        for (int k = 0; k < 4; ++k) F[k] = Fi[k] - fv[k];
+        for (int k = 0; k < 4; ++k) F[k] = AV ? Fi[k] - fv[k] - (-(lap * (qo[k] - uSB[k]))) * dS : Fi[k] - fv[k];
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];

@@ -34,6 +34,9 @@ struct Phys {
 template <typename real> __device__ __forceinline__ real sqrt_r(real x);
 template <> __device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
 template <> __device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
+template <typename real> __device__ __forceinline__ real pow_r(real x, real y);
+template <> __device__ __forceinline__ double pow_r(double x, double y) { return pow(x, y); }
+template <> __device__ __forceinline__ float pow_r(float x, float y) { return powf(x, y); }
 
 template <typename real>
 __device__ __forceinline__ void inviscid_flux(const Phys<real>& ph, const real* u, real* f, real* g) {

@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(block_for(P)) trace_kernel(int n_el, const dou
 }
 
 // Max over the per-CTA residual partials: out[k] = max_b part[b*4+k] (NaN kept).
-__global__ void residual_reduce_kernel(int nblocks, const double* part, double* out) {
+static __global__ void residual_reduce_kernel(int nblocks, const double* part, double* out) {
   __shared__ double s[4][256];
   double m[4] = {0.0, 0.0, 0.0, 0.0};
   for (int b = threadIdx.x; b < nblocks; b += blockDim.x)

@@ -40,7 +40,8 @@ class GpuDGSEM:
 
     def __init__(self, mesh, *, mach, node_type=L.NODES_LGL, riemann=L.ROE, bcs=(), precision=L.PREC_FP64,
                  reynolds=0.0, prandtl=0.72, navier_stokes=0, viscous=L.BR1, ip_method=L.SIPG, sigma0_ip=1.0,
-                 pressure_ref=101325.0, temperature_ref=273.15, reynolds_length=1.0, gamma=1.4):
+                 pressure_ref=101325.0, temperature_ref=273.15, reynolds_length=1.0, gamma=1.4, av_type=L.AV_NONE,
+                 av_intensity=1.0):
         lib = L.load()
         self._keep = []
         md = L.MeshDesc()
@@ -74,7 +75,7 @@ class GpuDGSEM:
         ph = L.PhysicsDesc(node_type=node_type, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous,
                            ip_method=ip_method, sigma0_ip=sigma0_ip, mach=mach, reynolds=reynolds,
                            prandtl=prandtl, pressure_ref=pressure_ref, temperature_ref=temperature_ref, reynolds_length=reynolds_length, gamma=gamma,
-                           gas_R=287.15)
+                           gas_R=287.15, av_type=av_type, av_intensity=av_intensity)
         barr = (L.BCDesc * max(1, len(bcs)))()
         for k, b in enumerate(bcs):
             barr[k].type = b["type"]
@@ -87,6 +88,8 @@ class GpuDGSEM:
             barr[k].wall_v[0], barr[k].wall_v[1] = wv[0], wv[1]
             barr[k].wall_type = b.get("wall_type", 2)
             barr[k].outflow_type = b.get("outflow_type", 1)
+            barr[k].nd_mode = b.get("mode", 0)
+            barr[k].nd_outflow_total = b.get("outflow_total", 0)
         self._keep.append(barr)
         h = C.c_void_p()
         rc = lib.hg_create(C.byref(md), C.byref(ph), barr, len(bcs), precision, C.byref(h))

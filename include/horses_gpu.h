@@ -40,7 +40,9 @@ enum { HG_SCHEME_EULER = 0, HG_SCHEME_RK3 = 1, HG_SCHEME_RK5 = 2 }; /* DGTimeInt
 enum { HG_PREC_FP64 = 0, HG_PREC_FP32 = 1 };
 /* Boundary-condition kinds, numbered as Generic/Defines.h PERIODIC_BC .. PRESSUREOUTLET_BC. */
 enum { HG_BC_PERIODIC = 1, HG_BC_DIRICHLET = 2, HG_BC_EULERWALL = 3, HG_BC_VISCOUSWALL = 4,
-       HG_BC_FARFIELD = 5, HG_BC_PRESSUREOUTLET = 6 };
+       HG_BC_FARFIELD = 5, HG_BC_PRESSUREOUTLET = 6, HG_BC_NEWDIRICHLET = 7 };
+/* Artificial dissipation (Approximation/DGArtificialDissipation.f90), jumps-based indicator. */
+enum { HG_AV_NONE = 0, HG_AV_LAPLACIAN = 1, HG_AV_PHYSICAL = 2 };
 
 /* Physics and discretization choices (Setup_t, PhysicsNS InitializePhysics). */
 typedef struct {
@@ -54,6 +56,8 @@ typedef struct {
   double  pressure_ref, temperature_ref, reynolds_length;
   double  gamma;           /* 1.4 for the reference's "Air" */
   double  gas_R;           /* 287.15 */
+  int32_t av_type;         /* HG_AV_*: "Artificial dissipation (0/1)" + "Artificial dissipation type" */
+  double  av_intensity;    /* "Artificial dissipation intensity" (Ceps, default 1) */
 } hg_physics_desc;
 
 /* One boundary zone (marker), as constructed by the reference's BC classes
@@ -68,6 +72,8 @@ typedef struct {
   double  wall_v[2];       /* viscous wall velocity, dimensionless: sqrt(gamma) * Mach * direction */
   int32_t wall_type;       /* 1 isothermal, 2 adiabatic */
   int32_t outflow_type;    /* pressure outlet: 1 reflective, 2 partially non-reflective (default) */
+  int32_t nd_mode;         /* newDirichlet "Mode": 0 specify speed (default), 1 specify total pressure */
+  int32_t nd_outflow_total;/* newDirichlet "Outflow pressure": 0 static (default), 1 total */
 } hg_bc_desc;
 
 /* The mesh after the reference's construction (QuadMesh_t after
