@@ -23,6 +23,11 @@ Workloads (synthetic inputs with the configurations' shapes; seeds fixed):
              M 0.5 at 45 deg, LGL nodes, Roe, packed by polynomial order into one
              element list per order; FP32 bulk with FP64 state accumulator by default.
   box512   : one 512 x 512 periodic vortex box, N = 4, LGL, Roe, FP64 (profiling case).
+  shock    : the learned-sensor case: [0,10] x [0,1], 512 x 64 elements, N = 3, Mach-3 normal shock
+             with an upstream entropy wave (amplitude 0.2), HLL, Re = 0, Laplacian artificial
+             dissipation; the sensor network is first trained on the GPU on 2 x 100 solver snapshots
+             (shock position +-0.5, amplitude 0.1-0.3, seed 20261203); value = FP32 bulk + learned
+             sensor, beside the plain FP64 path with the modal-decay sensor.
 Multi-GPU: independent replicas (the workload does not exchange data), weak scaling.
 """
 import argparse
@@ -41,7 +46,7 @@ sys.path.insert(0, ROOT)
 
 SEED = 20261203
 L2_BYTES = 126 * 2 ** 20
-CONFIGS = ("cylinder", "vortex16", "ensemble", "box512")
+CONFIGS = ("cylinder", "vortex16", "ensemble", "box512", "shock")
 
 
 def peaks():
@@ -204,6 +209,22 @@ class CpuArm:
         self.config = config
         self.threads = threads or os.cpu_count() or 1
         self.steps_done = []
+        if config == "shock":
+            from horses2d_b200 import sensor as S
+            O.lib().or_set_threads(self.threads)
+            (r1, u1, p1), (r2, u2, p2) = S.rankine_hugoniot(3.0)
+            bcs = [dict(type=O.BC_EULERWALL), dict(type=O.BC_EULERWALL), dict(type=O.BC_DIRICHLET),
+                   dict(type=O.BC_NEWDIRICHLET, pressure=101325.0 * p2, temperature=273.15 * p2 / r2,
+                        mach=u2 / np.sqrt(1.4 * p2 / r2))]
+            o = O.Oracle(hmesh.cartesian(512, 64, 0.0, 10.0, 0.0, 1.0), 3, nodes=O.LG, riemann=O.HLL, mach=3.0,
+                         reynolds=0.0, navier_stokes=1, viscous=O.IP, ip_method=0, sigma0_ip=10.0, bcs=bcs,
+                         av_type=O.AV_LAPLACIAN, av_intensity=1.0, av_indicator=O.IND_MODAL)
+            x = o.coords()[:, 0]
+            up = x < 5.0
+            o.set_state(S.conservative(np.where(up, 1.0 + 0.2 * np.sin(5.0 * x), r2), np.where(up, u1, u2),
+                                       np.where(up, 1.0, p2)).ravel())
+            self.orcs = [(o, o.estimate_dt(0.1, 1.0))]
+            return
         if config == "cylinder":
             O.lib().or_set_threads(self.threads)
             o = O.Oracle(cylinder_mesh(), 5, nodes=O.LG, riemann=O.ROE, mach=0.2, reynolds=100.0, prandtl=0.72,
@@ -240,10 +261,11 @@ class CpuArm:
     def sample(self, budget_s):
         """(DOF-stage/s, cores, description) of ~budget_s seconds of RK3 steps."""
         from concurrent.futures import ThreadPoolExecutor
-        if self.config == "cylinder":
+        if self.config in ("cylinder", "shock"):
             n, el, steps = self._run(self.orcs[0], budget_s, False)
-            return (n / el, self.threads, f"full cylinder workload (NDOF {self.orcs[0][0].ndof}), {steps} RK3 steps "
-                    f"in {el:.1f} s, OpenMP element loops on {self.threads} threads")
+            return (n / el, self.threads, f"full {self.config} workload (NDOF {self.orcs[0][0].ndof}), {steps} RK3 "
+                    f"steps in {el:.1f} s, OpenMP element loops on {self.threads} threads, FP64"
+                    + (", modal-decay sensor" if self.config == "shock" else ""))
         with ThreadPoolExecutor(max_workers=self.threads) as ex:
             res = list(ex.map(lambda a: self._run(a, budget_s, True), self.orcs))
         rate = sum(r[0] / r[1] for r in res)
@@ -364,6 +386,104 @@ def kernel_split(ctxs, steps, dt, stream, flush):
     return tot
 
 
+def run_shock(args, rank, world, local, dist):
+    """The learned-sensor workload: train, then time FP32 + learned beside FP64 + modal."""
+    import torch
+    import horses2d_b200 as hg
+    from horses2d_b200 import sensor as S
+    nx, ny, N = 512, 64, 3
+    t0 = time.perf_counter()
+    params, lo, hi, info = S.train_two_rounds(100, SEED, nx=nx, ny=ny, N=N, steps=100, epochs=30, batch=4096)
+    train_s = time.perf_counter() - t0
+    desc, kw = S.shock_case(nx, ny, N)
+    Q0 = S.shock_state(desc, S.snap_to_face(5.0, nx), 0.2)
+    stream = torch.cuda.Stream()
+    parts = [(desc, Q0, N, 1, kw, 0.1)]
+
+    def ctx(prec, learned):
+        c = make_contexts(parts, prec, stream)
+        if learned:
+            c[0]["g"].set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
+        else:
+            c[0]["g"].set_sensor(hg.SENSOR_MODAL)
+        return c
+
+    c32, c64 = ctx(hg.PREC_FP32, True), ctx(hg.PREC_FP64, False)
+    ndof = c32[0]["g"].ndof
+    dt = info["dt"]
+    flush = L2Flush(ndof * 8 * 3 < 2 * L2_BYTES)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms32, launches = device_timed(c32, args.steps, args.warmup, dt, stream, world, dist, flush, min_load_s=2.0)
+    clk = clocks.stop()
+    ms64, _ = device_timed(c64, args.steps, args.warmup, dt, stream, world, dist, flush)
+    split = kernel_split(c32, max(3, min(args.steps, 10)), dt, stream, flush)
+    # accuracy: FP32 + learned against FP64 + learned from the same state, and the sensors' statistics
+    c64l = ctx(hg.PREC_FP64, True)
+    steps_acc = 200
+    for c in (c32[0], c64[0], c64l[0]):
+        c["g"].set_state(Q0)
+        c["g"].time_steps(hg.SCHEME_RK3, steps_acc, 0.0, dt)
+    Q32, Q64, Q64l = (c["g"].state() for c in (c32[0], c64[0], c64l[0]))
+    rho_err = float(np.linalg.norm(Q32[0::4] - Q64l[0::4]) / np.linalg.norm(Q64l[0::4]))
+    _, out32 = c32[0]["g"].sensor_eval()
+    _, out64 = c64[0]["g"].sensor_eval()
+    m_learned = S.shock_metrics(Q32, out32[:, 3], nx, ny)
+    m_modal = S.shock_metrics(Q64, out64[:, 3], nx, ny)
+    # end to end through the public API with host buffers (FP32 + learned)
+    g = c32[0]["g"]
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    g.set_state(c32[0]["Qh"].numpy())
+    res = np.zeros(4)
+    for s in range(args.steps):
+        g.time_step(hg.SCHEME_RK3, s * dt, dt)
+        res = np.maximum(res, g.residuals())
+    Qe = g.state()
+    e2e_ms = (time.perf_counter() - t1) * 1e3
+    if not (np.all(np.isfinite(Qe)) and np.all(np.isfinite(res))):
+        raise SystemExit("non-finite state after the timed steps")
+    value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
+    value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
+    bpd = stage_bytes_per_dof("shock", True, True) + 0.0
+    st_ms, st_n = split["stage"]
+    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
+    achieved = bpd * ndof / avg_stage_s / 1e9
+    peak, peak_kind = peaks()
+    total_split = sum(v[0] for v in split.values()) or 1.0
+    line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
+            "config": {"workload": "shock", "ndof": ndof, "mesh": f"{nx}x{ny}", "N": N, "precision": "fp32",
+                       "sensor": "learned (MLP 16-32-32-1) with modal fallback", "scheme": "Williamson RK3",
+                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
+                              if flush.buf is not None else "inputs larger than L2"),
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": ndof * 3 * args.steps / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
+                    "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
+            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
+            "fp64_plain_modal": {"value": value64, "ms_per_step": ms64 / args.steps, "speedup_fp32_learned": ms64 / ms32},
+            "accuracy": {"rel_l2_density_fp32_vs_fp64_after_200_steps": rho_err},
+            "sensor": {"training_s": train_s, "samples": info["samples"], "snapshots": 200,
+                       "final_loss": info["loss_round2"][-1], "learned": m_learned, "modal": m_modal,
+                       "troubled_cell_disagreement": S.disagreement(out32[:, 0], out32[:, 3]),
+                       "ood_elements": int(out32[:, 2].sum())},
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, cores, sample = CpuArm("shock").sample(12.0)
+        line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for c in c32 + c64 + c64l:
+        c["g"].close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -386,6 +506,8 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    if args.config == "shock":
+        return run_shock(args, rank, world, local, dist)
     precision = args.precision or ("fp32" if args.config == "ensemble" else "fp64")
     prec = hg.PREC_FP32 if precision == "fp32" else hg.PREC_FP64
     parts = build_parts(args.config)

@@ -32,7 +32,7 @@ static void free_ctx(hg_ctx* c) {
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
-                  c->d_av_el, c->d_side_area, c->d_mu_av};
+                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
@@ -89,6 +89,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.av_el = c->d_av_el;
   a.side_area = c->d_side_area;
   a.mu_av = c->d_mu_av;
+  a.sensor = sensor_args(c);
   HG_DISPATCH_P(c->P, launch_ns_P, c, a);
   if (update) c->cur ^= 1;
 }
@@ -218,6 +219,9 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   mats.insert(mats.end(), ops.dlbw0.begin(), ops.dlbw0.end());
   mats.insert(mats.end(), ops.dlbw1.begin(), ops.dlbw1.end());
   mats.insert(mats.end(), ops.w.begin(), ops.w.end());
+  mats.insert(mats.end(), ops.Vinv.begin(), ops.Vinv.end());
+  c->sensor_s0 = std::log10(1.0 / std::pow(double(N + 1), 4.0));   // modal ramp defaults
+  c->sensor_kappa = 1.0;
 
   // volume metrics
   std::vector<double> vg(size_t(E) * NP * 5);
@@ -563,6 +567,73 @@ extern "C" int hg_kernel_times(hg_ctx* c, double* ms, int64_t* launches, int32_t
       if (ms) ms[k] = c->prof_ms[k];
       if (launches) launches[k] = c->prof_n[k];
     }
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_set_sensor(hg_ctx* c, int32_t kind, double s0, double kappa, const float* mlp, const float* lo,
+                             const float* hi) {
+  try {
+    if (kind < HG_SENSOR_JUMPS || kind > HG_SENSOR_LEARNED) throw std::runtime_error("unknown sensor kind");
+    if (kind == HG_SENSOR_LEARNED && !mlp) throw std::runtime_error("the learned sensor needs its weights");
+    if ((lo == nullptr) != (hi == nullptr)) throw std::runtime_error("feature box needs both bounds");
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    if (!std::isnan(s0)) c->sensor_s0 = s0;
+    if (!std::isnan(kappa)) {
+      if (!(kappa > 0.0)) throw std::runtime_error("sensor ramp half width must be positive");
+      c->sensor_kappa = kappa;
+    }
+    auto put = [](float*& d, const float* h, size_t n) {
+      if (!h) { if (d) { cudaFree(d); d = nullptr; } return; }
+      if (!d) d = dalloc<float>(n);
+      HG_CUDA(cudaMemcpy(d, h, n * sizeof(float), cudaMemcpyHostToDevice));
+    };
+    put(c->d_mlp, mlp, HG_MLP_PARAMS);
+    put(c->d_feat_lo, lo, HG_SENSOR_FEATURES);
+    put(c->d_feat_hi, hi, HG_SENSOR_FEATURES);
+    c->sensor_kind = kind;
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+template <int P, typename real>
+static void sensor_eval_dispatch(hg_ctx* c, float* f, double* o) { launch_sensor_eval_P<P, real>(c, f, o); }
+
+extern "C" int hg_sensor_eval(hg_ctx* c, float* features, double* out) {
+  try {
+    require_state(c);
+    float* df = features ? dalloc<float>(size_t(c->n_el) * HG_SENSOR_FEATURES) : nullptr;
+    double* dout = out ? dalloc<double>(size_t(c->n_el) * 4) : nullptr;
+    try {
+      if (c->precision == HG_PREC_FP32) {
+        using real = float;
+        HG_DISPATCH_P(c->P, sensor_eval_dispatch, c, df, dout);
+      } else {
+        using real = double;
+        HG_DISPATCH_P(c->P, sensor_eval_dispatch, c, df, dout);
+      }
+      HG_CUDA(cudaGetLastError());
+      if (df) HG_CUDA(cudaMemcpyAsync(features, df, size_t(c->n_el) * HG_SENSOR_FEATURES * sizeof(float),
+                                      cudaMemcpyDeviceToHost, c->stream));
+      if (dout) HG_CUDA(cudaMemcpyAsync(out, dout, size_t(c->n_el) * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                        c->stream));
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+    } catch (...) {
+      if (df) cudaFree(df);
+      if (dout) cudaFree(dout);
+      throw;
+    }
+    if (df) cudaFree(df);
+    if (dout) cudaFree(dout);
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_element_viscosity(hg_ctx* c, double* mu) {
+  try {
+    if (!c->d_mu_av) throw std::runtime_error("artificial dissipation is off for this context");
+    HG_CUDA(cudaMemcpyAsync(mu, c->d_mu_av, size_t(c->n_el) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }

@@ -42,6 +42,12 @@ struct hg_ctx {
   double* d_av_el = nullptr;      // [n_el][2] Ceps sqrt(Volume)/(N+1), sum of edge areas
   double* d_side_area = nullptr;  // [n_el*4] Area of each side's edge
   double* d_mu_av = nullptr;      // [n_el] element artificial viscosity of the current stage
+  // shock sensor (hg_sensor.cuh): indicator kind, modal ramp, learned-sensor weights and feature box
+  int sensor_kind = 0;
+  double sensor_s0 = 0.0, sensor_kappa = 1.0;
+  float* d_mlp = nullptr;
+  float* d_feat_lo = nullptr;
+  float* d_feat_hi = nullptr;
   double* d_jac = nullptr;        // [n_el][NP] J (curved meshes, gradient faces)
   void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
   bool state_set = false;
@@ -110,3 +116,15 @@ inline void max_carveout(K kernel) {
 template <int P, typename real> void launch_stage_P(hg_ctx* c, const StageArgs<real>& a);
 template <int P, typename real> void launch_trace_P(hg_ctx* c);
 template <int P, typename real> void launch_ns_P(hg_ctx* c, const NSArgs<real>& a);
+template <int P, typename real> void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out);
+
+inline SensorArgs sensor_args(const hg_ctx* c) {
+  SensorArgs s;
+  s.kind = c->sensor_kind;
+  s.s0 = c->sensor_s0;
+  s.kappa = c->sensor_kappa;
+  s.mlp = c->d_mlp;
+  s.lo = c->d_feat_lo;
+  s.hi = c->d_feat_hi;
+  return s;
+}

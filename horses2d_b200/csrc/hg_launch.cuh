@@ -65,3 +65,48 @@ void launch_ns_P(hg_ctx* c, const NSArgs<real>& a) {
     }
   }
 }
+
+// Sensor indicators of the resident state, per element: features [n_el][16] (optional) and
+// {modal G, learned G, out-of-distribution flag, G used} [n_el][4] (optional).  The learned G is
+// evaluated whenever weights are set.
+template <int P, int EPB, typename real>
+__global__ void __launch_bounds__(block_ns(P)) sensor_eval_kernel(int n_el, const double* Q, const double* mats,
+                                                                  SensorArgs sa, PhysConst pc, float* feat,
+                                                                  double* out) {
+  constexpr int NP = P * P;
+  __shared__ real sQ[4][EPB][NP];
+  __shared__ real sV[NP];
+  __shared__ real scr[EPB][sensor_scratch(P)];
+  const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
+  const int e = blockIdx.x * EPB + le;
+  const bool active = le < EPB && e < n_el;
+  for (int k = flat; k < NP; k += blockDim.x) sV[k] = real(mats[2 * NP + 7 * P + k]);
+  if (active) {
+    const double* q = Q + (size_t(e) * NP + tid) * 4;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) sQ[k][le][tid] = real(q[k]);
+  }
+  __syncthreads();
+  Phys<real> ph;
+  ph.load(pc);
+  SensorArgs s2 = sa;
+  if (sa.mlp) s2.kind = SENSOR_LEARNED;
+  SensorOut so = element_sensor<P, EPB, real>(s2, ph, sQ, scr[le < EPB ? le : 0], sV, le, tid, active,
+                                             (active && feat) ? feat + size_t(e) * MLP_IN : nullptr);
+  if (active && tid == 0 && out) {
+    const double g = sa.kind == SENSOR_LEARNED ? so.g : (sa.kind == SENSOR_MODAL ? so.g_modal : -1.0);
+    out[size_t(e) * 4 + 0] = so.g_modal;
+    out[size_t(e) * 4 + 1] = sa.mlp ? so.g_learned : -1.0;
+    out[size_t(e) * 4 + 2] = so.ood;
+    out[size_t(e) * 4 + 3] = g;
+  }
+}
+
+template <int P, typename real>
+void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out) {
+  constexpr int EPB = epb_ns(P);
+  const int grid = (c->n_el + EPB - 1) / EPB;
+  sensor_eval_kernel<P, EPB, real><<<grid, block_ns(P), 0, c->stream>>>(c->n_el, c->d_Q, c->d_mats, sensor_args(c),
+                                                                         c->pc, feat, out);
+  ++c->launches;
+}

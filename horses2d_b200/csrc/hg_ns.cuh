@@ -17,6 +17,7 @@
 //        and the new Q traces.
 #pragma once
 #include "hg_stage.cuh"
+#include "hg_sensor.cuh"
 
 namespace hg {
 
@@ -47,6 +48,7 @@ struct NSArgs {
   const double* av_el;      // [n_el][2] Ceps sqrt(Volume)/(N+1), sum of the 4 edge areas
   const double* side_area;  // [n_el*4] Area of each side's edge
   double* mu_av;            // [n_el] element viscosity of the current state (written by the gradient kernel)
+  SensorArgs sensor;        // which indicator sets it (jumps, modal, learned)
 };
 
 __host__ __device__ constexpr int epb_ns(int P) {
@@ -58,7 +60,7 @@ __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) +
 template <int P, int EPB, typename real, bool AFFINE>
 struct NSTiles {
   static constexpr int NP = P * P, FT = 4 * P;
-  real mat[2 * NP + 7 * P];   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w
+  real mat[3 * NP + 7 * P];   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w Vinv
   real Q[4][EPB][NP];
   real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : NP];   // Ja00 Ja01 Ja10 Ja11 J
   real dQ[2][4][EPB][NP];
@@ -180,7 +182,7 @@ template <int P, int EPB, typename real, bool AFFINE>
 __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s, int flat, int le,
                                            int tid, int e, bool active, real* geoE) {
   constexpr int NP = P * P;
-  for (int k = flat; k < 2 * NP + 7 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
+  for (int k = flat; k < 3 * NP + 7 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
   if (active) {
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
@@ -208,6 +210,17 @@ template <int P, int EPB, typename real, bool AFFINE>
 __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
                                                   const Phys<real>& ph, int le, int tid, int e, bool active) {
   constexpr int NP = P * P, FT = 4 * P;
+  if (a.sensor.kind != SENSOR_JUMPS) {   // modal-decay or learned indicator (hg_sensor.cuh)
+    // evaluated on the first stage of a time step (and for a bare time derivative); the later stages
+    // of the step keep that viscosity.  The reference's jumps indicator is re-evaluated every stage.
+    if (!a.first) return;
+    __shared__ real s_scr[EPB][sensor_scratch(P)];
+    const SensorOut so = element_sensor<P, EPB, real>(a.sensor, ph, s.Q, s_scr[le < EPB ? le : 0],
+                                                      s.mat + 2 * NP + 7 * P, le, tid, active, nullptr);
+    if (active && tid == 0) a.mu_av[e] = a.av_el[2 * size_t(e)] * so.g;
+    __syncthreads();
+    return;
+  }
   const real* lb0 = s.mat + NP;
   const real* lb1 = lb0 + P;
   const real* wq = s.mat + 2 * NP + 6 * P;

@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cfloat>
 #include <stdexcept>
+#include <utility>
 
 namespace hg {
 
@@ -129,6 +130,36 @@ NodalOps make_nodal_ops(int N, int node_type) {
     for (int j = 0; j < P; ++j) { s0 += o.D[j * P + i] * o.lb0[j]; s1 += o.D[j * P + i] * o.lb1[j]; }
     o.dlbw0[i] = s0 / o.w[i];
     o.dlbw1[i] = s1 / o.w[i];
+  }
+  // modal transform (orthonormal Legendre on [0,1]) by Gauss-Jordan elimination with pivoting
+  {
+    std::vector<double> V(P * P), A(P * 2 * P, 0.0);
+    for (int i = 0; i < P; ++i)
+      for (int k = 0; k < P; ++k) {
+        double L, dL;
+        legendre(k, 2.0 * o.xi[i] - 1.0, L, dL);
+        V[i * P + k] = std::sqrt(2.0 * k + 1.0) * L;
+      }
+    for (int r = 0; r < P; ++r) {
+      for (int c = 0; c < P; ++c) A[r * 2 * P + c] = V[r * P + c];
+      A[r * 2 * P + P + r] = 1.0;
+    }
+    for (int c = 0; c < P; ++c) {
+      int piv = c;
+      for (int r = c + 1; r < P; ++r)
+        if (std::fabs(A[r * 2 * P + c]) > std::fabs(A[piv * 2 * P + c])) piv = r;
+      if (piv != c) for (int q = 0; q < 2 * P; ++q) std::swap(A[c * 2 * P + q], A[piv * 2 * P + q]);
+      const double d = A[c * 2 * P + c];
+      for (int q = 0; q < 2 * P; ++q) A[c * 2 * P + q] /= d;
+      for (int r = 0; r < P; ++r)
+        if (r != c) {
+          const double f = A[r * 2 * P + c];
+          for (int q = 0; q < 2 * P; ++q) A[r * 2 * P + q] -= f * A[c * 2 * P + q];
+        }
+    }
+    o.Vinv.assign(P * P, 0.0);
+    for (int k = 0; k < P; ++k)
+      for (int i = 0; i < P; ++i) o.Vinv[k * P + i] = A[k * 2 * P + P + i];
   }
   return o;
 }

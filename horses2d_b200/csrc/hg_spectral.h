@@ -15,6 +15,9 @@ namespace hg {
 struct NodalOps {
   int N = 0, P = 0;
   std::vector<double> xi, w, wb, D, hatD, lb0, lb1, lbw0, lbw1, dlbw0, dlbw1;
+  // nodal -> modal transform: Vinv = V^-1 with V(i,k) = sqrt(2k+1) L_k(2 xi_i - 1), the orthonormal
+  // Legendre basis on [0,1]; modal coefficients u_hat(k) = sum_i Vinv(k,i) u(xi_i)   [k*P+i]
+  std::vector<double> Vinv;
 };
 
 NodalOps make_nodal_ops(int N, int node_type);   // node_type: 1 LG, 2 LGL

@@ -93,13 +93,16 @@ def box_descriptor(nx, ny, x0, x1, y0, y1, N, node_type, *, elem_offset=0, edge_
     partner[o:o + ny] = np.arange(o + ny, o + 2 * ny) + edge_offset
     partner[o + ny:o + 2 * ny] = np.arange(o, o + ny) + edge_offset
     ee = np.concatenate(edges_elem)
+    # invh = Area / min(adjacent volumes) (QuadMesh_Construct.incf:270-303): 1/hx across x, 1/hy across y
+    invh = np.concatenate([np.full(ny * (nx - 1), 1.0 / hx), np.full(nx * (ny - 1), 1.0 / hy),
+                           np.full(2 * nx, 1.0 / hy), np.full(2 * ny, 1.0 / hx)])
     return dict(N=np.full(E, N, np.int32), Ja=Ja.reshape(-1), jac=jac, x=x, volume=np.full(E, hx * hy),
                 vertices=verts, edge_elem=ee.reshape(-1).astype(np.int32),
                 edge_side=np.concatenate(edges_side).reshape(-1).astype(np.int32),
                 edge_inverse=np.zeros(F, np.int32), edge_marker=np.concatenate(marker).astype(np.int32),
                 edge_n=np.concatenate(nrm).reshape(-1), edge_dS=np.concatenate(dS).reshape(-1),
                 periodic_partner=partner.astype(np.int32),
-                edge_invh=np.full(F, 0.0))
+                edge_invh=invh)
 
 
 def _same(a, b):

@@ -170,6 +170,34 @@ class GpuDGSEM:
         self._check(self._lib.hg_kernel_times(self._h, ms, cnt, n))
         return {k: (ms[i], cnt[i]) for i, k in enumerate(L.KERNEL_KINDS)}
 
+    # --- shock sensor of the artificial dissipation -------------------------
+    def set_sensor(self, kind, s0=float("nan"), kappa=float("nan"), mlp=None, lo=None, hi=None):
+        """Indicator that sets the artificial viscosity: L.SENSOR_JUMPS (reference), _MODAL, _LEARNED."""
+        def f32(a, n):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float32).ravel()
+            if a.size != n:
+                raise HorsesGpuError(f"expected {n} values, got {a.size}")
+            self._keep.append(a)
+            return a.ctypes.data_as(L.F32P)
+        self._check(self._lib.hg_set_sensor(self._h, kind, s0, kappa, f32(mlp, L.MLP_PARAMS),
+                                            f32(lo, L.SENSOR_FEATURES), f32(hi, L.SENSOR_FEATURES)))
+
+    def sensor_eval(self):
+        """(features [n_el,16] float32, out [n_el,4]: modal G, learned G, OOD flag, G in use)."""
+        n = self.info()["n_elements"]
+        f = np.zeros((n, L.SENSOR_FEATURES), np.float32)
+        o = np.zeros((n, 4))
+        self._check(self._lib.hg_sensor_eval(self._h, f.ctypes.data_as(L.F32P), o.ctypes.data_as(L.F64P)))
+        return f, o
+
+    def element_viscosity(self):
+        n = self.info()["n_elements"]
+        mu = np.zeros(n)
+        self._check(self._lib.hg_element_viscosity(self._h, mu.ctypes.data_as(L.F64P)))
+        return mu
+
     def info(self):
         """{N, n_elements, affine, precision} of the context."""
         out = (C.c_int32 * 4)()

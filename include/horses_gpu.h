@@ -154,6 +154,36 @@ int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
  * misaligned), 2 set-up failed, 3 launch or copy failed. */
 #define HG_NOALLOC_MAX_NDOF 536870912LL
 int  hg_residuals_noalloc(const double* qdot, int64_t ndof, void* cuda_stream, double out[4]);
+/* Shock sensor of the artificial dissipation (no reference counterpart beyond HG_SENSOR_JUMPS, the
+ * reference's jumps-based indicator, DGArtificialDissipation.f90:277-338, the default).  The
+ * viscosity law is always mu_e = av_intensity * sqrt(Volume)/(N+1) * G.
+ *   HG_SENSOR_MODAL    G = ramp(s; s0, kappa), s = max over rho, p of log10(E_N/E) of the element's
+ *                      orthonormal-Legendre modal energies (modal decay); the ramp is the reference's
+ *                      sine ramp; s0 = NaN keeps log10((N+1)^-4), kappa = NaN keeps 1.
+ *   HG_SENSOR_LEARNED  G = the MLP (16 -> 32 -> 32 -> 1, tanh, sigmoid output) on HG_SENSOR_FEATURES
+ *                      modal features, or the modal G where a feature leaves [lo, hi] (fallback);
+ *                      mlp = HG_MLP_PARAMS floats: W1[32][16] b1[32] W2[32][32] b2[32] W3[32] b3.
+ * hg_sensor_eval: per element, the features ([n_el][16] floats, may be NULL) and {modal G, learned G
+ * (-1 without weights), out-of-distribution flag, G used by the current kind (-1 for jumps)}
+ * ([n_el][4] doubles, may be NULL) of the resident state.  hg_element_viscosity: mu_e of the last
+ * stage ([n_el] doubles; contexts with artificial dissipation). */
+enum { HG_SENSOR_JUMPS = 0, HG_SENSOR_MODAL = 1, HG_SENSOR_LEARNED = 2 };
+#define HG_SENSOR_FEATURES 16
+#define HG_MLP_PARAMS 1633
+int  hg_set_sensor(hg_ctx* ctx, int32_t kind, double s0, double kappa, const float* mlp, const float* lo,
+                   const float* hi);
+int  hg_sensor_eval(hg_ctx* ctx, float* features, double* out);
+int  hg_element_viscosity(hg_ctx* ctx, double* mu);
+/* Learned-sensor network on the GPU (no context): batched inference y = sigmoid(MLP(X)) for n
+ * samples of HG_SENSOR_FEATURES floats; the mean weighted binary cross-entropy on the logit and its
+ * gradient (w may be NULL: unit weights); and Adam training (beta 0.9/0.999, eps 1e-8) over
+ * `epochs` shuffled passes (seeded) in mini-batches, params updated in place, epoch_loss[epochs]
+ * optional.  All arrays are host arrays.  Returns 0 ok, 1 bad argument, 3 CUDA failure. */
+int  hg_mlp_forward(const float* params, const float* X, int64_t n, float* y);
+int  hg_mlp_grad(const float* params, const float* X, const float* t, const float* w, int64_t n, double* loss,
+                 float* grad);
+int  hg_mlp_train(float* params, const float* X, const float* t, const float* w, int64_t n, int32_t epochs,
+                  int32_t batch, double lr, uint64_t seed, double* epoch_loss);
 /* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
 int  hg_info(const hg_ctx* ctx, int32_t out[4]);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N

@@ -176,6 +176,22 @@ extern "C" int or_integrate(void* h, int scheme, int mode, double t0, double t_e
 
 // OpenMP team size of the calling host thread's parallel regions (the reference runs
 // with OMP_NUM_THREADS threads; callers that step one oracle per host thread pass 1).
+extern "C" void or_zone_state(void* h, int zone, double* q) {
+  auto& o = *static_cast<orc::Oracle*>(h);
+  for (int k = 0; k < 4; ++k) q[k] = (zone >= 1 && zone < int(o.zones.size()) && o.zones[zone].q.size() == 4)
+                                          ? o.zones[zone].q[k] : 0.0;
+}
+
+extern "C" void or_set_av_g(void* h, const double* G) {
+  auto& o = *static_cast<orc::Oracle*>(h);
+  o.av_g_ext.assign(G, G + o.el.size());
+}
+
+extern "C" void or_av_viscosity(void* h, double* mu) {
+  auto& o = *static_cast<orc::Oracle*>(h);
+  for (size_t e = 0; e < o.el.size(); ++e) mu[e] = e < o.av_mu.size() ? o.av_mu[e] : 0.0;
+}
+
 extern "C" void or_set_threads(int n) {
 #ifdef _OPENMP
   omp_set_num_threads(n > 0 ? n : 1);

@@ -8,6 +8,13 @@
  *   PhysicalDissipation_*        :251-269   mu_a added to mu in every viscous flux
  * and the edge jumps Edge_ComputeJumps / CurvedEdge_ / SubdividedEdge_ / CurvedSubdividedEdge_ /
  * StraightBdryEdge_ / CurvedBdryEdge_ComputeJumps (Mesh/QuadElement_EdgeProcedures.incf:1348-1619).
+ *
+ * Two indicators without a reference counterpart feed the same viscosity law Ceps sqrt(V)/(N+1) G:
+ * the modal-decay indicator (Persson & Peraire, "Sub-cell shock capturing for discontinuous Galerkin
+ * methods", AIAA 2006-112): s = max over rho and p of log10(E_N/E), E the energy of the element's
+ * modal coefficients in the orthonormal Legendre basis of [0,1] and E_N that of the modes whose higher
+ * index is N, G = the reference's sine ramp around s0 of half width kappa; and an external G per
+ * element (the library's learned sensor, checked through it).
  */
 #include "oracle_internal.h"
 #include "viscous.h"
@@ -106,11 +113,89 @@ double av_element_viscosity(const Oracle& o, const Element& e) {
   return o.cas.av_intensity * maxVisc * G;
 }
 
+// nodal -> modal matrix of the orthonormal Legendre basis sqrt(2k+1) L_k(2x-1) at the element nodes
+static std::vector<double> modal_matrix(const Spectral& sp) {
+  const int P = sp.P;
+  std::vector<double> A(size_t(P) * 2 * P, 0.0);
+  for (int i = 0; i < P; ++i) {
+    const double x = 2.0 * sp.xi[i] - 1.0;
+    double l0 = 1.0, l1 = x;
+    for (int k = 0; k < P; ++k) {
+      double Lk;
+      if (k == 0) Lk = 1.0;
+      else if (k == 1) Lk = x;
+      else { const double l2 = ((2.0 * k - 1.0) * x * l1 - (k - 1.0) * l0) / k; l0 = l1; l1 = l2; Lk = l2; }
+      A[size_t(i) * 2 * P + k] = std::sqrt(2.0 * k + 1.0) * Lk;
+    }
+    A[size_t(i) * 2 * P + P + i] = 1.0;
+  }
+  for (int c = 0; c < P; ++c) {   // Gauss-Jordan with partial pivoting
+    int piv = c;
+    for (int r = c + 1; r < P; ++r) if (std::fabs(A[size_t(r) * 2 * P + c]) > std::fabs(A[size_t(piv) * 2 * P + c])) piv = r;
+    if (piv != c) for (int q = 0; q < 2 * P; ++q) std::swap(A[size_t(c) * 2 * P + q], A[size_t(piv) * 2 * P + q]);
+    const double d = A[size_t(c) * 2 * P + c];
+    for (int q = 0; q < 2 * P; ++q) A[size_t(c) * 2 * P + q] /= d;
+    for (int r = 0; r < P; ++r)
+      if (r != c) {
+        const double f = A[size_t(r) * 2 * P + c];
+        for (int q = 0; q < 2 * P; ++q) A[size_t(r) * 2 * P + q] -= f * A[size_t(c) * 2 * P + q];
+      }
+  }
+  std::vector<double> Vinv(size_t(P) * P);
+  for (int k = 0; k < P; ++k) for (int i = 0; i < P; ++i) Vinv[size_t(k) * P + i] = A[size_t(k) * 2 * P + P + i];
+  return Vinv;
+}
+
+static double ramp(double s, double s0, double k) {
+  if (s < s0 - k) return 0.0;
+  if (s < s0 + k) return 0.5 * std::sin(0.5 * PI * (s - s0) / k) + 0.5;
+  return 1.0;
+}
+
+double modal_indicator(const Oracle& o, const Element& e) {
+  const int P = e.P, N = e.N, NP = P * P;
+  const std::vector<double> Vinv = modal_matrix(*e.sp);
+  const double* Q = &o.Q[e.offset];
+  double smax = -DBL_MAX;
+  for (int v = 0; v < 2; ++v) {
+    std::vector<double> u(NP);
+    for (int q = 0; q < NP; ++q) {
+      const double* qq = &Q[4 * q];
+      u[q] = v == 0 ? qq[0] : o.ph.gm1 * (qq[3] - 0.5 * (qq[1] * qq[1] + qq[2] * qq[2]) / qq[0]);
+    }
+    double E = 0.0, EN = 0.0;
+    for (int n = 0; n < P; ++n)
+      for (int m = 0; m < P; ++m) {
+        double c = 0.0;
+        for (int j = 0; j < P; ++j) {
+          double a = 0.0;
+          for (int i = 0; i < P; ++i) a += Vinv[size_t(m) * P + i] * u[j * P + i];
+          c += Vinv[size_t(n) * P + j] * a;
+        }
+        E += c * c;
+        if (m == N || n == N) EN += c * c;
+      }
+    const double s = (E > 0.0 && EN > 0.0) ? std::log10(EN / E) : -DBL_MAX;
+    smax = std::fmax(smax, s);
+  }
+  return ramp(smax, o.cas.av_s0, o.cas.av_kappa);
+}
+
 void compute_av_viscosity(Oracle& o) {
   o.av_mu.assign(o.el.size(), 0.0);
   if (!o.cas.navier_stokes || o.cas.av_type == OR_AV_NONE) return;
 #pragma omp parallel for schedule(static)
-  for (size_t e = 0; e < o.el.size(); ++e) o.av_mu[e] = av_element_viscosity(o, o.el[e]);
+  for (size_t e = 0; e < o.el.size(); ++e) {
+    const Element& E = o.el[e];
+    if (o.cas.av_indicator == OR_IND_JUMPS) {
+      o.av_mu[e] = av_element_viscosity(o, E);
+    } else {
+      const double G = o.cas.av_indicator == OR_IND_MODAL ? modal_indicator(o, E)
+                                                          : (e < o.av_g_ext.size() ? o.av_g_ext[e] : 0.0);
+      const double maxVisc = std::sqrt(E.volume) / (E.N + 1);
+      o.av_mu[e] = o.cas.av_intensity * maxVisc * G;
+    }
+  }
 }
 
 double av_edge_viscosity(const Oracle& o, const Edge& f) {

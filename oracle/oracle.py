@@ -20,6 +20,7 @@ LG, LGL = 1, 2
 EULER, RK3, RK5 = 0, 1, 2
 BR1, IP = 0, 1
 AV_NONE, AV_LAPLACIAN, AV_PHYSICAL = 0, 1, 2
+IND_JUMPS, IND_MODAL, IND_EXTERNAL = 0, 1, 2
 
 
 class OrBC(C.Structure):
@@ -34,7 +35,8 @@ class OrCase(C.Structure):
                 ("ip_method", C.c_int), ("sigma0_ip", C.c_double), ("sigma1_ip", C.c_double),
                 ("mach", C.c_double), ("reynolds", C.c_double), ("prandtl", C.c_double),
                 ("pressure_ref", C.c_double), ("temperature_ref", C.c_double), ("reynolds_length", C.c_double),
-                ("n_markers", C.c_int), ("bcs", C.POINTER(OrBC)), ("av_type", C.c_int), ("av_intensity", C.c_double)]
+                ("n_markers", C.c_int), ("bcs", C.POINTER(OrBC)), ("av_type", C.c_int), ("av_intensity", C.c_double),
+                ("av_indicator", C.c_int), ("av_s0", C.c_double), ("av_kappa", C.c_double)]
 
 
 class OrMesh(C.Structure):
@@ -81,6 +83,9 @@ def lib():
         L.or_integrate.argtypes = [vp, i, i, d, d, i, d, d, d, dp]
         L.or_ref_values.argtypes = [vp, dp]
         L.or_set_threads.argtypes = [C.c_int]
+        L.or_set_av_g.argtypes = [vp, dp]
+        L.or_zone_state.argtypes = [vp, C.c_int, dp]
+        L.or_av_viscosity.argtypes = [vp, dp]
         L.or_element_geometry.argtypes = [vp, dp, dp, dp]
         L.or_edge_count_by_type.restype = i
         L.or_edge_count_by_type.argtypes = [vp, i]
@@ -102,7 +107,8 @@ class Oracle:
 
     def __init__(self, mesh, poly_order, *, nodes=LGL, riemann=ROE, mach=0.5, reynolds=0.0, prandtl=0.72,
                  pressure_ref=101325.0, temperature_ref=273.15, reynolds_length=1.0, bcs=(), navier_stokes=0,
-                 viscous=BR1, ip_method=0, sigma0_ip=1.0, sigma1_ip=0.0, av_type=0, av_intensity=1.0):
+                 viscous=BR1, ip_method=0, sigma0_ip=1.0, sigma1_ip=0.0, av_type=0, av_intensity=1.0, av_indicator=0, av_s0=None,
+                 av_kappa=1.0):
         self._keep = []
         m = OrMesh()
         pts = np.ascontiguousarray(mesh["points"], dtype=np.float64)
@@ -147,7 +153,9 @@ class Oracle:
                    sigma0_ip=sigma0_ip, sigma1_ip=sigma1_ip, mach=mach, reynolds=reynolds, prandtl=prandtl,
                    pressure_ref=pressure_ref, temperature_ref=temperature_ref, reynolds_length=reynolds_length,
                    n_markers=len(bcs), bcs=C.cast(bc_arr, C.POINTER(OrBC)), av_type=av_type,
-                   av_intensity=av_intensity)
+                   av_intensity=av_intensity, av_indicator=av_indicator,
+                   av_s0=(np.log10(1.0 / (int(np.max(poly_order)) + 1) ** 4) if av_s0 is None else av_s0),
+                   av_kappa=av_kappa)
         err = C.create_string_buffer(512)
         self.h = lib().or_create(C.byref(c), C.byref(m), err, 512)
         if not self.h:
@@ -199,6 +207,23 @@ class Oracle:
         r = np.zeros(4)
         lib().or_residuals(self.h, _p(r, C.c_double))
         return r
+
+    def zone_state(self, zone):
+        """Dimensionless state of zone `zone` (1-based marker) as the oracle built it."""
+        q = np.zeros(4)
+        lib().or_zone_state(self.h, zone, _p(q, C.c_double))
+        return q
+
+    def set_av_g(self, G):
+        """Per-element indicator G used by av_indicator=IND_EXTERNAL."""
+        G = np.ascontiguousarray(G, dtype=np.float64)
+        lib().or_set_av_g(self.h, _p(G, C.c_double))
+
+    def av_viscosity(self):
+        """Element artificial viscosity computed by the last time derivative."""
+        mu = np.zeros(self.n_elements)
+        lib().or_av_viscosity(self.h, _p(mu, C.c_double))
+        return mu
 
     def integrate(self, scheme, *, transient=True, t0=0.0, t_end=1.0, max_iter=1000, cfl=0.1, dt_cap=0.01,
                   residual_target=1e-12):

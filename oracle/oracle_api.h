@@ -31,6 +31,7 @@ enum { OR_SCHEME_EULER = 0, OR_SCHEME_RK3 = 1, OR_SCHEME_RK5 = 2 };
 enum { OR_VISC_BR1 = 0, OR_VISC_IP = 1 };
 enum { OR_IP_SIPG = 0, OR_IP_NIPG = 1, OR_IP_IIPG = 2 };
 enum { OR_AV_NONE = 0, OR_AV_LAPLACIAN = 1, OR_AV_PHYSICAL = 2 };
+enum { OR_IND_JUMPS = 0, OR_IND_MODAL = 1, OR_IND_EXTERNAL = 2 };
 
 typedef struct {
   int    type;              /* OR_BC_* */
@@ -63,6 +64,8 @@ typedef struct {
   const or_bc* bcs;         /* [n_markers], zone k+1 */
   int    av_type;           /* artificial dissipation: OR_AV_NONE / LAPLACIAN / PHYSICAL (jumps-based indicator) */
   double av_intensity;      /* "Artificial dissipation intensity" (Ceps) */
+  int    av_indicator;      /* OR_IND_JUMPS (reference), OR_IND_MODAL, OR_IND_EXTERNAL (G from or_set_av_g) */
+  double av_s0, av_kappa;   /* modal ramp centre and half width */
 } or_case;
 
 typedef struct {
@@ -96,6 +99,9 @@ void    or_residuals(void* h, double out[4]);
  * mode 1 transient, 0 steady.  Returns the number of iterations run. */
 int     or_integrate(void* h, int scheme, int mode, double t0, double t_end, int max_iter,
                      double cfl, double dt_cap, double residual_target, double* t_out);
+void    or_zone_state(void* h, int zone, double* q);  /* dimensionless state of zone (marker) 1..n */
+void    or_set_av_g(void* h, const double* G);   /* per-element indicator G for OR_IND_EXTERNAL */
+void    or_av_viscosity(void* h, double* mu);     /* element viscosity of the current state (after a derivative) */
 void    or_set_threads(int n);             /* OpenMP threads of the calling thread's regions */
 /* Physics constants resolved by InitializePhysics (Physics/PhysicsNS.f90:405-481). */
 void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless, invSqrtGammaMach */
