@@ -124,19 +124,23 @@ def build_parts(config):
     return parts
 
 
-def stage_bytes_per_dof(config, prec_fp32, affine):
+def stage_bytes_per_dof(config, prec_fp32, affine, ns=False):
     """Algorithmic DRAM bytes per DOF of one launch of the fused stage kernel (RK3 average).
 
     State Q read + written in FP64 (16 B), RK register G written every stage and read in
-    stages 2-3 (sG = 4 or 8 B), volume metrics (Ja, 1/J: 5 FP64 per node = 10 B/DOF) on
-    curved meshes, 0 on affine ones.  Face traces and nodal matrices are cache-resident."""
+    stages 2-3 (sG = 4 or 8 B), volume metrics (Ja, 1/J: 5 values per node in the arithmetic
+    precision = 10 or 5 B/DOF) on curved meshes, 0 on affine ones; Navier-Stokes: the element
+    gradient written by the gradient kernel is read back (8 values per node = 2 sG B/DOF).
+    Face traces and nodal matrices are cache-resident."""
     sg = 4 if prec_fp32 else 8
-    return 16.0 + sg * (1.0 + 2.0 / 3.0) + (0.0 if affine else 10.0)
+    return 16.0 + sg * (1.0 + 2.0 / 3.0) + (0.0 if affine else 1.25 * sg) + (2.0 * sg if ns else 0.0)
 
 
-def gradient_bytes_per_dof(affine):
-    """Navier-Stokes gradient pass: Q read (8 B) + volume metrics (10 B/DOF when curved)."""
-    return 8.0 + (0.0 if affine else 10.0)
+def gradient_bytes_per_dof(prec_fp32, affine):
+    """Navier-Stokes gradient pass: Q read (8 B), volume metrics (1.25 sG B/DOF when curved), the
+    element gradient written (2 sG B/DOF)."""
+    sg = 4 if prec_fp32 else 8
+    return 8.0 + (0.0 if affine else 1.25 * sg) + 2.0 * sg
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -445,7 +449,7 @@ def run_shock(args, rank, world, local, dist):
         raise SystemExit("non-finite state after the timed steps")
     value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
     value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
-    bpd = stage_bytes_per_dof("shock", True, True) + 0.0
+    bpd = stage_bytes_per_dof("shock", True, True, True)
     st_ms, st_n = split["stage"]
     avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
     achieved = bpd * ndof / avg_stage_s / 1e9
@@ -555,7 +559,7 @@ def main():
     e2e = ndof * 3 * args.steps * world / (e2e_ms * 1e-3)
 
     # ---- roofline of the dominant kernel (fused stage kernel), from its own event times
-    bpd = stage_bytes_per_dof(args.config, prec == hg.PREC_FP32, affine)
+    bpd = stage_bytes_per_dof(args.config, prec == hg.PREC_FP32, affine, ns)
     st_ms, st_n = split["stage"]
     avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
     stage_launch_bytes = bpd * ndof / len(ctxs)
@@ -568,7 +572,7 @@ def main():
             traffic = json.load(open(tpath))["bytes_per_dof"] * ndof / len(ctxs)
         except Exception:
             traffic = None
-    step_bytes_per_dof_stage = bpd + (gradient_bytes_per_dof(affine) if ns else 0.0)
+    step_bytes_per_dof_stage = bpd + (gradient_bytes_per_dof(prec == hg.PREC_FP32, affine) if ns else 0.0)
     step_achieved = step_bytes_per_dof_stage * ndof * 3 * args.steps / (ms * 1e-3) / 1e9
     total_split = sum(v[0] for v in split.values()) or 1.0
     line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,

@@ -32,7 +32,7 @@ static void free_ctx(hg_ctx* c) {
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
-                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi};
+                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
@@ -63,10 +63,10 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   NSArgs<real> a{};
   a.n_el = c->n_el;
   a.side = c->d_side;
-  a.side_geo = c->d_side_geo;
+  a.side_geo = static_cast<const real*>(c->d_side_geo);
   a.side_invh = c->d_side_invh;
-  a.vol_geo = c->d_vol_geo;
-  a.jac = c->d_jac;
+  a.vol_geo = static_cast<const real*>(c->d_vol_geo);
+  a.jac = static_cast<const real*>(c->d_jac);
   a.mats = c->d_mats;
   a.zones = c->d_zones;
   a.Q = c->d_Q;
@@ -74,6 +74,12 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
   a.T_out = static_cast<real*>(c->d_T[c->cur ^ 1]);
   a.GT = static_cast<real*>(c->d_GT);
+  a.dQ = static_cast<real*>(c->d_dQ);
+  a.viscous = (c->pc.mu != 0.0 || c->av == HG_AV_PHYSICAL) ? 1 : 0;
+  // BR1 always needs the lifted gradient; IP only for gradient traces (viscous fluxes) or the indicator
+  // (the jumps indicator every stage, the modal and learned ones on the first stage of a step)
+  a.run_gradient = (!c->ip || a.viscous ||
+                    (c->av != HG_AV_NONE && (c->sensor_kind == HG_SENSOR_JUMPS || first))) ? 1 : 0;
   a.QDot = qdot;
   a.resid = resid ? c->d_resid : nullptr;
   a.a = ca; a.b = cb; a.c = cc;
@@ -100,8 +106,8 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   StageArgs<real> a{};
   a.n_el = c->n_el;
   a.side = c->d_side;
-  a.side_geo = c->d_side_geo;
-  a.vol_geo = c->d_vol_geo;
+  a.side_geo = static_cast<const real*>(c->d_side_geo);
+  a.vol_geo = static_cast<const real*>(c->d_vol_geo);
   a.mats = c->d_mats;
   a.zones = c->d_zones;
   a.Q = c->d_Q;
@@ -347,8 +353,19 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->own_stream = true;
   const size_t rs = c->precision == HG_PREC_FP32 ? sizeof(float) : sizeof(double);
   c->d_side = dalloc<int4>(side.size());
-  c->d_side_geo = dalloc<double>(sg.size());
-  c->d_vol_geo = dalloc<double>(vg.size());
+  // geometry in the arithmetic precision of the context (FP32 bulk path: float, half the bytes)
+  auto upload_real = [&](void*& dst, const double* src, size_t n) {
+    if (c->precision == HG_PREC_FP32) {
+      std::vector<float> f(src, src + n);
+      dst = dalloc<float>(n);
+      HG_CUDA(cudaMemcpy(dst, f.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    } else {
+      dst = dalloc<double>(n);
+      HG_CUDA(cudaMemcpy(dst, src, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  };
+  upload_real(c->d_side_geo, sg.data(), sg.size());
+  upload_real(c->d_vol_geo, vg.data(), vg.size());
   c->d_mats = dalloc<double>(mats.size());
   c->d_zones = dalloc<Zone>(zones.size());
   c->d_Q = dalloc<double>(c->ndof);
@@ -387,15 +404,13 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
     if (c->ip && !m->edge_invh) throw std::runtime_error("interior penalty needs edge_invh");
     c->d_side_invh = dalloc<double>(sinvh.size());
     c->d_GT = dalloc<char>(size_t(E) * 4 * P * 8 * rs);
+    c->d_dQ = dalloc<char>(size_t(c->ndof) * 2 * rs);
     HG_CUDA(cudaMemcpy(c->d_side_invh, sinvh.data(), sinvh.size() * sizeof(double), cudaMemcpyHostToDevice));
     if (!c->affine) {
-      c->d_jac = dalloc<double>(size_t(E) * NP);
-      HG_CUDA(cudaMemcpy(c->d_jac, m->jac, size_t(E) * NP * sizeof(double), cudaMemcpyHostToDevice));
+      upload_real(c->d_jac, m->jac, size_t(E) * NP);
     }
   }
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  HG_CUDA(cudaMemcpy(c->d_side_geo, sg.data(), sg.size() * sizeof(double), cudaMemcpyHostToDevice));
-  HG_CUDA(cudaMemcpy(c->d_vol_geo, vg.data(), vg.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemset(c->d_resid, 0, size_t(grid_for(c)) * 4 * sizeof(double)));

@@ -22,8 +22,8 @@ struct hg_ctx {
   double mach = 0, gamma = 1.4;
   // device buffers
   int4* d_side = nullptr;
-  double* d_side_geo = nullptr;
-  double* d_vol_geo = nullptr;
+  void* d_side_geo = nullptr;     // geometry in the context's precision (FP32 path: float)
+  void* d_vol_geo = nullptr;
   double* d_mats = nullptr;
   Zone* d_zones = nullptr;
   double* d_Q = nullptr;
@@ -48,8 +48,9 @@ struct hg_ctx {
   float* d_mlp = nullptr;
   float* d_feat_lo = nullptr;
   float* d_feat_hi = nullptr;
-  double* d_jac = nullptr;        // [n_el][NP] J (curved meshes, gradient faces)
+  void* d_jac = nullptr;          // [n_el][NP] J (curved meshes), context precision
   void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
+  void* d_dQ = nullptr;           // element gradients [n_el][2][4][NP] (Navier-Stokes)
   bool state_set = false;
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)

@@ -41,11 +41,14 @@ static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
     max_carveout(ns_stage_kernel<P, EPB, real, AFFINE, IP, AV>);
     attr = true;
   }
-  timed(c, HG_KERNEL_GRADIENT,
-        [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, block_ns(P), 0, c->stream>>>(a); });
+  if (a.run_gradient) {
+    timed(c, HG_KERNEL_GRADIENT,
+          [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, block_ns(P), 0, c->stream>>>(a); });
+    ++c->launches;
+  }
   timed(c, HG_KERNEL_STAGE,
         [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, block_ns(P), 0, c->stream>>>(a); });
-  c->launches += 2;
+  ++c->launches;
 }
 
 template <int P, typename real>

@@ -8,7 +8,11 @@
 //        gradient (ComputeInteriorGradient, Mesh/QuadElement_QuadProcedures.incf:42-88) -- and
 //        writes only its traces on the four sides (interpolateGradientsToBoundaries,
 //        DGSpatialDiscretizationMethods.f90:1577-1631);
-//   ns_stage_kernel     recomputes dQ in shared memory (the full gradient never goes to HBM),
+//   ns_gradient_kernel also stores the BR1 gradient dQ ([n_el][2][4][NP], coalesced per node); the
+//        interior-penalty gradient is element-local and the stage kernel recomputes it, so with IP the
+//        gradient kernel runs only when something else needs it (gradient traces for viscous fluxes,
+//        the artificial-viscosity indicator);
+//   ns_stage_kernel     reads the BR1 dQ back (written once, read once per stage),
 //        F = Fi - Fv at the nodes (QDotVolumeLoop :243-268), face fluxes
 //        F* = (Fi* - Fv*) dS with the neighbours' Q and dQ traces (BR1: (FvL+FvR)/2 . n; IP adds
 //        sigma0 mu N^2 invh (uL - uR), DGViscous_IP.f90:45-130), boundary viscous fluxes by
@@ -25,10 +29,10 @@ template <typename real>
 struct NSArgs {
   int n_el;
   const int4* side;         // [n_el*4] {neighbour trace slot, flags, zone, 0}
-  const double* side_geo;   // normals / dS (per node, or per side when AFFINE)
+  const real* side_geo;     // normals / dS (per node, or per side when AFFINE)
   const double* side_invh;  // [n_el*4] invh of the side's edge
-  const double* vol_geo;    // Ja00 Ja01 Ja10 Ja11 1/J (per node, or per element when AFFINE)
-  const double* jac;        // [n_el][NP] J per node (curved gradient faces)
+  const real* vol_geo;      // Ja00 Ja01 Ja10 Ja11 1/J (per node, or per element when AFFINE)
+  const real* jac;          // [n_el][NP] J per node (curved meshes)
   const double* mats;       // hatD[NP] lb0 lb1 lbw0 lbw1 [P each] D[NP] dlbw0 dlbw1 [P each]
   const Zone* zones;
   double* Q;
@@ -36,6 +40,9 @@ struct NSArgs {
   const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
   real* T_out;
   real* GT;                 // dQ traces                      [n_el*4][P][2][4]
+  real* dQ;                 // element gradients              [n_el][2][4][NP]
+  int viscous;              // viscous fluxes present: mu != 0 or the Physical artificial viscosity
+  int run_gradient;         // host side: whether this stage needs the gradient kernel
   double* QDot;
   double* resid;
   double a, b, c;
@@ -106,7 +113,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
         real qo[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
-        const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
+        const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
         const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
         real us[4];
         if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
@@ -192,7 +199,7 @@ __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB
 #pragma unroll
       for (int k = 0; k < 5; ++k) geoE[k] = real(a.vol_geo[size_t(e) * 5 + k]);
     } else {
-      const double* gp = a.vol_geo + (size_t(e) * NP + tid) * 5;
+      const real* gp = a.vol_geo + (size_t(e) * NP + tid) * 5;
 #pragma unroll
       for (int k = 0; k < 4; ++k) s.Ja[k][le][tid] = real(gp[k]);
       s.Ja[4][le][tid] = real(a.jac[size_t(e) * NP + tid]);
@@ -243,7 +250,7 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
         qn3 = tp[3];
         node0 = sd.z >= 0;   // periodic edges are boundary edges of the reference
       } else {
-        const double* g3 = AFFINE ? a.side_geo + sbase * 3 : a.side_geo + (sbase * P + kk) * 3;
+        const real* g3 = AFFINE ? a.side_geo + sbase * 3 : a.side_geo + (sbase * P + kk) * 3;
         real uB[4], uS[4];
         bc_states(ph, a.zones[sd.z], qo, real(g3[0]), real(g3[1]), uB, uS);
         qn0 = uS[0];
@@ -300,6 +307,14 @@ __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a
   __syncthreads();
   if (AV) element_viscosity<P, EPB, real, AFFINE>(a, s, ph, le, tid, e, active);
   if (!active) return;
+  if (!IP) {   // the lifted gradient is not local: store it for the stage kernel
+    real* g = a.dQ + size_t(e) * 8 * NP + tid;
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) g[(d * 4 + k) * NP] = s.dQ[d][k][le][tid];
+  }
+  if (!a.viscous) return;   // gradient traces only feed viscous face fluxes
   const real* lb0 = s.mat + NP;
   const real* lb1 = lb0 + P;
   for (int t = tid; t < FT; t += NP) {
@@ -327,8 +342,18 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
   real geoE[5];
   load_tiles(a, s, flat, le, tid, e, active, geoE);
   const real mu_e = (AV && active) ? real(a.mu_av[e]) : real(0);
+  if (IP) {   // the interior-penalty gradient is element-local: recompute it here
+    __syncthreads();
+    element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+  } else if (active) {
+    const real* g = a.dQ + size_t(e) * 8 * NP + tid;
+#pragma unroll
+    for (int d = 0; d < 2; ++d)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s.dQ[d][k][le][tid] = g[(d * 4 + k) * NP];
+  }
   __syncthreads();
-  element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+  const bool visc = a.viscous != 0;
   const int i = tid % P, j = tid / P;
   const real* hatD = s.mat;
   const real* lb0 = s.mat + NP;
@@ -346,7 +371,11 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) { q[k] = s.Q[k][le][tid]; gx[k] = s.dQ[0][k][le][tid]; gy[k] = s.dQ[1][k][le][tid]; }
     inviscid_flux(ph, q, fi, gi);
-    viscous_flux(ph, q, gx, gy, fv, gv);
+    if (visc) viscous_flux(ph, q, gx, gy, fv, gv);
+    else {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { fv[k] = real(0); gv[k] = real(0); }
+    }
     const real mu_v = (AV && a.av == 2) ? mu + mu_e : mu;
     real ax[4] = {real(0), real(0), real(0), real(0)}, ay[4] = {real(0), real(0), real(0), real(0)};
     if (AV && a.av == 1) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
@@ -385,14 +414,17 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       const int4 sd = a.side[size_t(e) * 4 + sd_];
       const int kind = sd.y & 15;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
-      real qo[4], gox[4], goy[4];
+      real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
-        gox[k] = trace_of(s, s.dQ[0], k, le, sd_, kk, lbv);
-        goy[k] = trace_of(s, s.dQ[1], k, le, sd_, kk, lbv);
+      for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+      if (visc) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          gox[k] = trace_of(s, s.dQ[0], k, le, sd_, kk, lbv);
+          goy[k] = trace_of(s, s.dQ[1], k, le, sd_, kk, lbv);
+        }
       }
-      const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
+      const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
       const real invh = real(a.side_invh[size_t(e) * 4 + sd_]);
       // edge viscosity (JumpsBasedEdgeViscosity): mean over the edge's elements; boundary and
@@ -407,19 +439,26 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
         const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
         const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
-        const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
-        real qn[4], gnx[4], gny[4];
+        real qn[4], gnx[4] = {real(0), real(0), real(0), real(0)}, gny[4] = {real(0), real(0), real(0), real(0)};
 #pragma unroll
-        for (int k = 0; k < 4; ++k) { qn[k] = tp[k]; gnx[k] = gp[k]; gny[k] = gp[4 + k]; }
+        for (int k = 0; k < 4; ++k) qn[k] = tp[k];
+        if (visc) {
+          const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) { gnx[k] = gp[k]; gny[k] = gp[4 + k]; }
+        }
         const bool right = kind == SIDE_RIGHT;
         const real* QL = right ? qn : qo;
         const real* QR = right ? qo : qn;
         int solver = a.riemann;
         if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
-        real Fi[4], FLx[4], FLy[4], FRx[4], FRy[4];
+        real Fi[4], FLx[4] = {real(0), real(0), real(0), real(0)}, FLy[4] = {real(0), real(0), real(0), real(0)};
+        real FRx[4] = {real(0), real(0), real(0), real(0)}, FRy[4] = {real(0), real(0), real(0), real(0)};
         riemann(solver, ph, QL, QR, nx, ny, Fi);
-        viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
-        viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
+        if (visc) {
+          viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
+          viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
+        }
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           real fv = real(0.5) * (mu_f * FLx[k] + mu_f * FRx[k]) * nx + real(0.5) * (mu_f * FLy[k] + mu_f * FRy[k]) * ny;
@@ -432,7 +471,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
           }
           if (right) F[k] = -F[k];
         }
-        if (IP && a.grad_faces) {
+        if (IP && a.grad_faces && visc) {
           real fgx[4], fgy[4], Ax[4], Ay[4];
 #pragma unroll
           for (int k = 0; k < 4; ++k) { fgx[k] = (QL[k] - QR[k]) * nx; fgy[k] = (QL[k] - QR[k]) * ny; }
@@ -455,7 +494,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
           for (int k = 0; k < 4; ++k) Fi[k] = Fi[k] * dS;
         }
         real fv[4] = {real(0), real(0), real(0), real(0)};
-        if (vbc != VBC_NEUMANN) {
+        if (vbc != VBC_NEUMANN && visc) {
           real Fx[4], Fy[4];
           if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, gox, goy, Fx, Fy);
           else viscous_flux(ph, qo, gox, goy, Fx, Fy);
@@ -481,7 +520,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];
-      if (IP && a.grad_faces) {
+      if (IP && a.grad_faces && visc) {
         // metrics at the face node (interpolated along the other direction) and contravariant G
         real fJa00, fJa01, fJa10, fJa11, fJ;
         if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
@@ -516,7 +555,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       qd[k] = qd[k] - s.face[k][le][2 * P + i] * lbw1[j];
       qd[k] = qd[k] - s.face[k][le][3 * P + j] * lbw0[i];
     }
-    if (IP && a.grad_faces) {
+    if (IP && a.grad_faces && visc) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         real dFb = real(0), dGr = real(0), dFt = real(0), dGl = real(0);

@@ -38,8 +38,8 @@ template <typename real>
 struct StageArgs {
   int n_el;
   const int4* side;        // [n_el*4] {neighbour trace slot, flags, zone, 0}
-  const double* side_geo;  // [n_el*4][P][3] (or [n_el*4][3] affine)  nx, ny, dS in this element's side order
-  const double* vol_geo;   // [n_el][P*P][5] (or [n_el][5] affine)  Ja00 Ja01 Ja10 Ja11 1/J
+  const real* side_geo;    // [n_el*4][P][3] (or [n_el*4][3] affine)  nx, ny, dS in this element's side order
+  const real* vol_geo;     // [n_el][P*P][5] (or [n_el][5] affine)  Ja00 Ja01 Ja10 Ja11 1/J
   const double* mats;      // hatD[P*P], lb0[P], lb1[P], lbw0[P], lbw1[P]
   const Zone* zones;
   double* Q;               // [n_el][P*P][4]
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
     const real q[4] = {real(q01.x), real(q01.y), real(q23.x), real(q23.y)};
-    const double* gp = AFFINE ? a.vol_geo + size_t(e) * 5 : a.vol_geo + (size_t(e) * NP + tid) * 5;
+    const real* gp = AFFINE ? a.vol_geo + size_t(e) * 5 : a.vol_geo + (size_t(e) * NP + tid) * 5;
 #pragma unroll
     for (int k = 0; k < 5; ++k) geo[k] = real(gp[k]);
     real f[4], g[4];
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
 #pragma unroll
         for (int k = 0; k < 4; ++k) qo[k] += s_Q[k][le][node] * lbv[l];
       }
-      const double* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + s) * 3 : a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
+      const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + s) * 3 : a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
       real F[4];
       if (kind == SIDE_WALL) {
