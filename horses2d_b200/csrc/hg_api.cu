@@ -27,8 +27,15 @@ static T* dalloc(size_t n) {
   return static_cast<T*>(p);
 }
 
+static void drop_graph(hg_ctx* c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  c->gexec = nullptr;
+  c->g_scheme = -1;
+}
+
 static void free_ctx(hg_ctx* c) {
   if (!c) return;
+  drop_graph(c);
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
@@ -500,10 +507,57 @@ extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
 
+// Steps in pairs through a CUDA graph captured from the context's stream: two steps leave the trace
+// buffers in their starting parity, so one graph serves every pair.  Kernel arguments that change
+// between steps would invalidate it; with a constant dt none do (the schemes' coefficients depend on
+// dt only, the stepping time t enters no kernel).
+static void graph_steps(hg_ctx* c, int scheme, int n_steps, double t0, double dt) {
+  int s = 0;
+  one_step(c, scheme, t0, dt);   // first launches set kernel attributes outside any capture
+  ++s;
+  if (!c->gexec || c->g_scheme != scheme || c->g_dt != dt || c->g_cur != c->cur) {
+    drop_graph(c);
+    const int64_t l0 = c->launches;
+    const int cur0 = c->cur;
+    HG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      one_step(c, scheme, t0, dt);
+      one_step(c, scheme, t0, dt);
+    } catch (...) {
+      cudaGraph_t g0 = nullptr;
+      cudaStreamEndCapture(c->stream, &g0);
+      if (g0) cudaGraphDestroy(g0);
+      c->launches = l0;
+      c->cur = cur0;
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    HG_CUDA(cudaStreamEndCapture(c->stream, &g));
+    const cudaError_t ie = cudaGraphInstantiate(&c->gexec, g, 0);
+    cudaGraphDestroy(g);
+    HG_CUDA(ie);
+    c->g_launches = c->launches - l0;
+    c->launches = l0;
+    c->cur = cur0;
+    c->g_scheme = scheme;
+    c->g_dt = dt;
+    c->g_cur = c->cur;
+  }
+  for (; s + 2 <= n_steps; s += 2) {
+    HG_CUDA(cudaGraphLaunch(c->gexec, c->stream));
+    c->launches += c->g_launches;
+  }
+  for (; s < n_steps; ++s) one_step(c, scheme, t0 + s * dt, dt);
+}
+
 extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double t0, double dt) {
   try {
     require_state(c);
-    for (int s = 0; s < n_steps; ++s) one_step(c, scheme, t0 + s * dt, dt);
+    if (n_steps >= 5 && !c->prof && c->stream != nullptr) {
+      graph_steps(c, scheme, n_steps, t0, dt);
+    } else {
+      for (int s = 0; s < n_steps; ++s) one_step(c, scheme, t0 + s * dt, dt);
+    }
     HG_CUDA(cudaGetLastError());
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
@@ -603,6 +657,7 @@ extern "C" int hg_set_sensor(hg_ctx* c, int32_t kind, double s0, double kappa, c
       if (!d) d = dalloc<float>(n);
       HG_CUDA(cudaMemcpy(d, h, n * sizeof(float), cudaMemcpyHostToDevice));
     };
+    drop_graph(c);
     put(c->d_mlp, mlp, HG_MLP_PARAMS);
     put(c->d_feat_lo, lo, HG_SENSOR_FEATURES);
     put(c->d_feat_hi, hi, HG_SENSOR_FEATURES);

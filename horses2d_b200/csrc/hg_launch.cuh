@@ -9,13 +9,21 @@ void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   const int grid = (a.n_el + EPB - 1) / EPB;
   static bool attr = false;
   if (!attr) {
-    max_carveout(stage_kernel<P, EPB, real, true>);
-    max_carveout(stage_kernel<P, EPB, real, false>);
+    max_carveout(stage_kernel<P, EPB, real, true, false>);
+    max_carveout(stage_kernel<P, EPB, real, false, false>);
+    max_carveout(stage_kernel<P, EPB, real, true, true>);
+    max_carveout(stage_kernel<P, EPB, real, false, true>);
     attr = true;
   }
+  const bool lgl = c->node_type == HG_NODES_LGL;
   timed(c, HG_KERNEL_STAGE, [&] {
-    if (c->affine) stage_kernel<P, EPB, real, true><<<grid, block_for(P), 0, c->stream>>>(a);
-    else stage_kernel<P, EPB, real, false><<<grid, block_for(P), 0, c->stream>>>(a);
+    if (c->affine) {
+      if (lgl) stage_kernel<P, EPB, real, true, true><<<grid, block_for(P), 0, c->stream>>>(a);
+      else stage_kernel<P, EPB, real, true, false><<<grid, block_for(P), 0, c->stream>>>(a);
+    } else {
+      if (lgl) stage_kernel<P, EPB, real, false, true><<<grid, block_for(P), 0, c->stream>>>(a);
+      else stage_kernel<P, EPB, real, false, false><<<grid, block_for(P), 0, c->stream>>>(a);
+    }
   });
   ++c->launches;
 }

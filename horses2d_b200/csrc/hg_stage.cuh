@@ -65,7 +65,14 @@ __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || 
 
 // AFFINE: metrics constant per element (vol_geo [n_el][5]) and normals/dS constant
 // per side (side_geo [n_el*4][3]), as for parallelogram elements with straight edges.
-template <int P, int EPB, typename real, bool AFFINE>
+// LGL: Gauss-Lobatto nodes, whose boundary interpolants are unit vectors (lb = e_0 / e_N): traces are
+// node values and the lift touches only the boundary rows -- the same arithmetic as the dense form
+// with its exact zeros left out.
+__host__ __device__ constexpr int face_node(int P, int side, int l, int kk) {
+  return (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
+}
+
+template <int P, int EPB, typename real, bool AFFINE, bool LGL>
 __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) {
   constexpr int NP = P * P;
   constexpr int FT = 4 * P;
@@ -87,9 +94,10 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
   ph.load(a.pc);
   const int i = tid % P, j = tid / P;
 
+  const size_t off = (size_t(e) * NP + tid) * 4;
   real geo[5];
   if (active) {
-    const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
+    const double2* qp = reinterpret_cast<const double2*>(a.Q + off);
     const double2 q01 = qp[0], q23 = qp[1];
     const real q[4] = {real(q01.x), real(q01.y), real(q23.x), real(q23.y)};
     const real* gp = AFFINE ? a.vol_geo + size_t(e) * 5 : a.vol_geo + (size_t(e) * NP + tid) * 5;
@@ -119,14 +127,20 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
       const int kind = sd.y & 15;
       const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
       real qo[4] = {real(0), real(0), real(0), real(0)};
+      if (LGL) {
+        const int node = face_node(P, s, (s == 0 || s == 3) ? 0 : P - 1, kk);
 #pragma unroll
-      for (int l = 0; l < P; ++l) {
-        const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+        for (int k = 0; k < 4; ++k) qo[k] = s_Q[k][le][node];
+      } else {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) qo[k] += s_Q[k][le][node] * lbv[l];
+        for (int l = 0; l < P; ++l) {
+          const int node = face_node(P, s, l, kk);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) qo[k] += s_Q[k][le][node] * lbv[l];
+        }
       }
       const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + s) * 3 : a.side_geo + ((size_t(e) * 4 + s) * P + kk) * 3;
-      const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
+      const real nx = g3[0], ny = g3[1], dS = g3[2];
       real F[4];
       if (kind == SIDE_WALL) {
         euler_wall_flux(ph, qo, nx, ny, dS, F);
@@ -172,13 +186,19 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
     // lift: bottom F(i) lbw0(j), right F(j) lbw1(i), top F(i) lbw1(j), left F(j) lbw0(i)
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      qd[k] = qd[k] - s_F[k][le][0 * P + i] * lbw0[j];
-      qd[k] = qd[k] - s_F[k][le][1 * P + j] * lbw1[i];
-      qd[k] = qd[k] - s_F[k][le][2 * P + i] * lbw1[j];
-      qd[k] = qd[k] - s_F[k][le][3 * P + j] * lbw0[i];
+      if (LGL) {
+        if (j == 0) qd[k] = qd[k] - s_F[k][le][0 * P + i] * lbw0[0];
+        if (i == P - 1) qd[k] = qd[k] - s_F[k][le][1 * P + j] * lbw1[P - 1];
+        if (j == P - 1) qd[k] = qd[k] - s_F[k][le][2 * P + i] * lbw1[P - 1];
+        if (i == 0) qd[k] = qd[k] - s_F[k][le][3 * P + j] * lbw0[0];
+      } else {
+        qd[k] = qd[k] - s_F[k][le][0 * P + i] * lbw0[j];
+        qd[k] = qd[k] - s_F[k][le][1 * P + j] * lbw1[i];
+        qd[k] = qd[k] - s_F[k][le][2 * P + i] * lbw1[j];
+        qd[k] = qd[k] - s_F[k][le][3 * P + j] * lbw0[i];
+      }
       qd[k] = qd[k] * geo[4];
     }
-    const size_t off = (size_t(e) * NP + tid) * 4;
     if (a.QDot) {
       double2* dp = reinterpret_cast<double2*>(a.QDot + off);
       dp[0] = make_double2(double(qd[0]), double(qd[1]));
@@ -231,11 +251,17 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
       const int s = t / P, kk = t % P;
       const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
       real tr[4] = {real(0), real(0), real(0), real(0)};
+      if (LGL) {
+        const int node = face_node(P, s, (s == 0 || s == 3) ? 0 : P - 1, kk);
 #pragma unroll
-      for (int l = 0; l < P; ++l) {
-        const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+        for (int k = 0; k < 4; ++k) tr[k] = s_Q[k][le][node];
+      } else {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
+        for (int l = 0; l < P; ++l) {
+          const int node = face_node(P, s, l, kk);
+#pragma unroll
+          for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
+        }
       }
       real* tp = a.T_out + ((size_t(e) * 4 + s) * P + kk) * 4;
 #pragma unroll
