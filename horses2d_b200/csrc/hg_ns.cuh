@@ -89,6 +89,21 @@ __device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE>& s,
   return t;
 }
 
+// The four variables' traces at face node kk of side `side` (the interpolant weights loaded once).
+template <int P, int EPB, typename real>
+__device__ __forceinline__ void trace4(const real (*src)[EPB][P * P], int le, int side, int kk, const real* lbv,
+                                       real* out) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) out[k] = real(0);
+#pragma unroll
+  for (int l = 0; l < P; ++l) {
+    const int node = (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
+    const real w = lbv[l];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] += src[k][le][node] * w;
+  }
+}
+
 // Element gradient into s.dQ (both kernels).  Requires s.Q (and s.Ja) filled and synchronized.
 template <int P, int EPB, typename real, bool AFFINE, bool IP>
 __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
@@ -111,8 +126,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
         const int kind = sd.y & 15;
         const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
         real qo[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+        trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
         const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
         const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
         real us[4];
@@ -140,46 +154,63 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
     if constexpr (AFFINE) { Ja00 = geoE[0]; Ja01 = geoE[1]; Ja10 = geoE[2]; Ja11 = geoE[3]; iJ = geoE[4]; }
     else { Ja00 = s.Ja[0][le][tid]; Ja01 = s.Ja[1][le][tid]; Ja10 = s.Ja[2][le][tid]; Ja11 = s.Ja[3][le][tid];
            iJ = real(1) / s.Ja[4][le][tid]; }
+    // the operator rows and metrics of a node are loaded once per l and reused for the 4 variables
     if (IP) {
+      real dxi[4] = {real(0), real(0), real(0), real(0)}, deta[4] = {real(0), real(0), real(0), real(0)};
+#pragma unroll
+      for (int l = 0; l < P; ++l) {
+        const real di = D[i * P + l], dj = D[j * P + l];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          dxi[k] += di * s.Q[k][le][j * P + l];
+          deta[k] += dj * s.Q[k][le][l * P + i];
+        }
+      }
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        real dxi = real(0), deta = real(0);
-#pragma unroll
-        for (int l = 0; l < P; ++l) {
-          dxi += D[i * P + l] * s.Q[k][le][j * P + l];
-          deta += D[j * P + l] * s.Q[k][le][l * P + i];
-        }
-        s.dQ[0][k][le][tid] = (dxi * Ja00 + deta * Ja01) * iJ;
-        s.dQ[1][k][le][tid] = (dxi * Ja10 + deta * Ja11) * iJ;
+        s.dQ[0][k][le][tid] = (dxi[k] * Ja00 + deta[k] * Ja01) * iJ;
+        s.dQ[1][k][le][tid] = (dxi[k] * Ja10 + deta[k] * Ja11) * iJ;
       }
     } else {
+      real v0[4] = {real(0), real(0), real(0), real(0)}, v1[4] = {real(0), real(0), real(0), real(0)};
+      if constexpr (AFFINE) {
+        real axi[4] = {real(0), real(0), real(0), real(0)}, aeta[4] = {real(0), real(0), real(0), real(0)};
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        real v0 = real(0), v1 = real(0);
-        if constexpr (AFFINE) {
-          real axi = real(0), aeta = real(0);
+        for (int l = 0; l < P; ++l) {
+          const real hi = hatD[i * P + l], hj = hatD[j * P + l];
 #pragma unroll
-          for (int l = 0; l < P; ++l) {
-            axi += hatD[i * P + l] * s.Q[k][le][j * P + l];
-            aeta += hatD[j * P + l] * s.Q[k][le][l * P + i];
-          }
-          v0 = axi * Ja00 + aeta * Ja01;
-          v1 = axi * Ja10 + aeta * Ja11;
-        } else {
-#pragma unroll
-          for (int l = 0; l < P; ++l) {
-            const int nx_ = j * P + l, ny_ = l * P + i;
-            const real qx = s.Q[k][le][nx_] * hatD[i * P + l], qy = s.Q[k][le][ny_] * hatD[j * P + l];
-            v0 += qx * s.Ja[0][le][nx_] + qy * s.Ja[1][le][ny_];
-            v1 += qx * s.Ja[2][le][nx_] + qy * s.Ja[3][le][ny_];
+          for (int k = 0; k < 4; ++k) {
+            axi[k] += hi * s.Q[k][le][j * P + l];
+            aeta[k] += hj * s.Q[k][le][l * P + i];
           }
         }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          v0[k] = axi[k] * Ja00 + aeta[k] * Ja01;
+          v1[k] = axi[k] * Ja10 + aeta[k] * Ja11;
+        }
+      } else {
+#pragma unroll
+        for (int l = 0; l < P; ++l) {
+          const int nx_ = j * P + l, ny_ = l * P + i;
+          const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+          const real j0 = s.Ja[0][le][nx_], j1 = s.Ja[1][le][ny_], j2 = s.Ja[2][le][nx_], j3 = s.Ja[3][le][ny_];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const real qx = s.Q[k][le][nx_] * hi, qy = s.Q[k][le][ny_] * hj;
+            v0[k] += qx * j0 + qy * j1;
+            v1[k] += qx * j2 + qy * j3;
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
         const real l0 = s.face[k][le][0 * P + i] * lbw0[j] + s.face[k][le][1 * P + j] * lbw1[i] +
                         s.face[k][le][2 * P + i] * lbw1[j] + s.face[k][le][3 * P + j] * lbw0[i];
         const real l1 = s.face[4 + k][le][0 * P + i] * lbw0[j] + s.face[4 + k][le][1 * P + j] * lbw1[i] +
                         s.face[4 + k][le][2 * P + i] * lbw1[j] + s.face[4 + k][le][3 * P + j] * lbw0[i];
-        s.dQ[0][k][le][tid] = (-v0 + l0) * iJ;
-        s.dQ[1][k][le][tid] = (-v1 + l1) * iJ;
+        s.dQ[0][k][le][tid] = (-v0[k] + l0) * iJ;
+        s.dQ[1][k][le][tid] = (-v1[k] + l1) * iJ;
       }
     }
   }
@@ -238,8 +269,7 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
       const int kind = sd.y & 15;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
       real qo[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+      trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
       const size_t sbase = size_t(e) * 4 + sd_;
       real qn0, qn3;
       bool node0 = true;
@@ -321,10 +351,11 @@ __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a
     const int sd_ = t / P, kk = t % P;
     const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
     real* gp = a.GT + ((size_t(e) * 4 + sd_) * P + kk) * 8;
+    real tx[4], ty[4];
+    trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, tx);
+    trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, ty);
 #pragma unroll
-    for (int d = 0; d < 2; ++d)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) gp[d * 4 + k] = trace_of(s, s.dQ[d], k, le, sd_, kk, lbv);
+    for (int k = 0; k < 4; ++k) { gp[k] = tx[k]; gp[4 + k] = ty[k]; }
   }
 }
 
@@ -415,14 +446,10 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       const int kind = sd.y & 15;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
       real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
-#pragma unroll
-      for (int k = 0; k < 4; ++k) qo[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+      trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
       if (visc) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          gox[k] = trace_of(s, s.dQ[0], k, le, sd_, kk, lbv);
-          goy[k] = trace_of(s, s.dQ[1], k, le, sd_, kk, lbv);
-        }
+        trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, gox);
+        trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, goy);
       }
       const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
       const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
@@ -620,8 +647,10 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       const int sd_ = t / P, kk = t % P;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
       real* tp = a.T_out + ((size_t(e) * 4 + sd_) * P + kk) * 4;
+      real tr[4];
+      trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, tr);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) tp[k] = trace_of(s, s.Q, k, le, sd_, kk, lbv);
+      for (int k = 0; k < 4; ++k) tp[k] = tr[k];
     }
   }
 }
