@@ -14,7 +14,8 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "libhorsesgpu.so")
 OBJ_DIR = os.path.join(HERE, "_build")
-SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu", "csrc/hg_mlp.cu", "csrc/hg_inst_euler.cu",
+SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu", "csrc/hg_mlp.cu", "csrc/hg_exact.cu",
+           "csrc/hg_inst_euler.cu",
            "csrc/hg_inst_sensor.cu"] + \
     [f"csrc/hg_inst_ns{prec}{part}.cu" for prec in ("64", "32") for part in "abcd"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -39,7 +39,8 @@ static void free_ctx(hg_ctx* c) {
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
-                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ};
+                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
+                  c->d_FX, c->d_bq};
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
@@ -76,6 +77,8 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.jac = static_cast<const real*>(c->d_jac);
   a.mats = c->d_mats;
   a.zones = c->d_zones;
+  a.bq = c->d_bq;
+  a.FX = static_cast<const real*>(c->d_FX);
   a.Q = c->d_Q;
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
@@ -103,6 +106,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.side_area = c->d_side_area;
   a.mu_av = c->d_mu_av;
   a.sensor = sensor_args(c);
+  if (c->exact) launch_exact_flux<real>(c);
   HG_DISPATCH_P(c->P, launch_ns_P, c, a);
   if (update) c->cur ^= 1;
 }
@@ -117,6 +121,8 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.vol_geo = static_cast<const real*>(c->d_vol_geo);
   a.mats = c->d_mats;
   a.zones = c->d_zones;
+  a.bq = c->d_bq;
+  a.FX = static_cast<const real*>(c->d_FX);
   a.Q = c->d_Q;
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
@@ -128,6 +134,7 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.update = update ? 1 : 0;
   a.riemann = c->riemann;
   a.pc = c->pc;
+  if (c->exact) launch_exact_flux<real>(c);
   HG_DISPATCH_P(c->P, launch_stage_P, c, a);
   if (update) c->cur ^= 1;
 }
@@ -206,7 +213,6 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->sigma0 = ph->sigma0_ip;
   c->epsilon = ph->ip_method == 0 ? -1.0 : (ph->ip_method == 1 ? 1.0 : 0.0);
   c->n_el = E; c->N = N; c->P = P; c->node_type = ph->node_type; c->riemann = ph->riemann;
-  if (c->riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
   c->ndof = int64_t(E) * NP * 4;
   const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
   c->gamma = gamma; c->mach = ph->mach;
@@ -246,7 +252,10 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
 
   // zones
   std::vector<Zone> zones(std::max(1, n_bcs));
+  c->zone_type.assign(std::max(1, n_bcs), -1);
+  c->zone_row0.assign(std::max(1, n_bcs), -1);
   for (int z = 0; z < n_bcs; ++z) {
+    c->zone_type[z] = bcs[z].type;
     zones[z].type = bcs[z].type;
     zones[z].riemann = bcs[z].riemann;
     for (int k = 0; k < 4; ++k) zones[z].q[k] = bcs[z].state[k];
@@ -257,11 +266,13 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
     zones[z].outflow_type = bcs[z].outflow_type;
     zones[z].nd_mode = bcs[z].nd_mode;
     zones[z].nd_outflow_total = bcs[z].nd_outflow_total;
-    if (bcs[z].riemann == HG_RIEMANN_EXACT) throw std::runtime_error("exact Riemann solver is not available on the device");
+    if (bcs[z].riemann == HG_RIEMANN_EXACT) c->exact = true;
   }
 
   // side tables
-  std::vector<int4> side(size_t(E) * 4, make_int4(-2, 0, -1, 0));
+  // {neighbour trace slot, flags, zone, per-node state row}; rows are assigned by hg_set_boundary_state
+  std::vector<int4> side(size_t(E) * 4, make_int4(-2, 0, -1, -1));
+  c->zone_sides.assign(std::max(1, n_bcs), std::vector<int>());
   std::vector<double> sinvh(size_t(E) * 4, 0.0);
   std::vector<double> sg(size_t(E) * 4 * P * 3, 0.0);
   auto set_geo = [&](int e, int s, int edge, bool rev) {
@@ -281,8 +292,8 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
     const int marker = m->edge_marker[f];
     if (marker == 0) {
       if (R < 0 || R >= E || sR < 0 || sR > 3) throw std::runtime_error("interior edge without RIGHT element");
-      side[size_t(L) * 4 + sL] = make_int4(R * 4 + sR, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), -1, 0);
-      side[size_t(R) * 4 + sR] = make_int4(L * 4 + sL, SIDE_RIGHT | (inv ? SIDE_REVERSED : 0), -1, 0);
+      side[size_t(L) * 4 + sL] = make_int4(R * 4 + sR, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), -1, -1);
+      side[size_t(R) * 4 + sR] = make_int4(L * 4 + sL, SIDE_RIGHT | (inv ? SIDE_REVERSED : 0), -1, -1);
       set_geo(L, sL, f, false);
       set_geo(R, sR, f, inv);
       if (m->edge_invh) sinvh[size_t(L) * 4 + sL] = sinvh[size_t(R) * 4 + sR] = m->edge_invh[f];
@@ -295,17 +306,18 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
           const int p = m->periodic_partner ? m->periodic_partner[f] : -1;
           if (p < 0 || p >= m->n_edges) throw std::runtime_error("periodic edge without partner");
           const int pe = m->edge_elem[2 * p], ps = m->edge_side[2 * p] - 1;
-          side[size_t(L) * 4 + sL] = make_int4(pe * 4 + ps, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), z, 0);
+          side[size_t(L) * 4 + sL] = make_int4(pe * 4 + ps, SIDE_LEFT | (inv ? SIDE_REVERSED : 0), z, -1);
           break;
         }
-        case HG_BC_EULERWALL: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_WALL, z, 0); break;
+        case HG_BC_EULERWALL: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_WALL, z, -1); break;
         case HG_BC_DIRICHLET:
         case HG_BC_VISCOUSWALL:
         case HG_BC_FARFIELD:
         case HG_BC_PRESSUREOUTLET:
-        case HG_BC_NEWDIRICHLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, 0); break;
+        case HG_BC_NEWDIRICHLET: side[size_t(L) * 4 + sL] = make_int4(-1, SIDE_STATE, z, -1); break;
         default: throw std::runtime_error("unknown boundary condition kind");
       }
+      c->zone_sides[z].push_back(L * 4 + sL);
       set_geo(L, sL, f, false);
       if (m->edge_invh) sinvh[size_t(L) * 4 + sL] = m->edge_invh[f];
     }
@@ -417,6 +429,9 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
       upload_real(c->d_jac, m->jac, size_t(E) * NP);
     }
   }
+  if (c->riemann == HG_RIEMANN_EXACT) c->exact = true;
+  if (c->exact) c->d_FX = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
+  c->h_side = side;
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
@@ -703,6 +718,40 @@ extern "C" int hg_element_viscosity(hg_ctx* c, double* mu) {
   try {
     if (!c->d_mu_av) throw std::runtime_error("artificial dissipation is off for this context");
     HG_CUDA(cudaMemcpyAsync(mu, c->d_mu_av, size_t(c->n_el) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, int64_t n_values) {
+  try {
+    if (zone < 1 || zone > int(c->zone_type.size()) || c->zone_type[zone - 1] < 0)
+      throw std::runtime_error("unknown zone " + std::to_string(zone));
+    const int z = zone - 1;
+    if (c->zone_type[z] != HG_BC_DIRICHLET)
+      throw std::runtime_error("per-node boundary states apply to Dirichlet zones only");
+    const std::vector<int>& sides = c->zone_sides[z];
+    const int64_t expect = int64_t(sides.size()) * c->P * 4;
+    if (!uB || n_values != expect)
+      throw std::runtime_error("zone " + std::to_string(zone) + " takes " + std::to_string(expect) + " values");
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    if (c->zone_row0[z] < 0) {
+      // first call for this zone: give its sides consecutive rows and grow the state buffer
+      const int row0 = c->n_bq_rows, rows = row0 + int(sides.size());
+      double* nb = dalloc<double>(size_t(rows) * c->P * 4);
+      if (c->d_bq) {
+        HG_CUDA(cudaMemcpy(nb, c->d_bq, size_t(row0) * c->P * 4 * sizeof(double), cudaMemcpyDeviceToDevice));
+        HG_CUDA(cudaFree(c->d_bq));
+      }
+      c->d_bq = nb;
+      c->n_bq_rows = rows;
+      c->zone_row0[z] = row0;
+      for (size_t k = 0; k < sides.size(); ++k) c->h_side[sides[k]].w = row0 + int(k);
+      HG_CUDA(cudaMemcpy(c->d_side, c->h_side.data(), c->h_side.size() * sizeof(int4), cudaMemcpyHostToDevice));
+      drop_graph(c);   // captured launches hold the old buffer
+    }
+    HG_CUDA(cudaMemcpyAsync(c->d_bq + size_t(c->zone_row0[z]) * c->P * 4, uB, size_t(expect) * sizeof(double),
+                            cudaMemcpyHostToDevice, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }

@@ -109,10 +109,13 @@ __device__ __noinline__ int new_dirichlet_state(const Phys<real>& ph, const Zone
   return vbc;
 }
 
-// Returns the inviscid ghost uB, the viscous state uSB and the viscous condition.
+// Returns the inviscid ghost uB, the viscous state uSB and the viscous condition.  qnode, when
+// given, is this node's own Dirichlet state (a zone fed per node by hg_set_boundary_state: the
+// reference's boundary-condition function, BoundaryConditions/BoundaryConditionFunctionDrivers.incf);
+// otherwise a Dirichlet zone holds its constant state.
 template <typename real>
 __device__ __forceinline__ int bc_states(const Phys<real>& ph, const Zone& z, const real* q, real nx, real ny, real* uB,
-                                         real* uSB) {
+                                         real* uSB, const double* qnode = nullptr) {
   const real gm1 = ph.gm1, gamma = ph.gamma, cv = ph.cv;
   switch (z.type) {
     case BC_EULERWALL: {
@@ -138,8 +141,9 @@ __device__ __forceinline__ int bc_states(const Phys<real>& ph, const Zone& z, co
       return iso ? VBC_DIRICHLET : VBC_ADIABATIC;
     }
     case BC_DIRICHLET: {
+      const double* zs = qnode ? qnode : z.q;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) uB[k] = real(z.q[k]);
+      for (int k = 0; k < 4; ++k) uB[k] = real(zs[k]);
       const real rhoL = q[0], uL = q[1] / rhoL, vL = q[2] / rhoL;
       const real vnL = uL * nx + vL * ny;
       const real pL = gm1 * (q[3] - real(0.5) * (q[1] * uL + q[2] * vL));

@@ -51,6 +51,15 @@ struct hg_ctx {
   void* d_jac = nullptr;          // [n_el][NP] J (curved meshes), context precision
   void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
   void* d_dQ = nullptr;           // element gradients [n_el][2][4][NP] (Navier-Stokes)
+  bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
+  void* d_FX = nullptr;           // its face fluxes of the current stage [n_el*4][P][4], context precision
+  // zones fed per node (hg_set_boundary_state): state rows [rows][P][4] indexed by side.w
+  double* d_bq = nullptr;
+  int n_bq_rows = 0;
+  std::vector<std::vector<int>> zone_sides;   // per zone: element sides (e*4+s) of its edges, in mesh edge order
+  std::vector<int> zone_type;                 // per zone: HG_BC_*
+  std::vector<int> zone_row0;                 // per zone: first state row, -1 until fed per node
+  std::vector<int4> h_side;                   // host copy of the side table
   bool state_set = false;
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
@@ -123,6 +132,7 @@ template <int P, typename real> void launch_stage_P(hg_ctx* c, const StageArgs<r
 template <int P, typename real> void launch_trace_P(hg_ctx* c);
 template <int P, typename real> void launch_ns_P(hg_ctx* c, const NSArgs<real>& a);
 template <int P, typename real> void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out);
+template <typename real> void launch_exact_flux(hg_ctx* c);
 
 inline SensorArgs sensor_args(const hg_ctx* c) {
   SensorArgs s;

@@ -28,13 +28,15 @@ namespace hg {
 template <typename real>
 struct NSArgs {
   int n_el;
-  const int4* side;         // [n_el*4] {neighbour trace slot, flags, zone, 0}
+  const int4* side;         // [n_el*4] {neighbour trace slot, flags, zone, per-node state row or -1}
   const real* side_geo;     // normals / dS (per node, or per side when AFFINE)
   const double* side_invh;  // [n_el*4] invh of the side's edge
   const real* vol_geo;      // Ja00 Ja01 Ja10 Ja11 1/J (per node, or per element when AFFINE)
   const real* jac;          // [n_el][NP] J per node (curved meshes)
   const double* mats;       // hatD[NP] lb0 lb1 lbw0 lbw1 [P each] D[NP] dlbw0 dlbw1 [P each]
   const Zone* zones;
+  const double* bq;         // per-node Dirichlet states [rows][P][4] (sides whose side.w >= 0)
+  const real* FX;           // exact-solver face fluxes [n_el*4][P][4] of this stage (RIEMANN_EXACT faces)
   double* Q;
   real* G;
   const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
@@ -137,7 +139,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
           for (int k = 0; k < 4; ++k) us[k] = kind == SIDE_RIGHT ? real(0.5) * (tp[k] + qo[k]) : real(0.5) * (qo[k] + tp[k]);
         } else {
           real uB[4];
-          bc_states(ph, a.zones[sd.z], qo, nx, ny, uB, us);
+          bc_states(ph, a.zones[sd.z], qo, nx, ny, uB, us, sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
         }
         const real sg = kind == SIDE_RIGHT ? real(-1) : real(1);
 #pragma unroll
@@ -282,7 +284,8 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
       } else {
         const real* g3 = AFFINE ? a.side_geo + sbase * 3 : a.side_geo + (sbase * P + kk) * 3;
         real uB[4], uS[4];
-        bc_states(ph, a.zones[sd.z], qo, real(g3[0]), real(g3[1]), uB, uS);
+        bc_states(ph, a.zones[sd.z], qo, real(g3[0]), real(g3[1]), uB, uS,
+                  sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
         qn0 = uS[0];
         qn3 = uS[3];
       }
@@ -481,7 +484,7 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
         if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
         real Fi[4], FLx[4] = {real(0), real(0), real(0), real(0)}, FLy[4] = {real(0), real(0), real(0), real(0)};
         real FRx[4] = {real(0), real(0), real(0), real(0)}, FRy[4] = {real(0), real(0), real(0), real(0)};
-        riemann(solver, ph, QL, QR, nx, ny, Fi);
+        face_riemann(solver, ph, QL, QR, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
         if (visc) {
           viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
           viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
@@ -510,13 +513,13 @@ __global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
       } else {
         const Zone& z = a.zones[sd.z];
         real uB[4], uSB[4];
-        const int vbc = bc_states(ph, z, qo, nx, ny, uB, uSB);
+        const int vbc = bc_states(ph, z, qo, nx, ny, uB, uSB, sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
         real Fi[4];
         if (kind == SIDE_WALL) {
           euler_wall_flux(ph, qo, nx, ny, dS, Fi);
         } else {
           const int solver = z.riemann >= 0 ? z.riemann : a.riemann;
-          riemann(solver, ph, qo, uB, nx, ny, Fi);
+          face_riemann(solver, ph, qo, uB, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
 #pragma unroll
           for (int k = 0; k < 4; ++k) Fi[k] = Fi[k] * dS;
         }

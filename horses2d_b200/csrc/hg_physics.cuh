@@ -7,6 +7,7 @@
 //   inviscid_flux   Physics/InviscidFluxes.f90:104-147 (scaled by 1/(sqrt(gamma) M),
 //                   _DIMENSIONLESS_TAU)
 //   roe / hll       Physics/RiemannSolvers.f90:189-305 / 307-399
+//   exact           Physics/RiemannSolvers.f90:33-187, 405-459 (Newton on the star pressure)
 //   lxf             Rusanov flux, no reference counterpart; same rotation and scaling
 //   euler_wall      BoundaryConditions/EulerWall.incf:71-158 (prescribed wall flux)
 #pragma once
@@ -155,12 +156,145 @@ __device__ __forceinline__ void lxf(const Phys<real>& ph, const real* qL, const 
   rotate_back_scale(ph, F, nx, ny);
 }
 
+// Exact Riemann solver (Physics/RiemannSolvers.f90:33-187 with the star-pressure iteration of
+// :405-459), in the face-normal frame.  It runs in its own kernel (exact_flux_kernel, hg_exact.cu)
+// ahead of the stage kernels, which read its face fluxes: the iteration and its many pow calls
+// would otherwise widen the register budget of every fused kernel.
+template <typename real>
+struct ExactFace {
+  real qn[2][4];   // left / right conserved state, momentum rotated to (normal, tangential)
+  real w[2][5];    // left / right {rho, u_n, u_t, p, a}
+  real gamma, gm1, cp, cv;
+};
+
+// Wave curve f(p) of one side and its derivative (shock branch above the side's pressure,
+// rarefaction branch below).
+template <typename real>
+__device__ __forceinline__ void exact_wave(const ExactFace<real>& X, real p, const real* W, real& F, real& dF) {
+  if (p > W[3]) {
+    const real A = real(2) / (W[0] * (X.gamma + real(1)));
+    const real B = X.gm1 * W[3] / (X.gamma + real(1));
+    const real s = sqrt_r(A / (p + B));
+    F = (p - W[3]) * s;
+    dF = s * (real(1) - real(0.5) * (p - W[3]) / (B + p));
+  } else {
+    F = real(2) * X.cv * W[4] * (pow_r(p / W[3], real(0.5) / X.cp) - real(1));
+    dF = real(1) / (W[0] * W[4]) * pow_r(p / W[3], real(-0.5) * (X.gamma + real(1)) / X.gamma);
+  }
+}
+
+// Star pressure: two-rarefaction guess, then Newton (at most 50 steps, stop at relative change
+// 1e-6); returns u* through ustar.
+template <typename real>
+__device__ __forceinline__ real exact_star(const ExactFace<real>& X, real& ustar) {
+  const real* wL = X.w[0];
+  const real* wR = X.w[1];
+  real pstar = pow_r((wL[4] + wR[4] - real(0.5) * X.gm1 * (wR[1] - wL[1])) /
+                         (wL[4] / pow_r(wL[3], real(0.5) / X.cp) + wR[4] / pow_r(wR[3], real(0.5) / X.cp)),
+                     real(2) * X.cp);
+  real FL = real(0), dFL = real(0), FR = real(0), dFR = real(0);
+#pragma unroll 1
+  for (int it = 1; it <= 50; ++it) {
+    exact_wave(X, pstar, wL, FL, dFL);
+    exact_wave(X, pstar, wR, FR, dFR);
+    const real Fn = FL + FR + wR[1] - wL[1], dF = dFL + dFR;
+    const real pold = pstar;
+    pstar = pold - Fn / dF;
+    if (fabs(real(0.5) * fabs(pstar - pold) / (pstar + pold)) < real(1.0e-6)) {
+      exact_wave(X, pstar, wL, FL, dFL);
+      exact_wave(X, pstar, wR, FR, dFR);
+      break;
+    }
+  }
+  ustar = real(0.5) * (wL[1] + wR[1] + FR - FL);
+  return pstar;
+}
+
+// Godunov flux at x/t = 0 (normal frame, unscaled) with the reference's branch conditions; a state
+// that meets none of them gives a zero flux, as in the reference.
+template <typename real>
+__device__ __forceinline__ void exact_sample(const ExactFace<real>& X, real pstar, real ustar, real* F) {
+  const real gamma = X.gamma, cp = X.cp, cv = X.cv;
+  const real g1 = gamma + real(1), gq = (gamma - real(1)) / (gamma + real(1));
+  const int side = ustar >= real(0) ? 0 : 1;
+  const real* w = X.w[side];
+  real rs = real(0), us = real(0), vs = real(0), ps = real(0);
+  bool star = false, upw = false;
+  const real sr = pow_r(pstar / w[3], real(0.5) / cp);
+  if (side == 0) {
+    const real ss = sqrt_r(g1 / (real(2) * gamma) * pstar / w[3] + real(0.5) / cp);
+    if (pstar <= w[3] && w[1] >= w[4]) upw = true;
+    else if (pstar <= w[3] && w[1] < w[4] && ustar < w[4] * sr) { rs = w[0] * pow_r(pstar / w[3], real(1) / gamma); star = true; }
+    else if (pstar <= w[3] && w[1] < w[4] && ustar >= w[4] * sr) {
+      us = real(2) * w[4] / g1 + (gamma - real(1)) / g1 * w[1];
+      rs = w[0] * pow_r(us / w[4], real(2) * cv);
+      ps = w[3] * pow_r(rs / w[0], gamma); vs = w[2];
+    } else if (pstar > w[3] && w[1] >= w[4] * ss) upw = true;
+    else if (pstar > w[3] && w[1] < w[4] * ss) {
+      rs = w[0] * ((pstar / w[3] + gq) / (pstar / w[3] * (gamma - real(1)) / g1 + real(1))); star = true;
+    }
+  } else {
+    if (pstar <= w[3] && w[1] + w[4] <= real(0)) upw = true;
+    else if (pstar <= w[3] && w[1] + w[4] >= real(0) && ustar + w[4] * sr >= real(0)) {
+      rs = w[0] * pow_r(pstar / w[3], real(1) / gamma); star = true;
+    } else if (pstar <= w[3] && w[1] + w[4] > real(0) && ustar + w[4] * sr < real(0)) {
+      us = real(-2) * w[4] / g1 + (gamma - real(1)) / g1 * w[1];
+      rs = w[0] * pow_r(-us / w[4], real(2) * cv);
+      ps = w[3] * pow_r(rs / w[0], gamma); vs = w[2];
+    } else if (pstar > w[3] && w[1] + w[4] * (real(0.5) * g1 / gamma * pstar / w[3] + real(0.5) / cp) <= real(0)) upw = true;
+    else if (pstar > w[3] && w[1] + w[4] * (g1 / (real(2) * gamma) * pstar / w[3] + real(0.5) / cp) > real(0)) {
+      rs = w[0] * ((pstar / w[3] + gq) / (pstar / w[3] * (gamma - real(1)) / g1 + real(1))); star = true;
+    }
+  }
+  if (star) { us = ustar; vs = w[2]; ps = pstar; }
+  if (upw) {
+    const real* qn = X.qn[side];
+    F[0] = qn[1]; F[1] = qn[1] * w[1] + w[3]; F[2] = qn[2] * w[1];
+    F[3] = w[1] * (cp * w[3] + real(0.5) * (qn[1] * w[1] + qn[2] * w[2]));
+  } else {
+    F[0] = rs * us; F[1] = rs * us * us + ps; F[2] = rs * us * vs;
+    F[3] = us * (cp * ps + real(0.5) * rs * (us * us + vs * vs));
+  }
+}
+
+template <typename real>
+__device__ __forceinline__ void exact(const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny, real* F) {
+  ExactFace<real> X;
+  X.gamma = ph.gamma; X.gm1 = ph.gm1; X.cp = ph.cp; X.cv = ph.cv;
+  const real* q[2] = {qL, qR};
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    real* qn = X.qn[s];
+    real* w = X.w[s];
+    qn[0] = q[s][0]; qn[1] = q[s][1] * nx + q[s][2] * ny; qn[2] = -q[s][1] * ny + q[s][2] * nx; qn[3] = q[s][3];
+    w[0] = qn[0]; w[1] = qn[1] / qn[0]; w[2] = qn[2] / qn[0];
+    w[3] = ph.gm1 * (qn[3] - real(0.5) * (qn[1] * w[1] + qn[2] * w[2])); w[4] = sqrt_r(ph.gamma * w[3] / w[0]);
+  }
+  real ustar;
+  const real pstar = exact_star(X, ustar);
+  exact_sample(X, pstar, ustar, F);
+  rotate_back_scale(ph, F, nx, ny);
+}
+
 template <typename real>
 __device__ __forceinline__ void riemann(int which, const Phys<real>& ph, const real* qL, const real* qR, real nx, real ny,
                                         real* F) {
   if (which == RIEMANN_HLL) hll(ph, qL, qR, nx, ny, F);
   else if (which == RIEMANN_LXF) lxf(ph, qL, qR, nx, ny, F);
   else roe(ph, qL, qR, nx, ny, F);
+}
+
+// Riemann flux of one face node in a stage kernel: the exact solver's value is read from the face
+// flux buffer [n_el*4][P][4] that exact_flux_kernel filled for this stage (same arguments).
+template <typename real>
+__device__ __forceinline__ void face_riemann(int which, const Phys<real>& ph, const real* qL, const real* qR, real nx,
+                                             real ny, const real* FX, size_t slot, real* F) {
+  if (which == RIEMANN_EXACT) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) F[k] = FX[slot * 4 + k];
+  } else {
+    riemann(which, ph, qL, qR, nx, ny, F);
+  }
 }
 
 // Prescribed Euler-wall flux F(q_wall) . n dS, q_wall = interior state with the normal momentum removed.

@@ -37,11 +37,13 @@ constexpr int SIDE_REVERSED = 16;
 template <typename real>
 struct StageArgs {
   int n_el;
-  const int4* side;        // [n_el*4] {neighbour trace slot, flags, zone, 0}
+  const int4* side;        // [n_el*4] {neighbour trace slot, flags, zone, per-node state row or -1}
   const real* side_geo;    // [n_el*4][P][3] (or [n_el*4][3] affine)  nx, ny, dS in this element's side order
   const real* vol_geo;     // [n_el][P*P][5] (or [n_el][5] affine)  Ja00 Ja01 Ja10 Ja11 1/J
   const double* mats;      // hatD[P*P], lb0[P], lb1[P], lbw0[P], lbw1[P]
   const Zone* zones;
+  const double* bq;        // per-node Dirichlet states [rows][P][4] (sides whose side.w >= 0)
+  const real* FX;          // exact-solver face fluxes [n_el*4][P][4] of this stage (RIEMANN_EXACT faces)
   double* Q;               // [n_el][P*P][4]
   real* G;                 // [n_el][P*P][4]
   const real* T_in;        // [n_el*4][P][4]
@@ -150,7 +152,7 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
         if (kind == SIDE_STATE) {
           const Zone& z = a.zones[sd.z];
           real us[4];
-          bc_states(ph, z, qo, nx, ny, qn, us);
+          bc_states(ph, z, qo, nx, ny, qn, us, sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
           if (z.riemann >= 0) solver = z.riemann;
         } else {
           const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
@@ -160,11 +162,11 @@ __global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) 
           if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
         }
         if (kind == SIDE_RIGHT) {
-          riemann(solver, ph, qn, qo, nx, ny, F);
+          face_riemann(solver, ph, qn, qo, nx, ny, a.FX, (size_t(e) * 4 + s) * P + kk, F);
 #pragma unroll
           for (int k = 0; k < 4; ++k) F[k] = -(F[k] * dS);
         } else {
-          riemann(solver, ph, qo, qn, nx, ny, F);
+          face_riemann(solver, ph, qo, qn, nx, ny, a.FX, (size_t(e) * 4 + s) * P + kk, F);
 #pragma unroll
           for (int k = 0; k < 4; ++k) F[k] = F[k] * dS;
         }

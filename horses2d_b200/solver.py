@@ -192,6 +192,12 @@ class GpuDGSEM:
         self._check(self._lib.hg_sensor_eval(self._h, f.ctypes.data_as(L.F32P), o.ctypes.data_as(L.F64P)))
         return f, o
 
+    def set_boundary_state(self, zone, uB):
+        """Per-node states of Dirichlet zone `zone` (1-based marker): the reference's boundary-condition
+        function evaluated at the zone's edge nodes, [edges x (N+1)] x 4 in mesh edge order."""
+        uB = np.ascontiguousarray(uB, dtype=np.float64).ravel()
+        self._check(self._lib.hg_set_boundary_state(self._h, int(zone), uB.ctypes.data_as(L.F64P), uB.size))
+
     def element_viscosity(self):
         n = self.info()["n_elements"]
         mu = np.zeros(n)

@@ -122,6 +122,15 @@ int  hg_residuals(hg_ctx* ctx, double out[4]);
 /* == EstimateTimeStep, including the reference's running maxima (SAVE). */
 int  hg_estimate_dt(hg_ctx* ctx, double cfl, double dt_cap, double* dt);
 
+/* Dirichlet zone fed per node: the problem file's boundary-condition function
+ * (BoundaryConditions/BoundaryConditionFunctionDrivers.incf, DirichletBC with a user
+ * function), evaluated by the caller at the zone's edge nodes.  uB holds N+1 conservative
+ * dimensionless states per edge of zone `zone` (1-based marker), edges in mesh order and
+ * nodes in the edge's own order: n_values = edges x (N+1) x 4.  The states are held until
+ * the next call and replace the zone's constant state in every later stage.  Other zone
+ * kinds recompute their ghost state from the zone state each stage and are rejected. */
+int  hg_set_boundary_state(hg_ctx* ctx, int32_t zone, const double* uB, int64_t n_values);
+
 /* Stream control: run on the caller's stream (e.g. a framework's current stream). */
 int  hg_set_stream(hg_ctx* ctx, void* cuda_stream);
 int  hg_synchronize(hg_ctx* ctx);
@@ -136,7 +145,7 @@ int64_t hg_launch_count(const hg_ctx* ctx);
  * hg_kernel_times synchronises and returns, per HG_KERNEL_* class (first n),
  * the summed milliseconds and the launch count since timing started. */
 enum { HG_KERNEL_STAGE = 0, HG_KERNEL_GRADIENT = 1, HG_KERNEL_TRACE = 2, HG_KERNEL_REDUCE = 3,
-       HG_KERNEL_SPEED = 4, HG_KERNEL_KINDS = 5 };
+       HG_KERNEL_SPEED = 4, HG_KERNEL_FACEFLUX = 5, HG_KERNEL_KINDS = 6 };
 int  hg_profile(hg_ctx* ctx, int32_t enable);
 int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
 /* hg_residuals_noalloc -- no reference counterpart.  Per-variable max |x| (the reduction of

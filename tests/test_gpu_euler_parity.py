@@ -37,6 +37,42 @@ def test_residual_periodic_vortex(nodes, N, riemann):
     assert np.allclose(res, np.abs(ref.reshape(-1, 4)).max(0), rtol=1e-11)
 
 
+@pytest.mark.parametrize("case", ["vortex", "supersonic_jumps"])
+def test_exact_riemann_solver(case):
+    """Exact Riemann solver (Newton on the star pressure, its own face-flux kernel): subsonic vortex
+    faces, and a Mach 1.5 stream with density / pressure jumps that reaches the supersonic, shock and
+    fan branches; residual and 10 RK3 steps."""
+    from horses2d_b200 import mesh as hmesh, cases as hcases
+    mach = 0.5 if case == "vortex" else 1.5
+    m = hmesh.cartesian(8, 8, -5.0, 5.0, -5.0, 5.0)
+    orc = O.Oracle(m, 4, nodes=O.LG, riemann=O.EXACT, mach=mach, bcs=hmesh.periodic_bcs_cartesian())
+    X = orc.coords()
+    if case == "vortex":
+        Q = perturbed(hcases.isentropic_vortex(X[:, 0], X[:, 1], mach=mach).ravel(), 0.02, seed=21)
+    else:
+        left = X[:, 0] < 0.3
+        rho = np.where(left, 1.0, 0.3)
+        p = np.where(left, 1.0, 0.25) * (1.0 + 0.5 * (X[:, 1] > 1.1))
+        u = np.where(left, 1.0, -0.4) + 0.3 * np.sin(X[:, 1])
+        v = 0.4 * np.cos(X[:, 0])
+        Q = perturbed(np.stack([rho, rho * u, rho * v, p / 0.4 + 0.5 * rho * (u * u + v * v)], 1).ravel(),
+                      0.01, seed=22)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g = hg.GpuDGSEM(orc.export_mesh(), mach=mach, node_type=hg.NODES_LG, riemann=hg.EXACT,
+                    bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    g.set_state(Q)
+    g.profile(True)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= TOL_STAGE
+    assert g.kernel_times()["face_flux"][1] == 1      # one exact-flux launch ahead of the stage kernel
+    g.profile(False)
+    dt = orc.estimate_dt(0.1, 1.0)
+    for s in range(10):
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, 10, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_STAGE * 10
+
+
 def test_rk3_stage_and_100_steps():
     orc, Q0, prm = vortex_case(n=16, N=4)
     orc.set_state(Q0)

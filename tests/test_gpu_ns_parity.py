@@ -71,7 +71,7 @@ def test_cylinder_ns_residual(N, nodes, viscous, ip):
     assert np.allclose(g.residuals(), np.abs(ref.reshape(-1, 4)).max(0), rtol=1e-11)
 
 
-@pytest.mark.parametrize("wall,riemann", [("adiabatic", O.HLL), ("isothermal", O.LXF)])
+@pytest.mark.parametrize("wall,riemann", [("adiabatic", O.HLL), ("isothermal", O.LXF), ("isothermal", O.EXACT)])
 def test_cylinder_ns_wall_types_and_fluxes(wall, riemann):
     orc, kw, Q0 = cylinder_ns(4, O.LG, O.BR1, wall=wall, riemann=riemann)
     _, out, ref = residual_pair(orc, kw, perturbed(Q0, 0.02, seed=3))
@@ -131,3 +131,54 @@ def test_ns_on_package_built_ogrid():
     Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=9)
     _, out, ref = residual_pair(orc, kw, Q, mesh=hmesh.build_descriptor(m, 5, hg.NODES_LG))
     assert rel_l2(out, ref) <= TOL_STAGE
+
+
+def test_zone_riemann_override_exact():
+    """Roe inside, the exact solver on the Dirichlet and far-field zones (per-zone override)."""
+    m = load_mesh("CylinderBench")
+    T_ref = 273.15
+    obcs = [dict(type=O.BC_DIRICHLET, riemann=O.EXACT), dict(type=O.BC_FARFIELD, riemann=O.EXACT),
+            dict(type=O.BC_FARFIELD), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2),
+            dict(type=O.BC_VISCOUSWALL, wall_type=1, wall_T=1.1 * T_ref)]
+    orc = O.Oracle(m, 3, nodes=O.LGL, riemann=O.ROE, mach=MACH, reynolds=RE, navier_stokes=1, viscous=O.BR1,
+                   bcs=obcs)
+    q = dirichlet_state(orc, MACH)
+    gbcs = [dict(type=hg.BC_DIRICHLET, state=q, riemann=hg.EXACT), dict(type=hg.BC_FARFIELD, state=q, riemann=hg.EXACT),
+            dict(type=hg.BC_FARFIELD, state=q), dict(type=hg.BC_PRESSUREOUTLET, state=q, outflow_type=2),
+            dict(type=hg.BC_VISCOUSWALL, wall_type=1, wall_T=1.1)]
+    kw = dict(mach=MACH, reynolds=RE, navier_stokes=1, viscous=hg.BR1, node_type=hg.NODES_LGL, riemann=hg.ROE,
+              bcs=gbcs)
+    _, out, ref = residual_pair(orc, kw, perturbed(np.tile(q, orc.ndof // 4), 0.02, seed=13))
+    assert rel_l2(out, ref) <= TOL_STAGE
+
+
+def test_zone_fed_per_node():
+    """A Dirichlet zone fed per node (the reference's boundary-condition function; here a free stream
+    with a varying density) against the oracle's per-node zone state, on the cylinder mesh with every
+    other zone kind present; the states persist over RK steps, a second call replaces them."""
+    orc, kw, Q0 = cylinder_ns(4, O.LG, O.BR1)
+    Q = perturbed(Q0, 0.01, seed=12)
+    Xb = orc.zone_edge_nodes(1)
+    q = orc.zone_state(1)
+    g = hg.GpuDGSEM(orc.export_mesh(), **kw)
+    g.set_state(Q)
+    before = g.compute_time_derivative(0.0)
+    for amp in (0.05, -0.03):
+        uB = (q[None, :] * (1.0 + amp * np.sin(3.0 * Xb[:, 0:1]) + 0.02 * Xb[:, 1:2] ** 2)).ravel()
+        orc.set_zone_state(1, uB)
+        orc.set_state(Q)
+        ref = orc.time_derivative(0.0)
+        g.set_boundary_state(1, uB)
+        g.set_state(Q)
+        out = g.compute_time_derivative(0.0)
+        assert rel_l2(out, ref) <= TOL_STAGE
+        assert rel_l2(before, ref) > 1e-8        # the per-node states change the residual
+    dt = orc.estimate_dt(0.2, 1.0)
+    for s in range(10):
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, 10, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_STAGE * 10
+    with pytest.raises(hg.HorsesGpuError):
+        g.set_boundary_state(1, uB[:-4])          # wrong size
+    with pytest.raises(hg.HorsesGpuError):
+        g.set_boundary_state(2, np.zeros(orc.zone_edge_nodes(2).size * 2))   # far field: not fed per node
