@@ -28,6 +28,11 @@ Workloads (synthetic inputs with the configurations' shapes; seeds fixed):
              dissipation; the sensor network is first trained on the GPU on 2 x 100 solver snapshots
              (shock position +-0.5, amplitude 0.1-0.3, seed 20261203); value = FP32 bulk + learned
              sensor, beside the plain FP64 path with the modal-decay sensor.
+  kh       : doubly periodic Kelvin-Helmholtz shear layer on [0,1]^2, 1024 x 1024 elements, N = 7
+             (NDOF 268,435,456), Re 1e4, M 0.3, tanh layers of thickness 0.01 with a seeded 4-mode
+             perturbation of amplitude 1e-2, SIPG (sigma0 10), Roe, Laplacian artificial viscosity
+             driven by the learned sensor (trained as for `shock`; out-of-distribution elements use
+             the modal indicator); FP32 bulk + learned beside FP64 + modal.  --kh-n sets the size.
 Multi-GPU: independent replicas (the workload does not exchange data), weak scaling.
 """
 import argparse
@@ -46,7 +51,8 @@ sys.path.insert(0, ROOT)
 
 SEED = 20261203
 L2_BYTES = 126 * 2 ** 20
-CONFIGS = ("cylinder", "vortex16", "ensemble", "box512", "shock")
+KH_DT_COEF = 0.05   # kh workload: dt = 0.05 / n^2 (half the measured interior-penalty stability limit)
+CONFIGS = ("cylinder", "vortex16", "ensemble", "box512", "shock", "kh")
 
 
 def peaks():
@@ -229,6 +235,17 @@ class CpuArm:
                                        np.where(up, 1.0, p2)).ravel())
             self.orcs = [(o, o.estimate_dt(0.1, 1.0))]
             return
+        if config == "kh":
+            # bounded sample: 128 x 128 elements of the 1024 x 1024 workload, same order and physics
+            O.lib().or_set_threads(self.threads)
+            o = O.Oracle(hmesh.cartesian(128, 128, 0.0, 1.0, 0.0, 1.0), 7, nodes=O.LG, riemann=O.ROE, mach=0.3,
+                         reynolds=1.0e4, navier_stokes=1, viscous=O.IP, ip_method=0, sigma0_ip=10.0,
+                         bcs=hmesh.periodic_bcs_cartesian(), av_type=O.AV_LAPLACIAN, av_intensity=1.0,
+                         av_indicator=O.IND_MODAL)
+            X = o.coords()
+            o.set_state(cases.kelvin_helmholtz(X[:, 0], X[:, 1], seed=SEED).ravel())
+            self.orcs = [(o, min(o.estimate_dt(0.2, 1.0), KH_DT_COEF / 128 ** 2))]
+            return
         if config == "cylinder":
             O.lib().or_set_threads(self.threads)
             o = O.Oracle(cylinder_mesh(), 5, nodes=O.LG, riemann=O.ROE, mach=0.2, reynolds=100.0, prandtl=0.72,
@@ -265,11 +282,13 @@ class CpuArm:
     def sample(self, budget_s):
         """(DOF-stage/s, cores, description) of ~budget_s seconds of RK3 steps."""
         from concurrent.futures import ThreadPoolExecutor
-        if self.config in ("cylinder", "shock"):
+        if self.config in ("cylinder", "shock", "kh"):
             n, el, steps = self._run(self.orcs[0], budget_s, False)
-            return (n / el, self.threads, f"full {self.config} workload (NDOF {self.orcs[0][0].ndof}), {steps} RK3 "
+            what = ("128 x 128 elements of the 1024 x 1024 kh workload" if self.config == "kh"
+                    else f"full {self.config} workload")
+            return (n / el, self.threads, f"{what} (NDOF {self.orcs[0][0].ndof}), {steps} RK3 "
                     f"steps in {el:.1f} s, OpenMP element loops on {self.threads} threads, FP64"
-                    + (", modal-decay sensor" if self.config == "shock" else ""))
+                    + (", modal-decay sensor" if self.config in ("shock", "kh") else ""))
         with ThreadPoolExecutor(max_workers=self.threads) as ex:
             res = list(ex.map(lambda a: self._run(a, budget_s, True), self.orcs))
         rate = sum(r[0] / r[1] for r in res)
@@ -500,6 +519,111 @@ def run_shock(args, rank, world, local, dist):
         dist.destroy_process_group()
 
 
+def run_kh(args, rank, world, local, dist):
+    """Kelvin-Helmholtz shear layer (NS, SIPG, Roe, Laplacian artificial viscosity driven by the learned
+    sensor): FP32 + learned timed beside FP64 + modal on the same workload; density error of FP32 +
+    learned against FP64 + learned after K steps from the same state."""
+    import torch
+    import horses2d_b200 as hg
+    from horses2d_b200 import sensor as S, mesh as hmesh, cases
+    n, N = args.kh_n, 7
+    t0 = time.perf_counter()
+    params, lo, hi, info = S.train_two_rounds(100, SEED, nx=512, ny=64, N=3, steps=100, epochs=30, batch=4096)
+    train_s = time.perf_counter() - t0
+    desc = hmesh.box_descriptor(n, n, 0.0, 1.0, 0.0, 1.0, N, hg.NODES_LG)
+    x = desc["x"].reshape(-1, 2)
+    Q0 = cases.kelvin_helmholtz(x[:, 0], x[:, 1], seed=SEED).ravel()
+    del x
+    kw = dict(mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0,
+              node_type=hg.NODES_LG, riemann=hg.ROE, av_type=hg.AV_LAPLACIAN, av_intensity=1.0,
+              bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    stream = torch.cuda.Stream()
+    parts = [(desc, Q0, N, 1, kw, 0.2)]
+    c32 = make_contexts(parts, hg.PREC_FP32, stream)
+    c32[0]["g"].set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
+    c64 = make_contexts(parts, hg.PREC_FP64, stream)
+    c64[0]["g"].set_sensor(hg.SENSOR_MODAL)
+    del desc
+    g32, g64 = c32[0]["g"], c64[0]["g"]
+    ndof = g32.ndof
+    # the interior-penalty terms at Re 1e4, N = 7 limit the step like h^2 (the reference's estimate is
+    # inviscid only): measured on the oracle, dt_max ~ 0.1 / n^2 at 32^2 and 64^2; half of it is used
+    dt = min(g64.estimate_time_step(0.2, 1.0), KH_DT_COEF / n ** 2)
+    flush = L2Flush(ndof * 8 * 3 < 2 * L2_BYTES)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms32, launches = device_timed(c32, args.steps, args.warmup, dt, stream, world, dist, flush, min_load_s=2.0)
+    clk = clocks.stop()
+    ms64, _ = device_timed(c64, args.steps, args.warmup, dt, stream, world, dist, flush)
+    split = kernel_split(c32, max(3, min(args.steps, 10)), dt, stream, flush)
+    # accuracy: FP32 + learned against FP64 + learned, K steps from the same state
+    g64.set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
+    for g in (g32, g64):
+        g.set_state(Q0)
+        g.time_steps(hg.SCHEME_RK3, args.steps, 0.0, dt)
+    r32 = g32.state()[0::4]
+    r64 = g64.state()[0::4]
+    rho_err = float(np.linalg.norm(r32 - r64) / np.linalg.norm(r64))
+    del r32, r64
+    _, out32 = g32.sensor_eval()
+    # end to end through the public API with host buffers (FP32 + learned)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    g32.set_state(c32[0]["Qh"].numpy())
+    res = np.zeros(4)
+    for s in range(args.steps):
+        g32.time_step(hg.SCHEME_RK3, s * dt, dt)
+        res = np.maximum(res, g32.residuals())
+    Qe = g32.state()
+    e2e_ms = (time.perf_counter() - t1) * 1e3
+    if not (np.all(np.isfinite(Qe)) and np.all(np.isfinite(res))):
+        raise SystemExit("non-finite state after the timed steps")
+    del Qe
+    value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
+    value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
+    bpd = stage_bytes_per_dof("kh", True, True, True)
+    st_ms, st_n = split["stage"]
+    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
+    achieved = bpd * ndof / avg_stage_s / 1e9
+    peak, peak_kind = peaks()
+    total_split = sum(v[0] for v in split.values()) or 1.0
+    line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
+            "config": {"workload": "kh", "ndof": ndof, "mesh": f"{n}x{n}", "N": N, "precision": "fp32",
+                       "physics": "NS Re 1e4 M 0.3, SIPG (sigma0 10), Roe, Laplacian artificial viscosity",
+                       "dt": dt,
+                       "sensor": "learned (MLP 16-32-32-1, trained on the shock workload's snapshots at N=3) "
+                                 "with modal fallback",
+                       "scheme": "Williamson RK3",
+                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
+                              if flush.buf is not None else "inputs larger than L2"),
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": ndof * 3 * args.steps / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
+                    "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
+            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
+            "fp64_plain_modal": {"value": value64, "ms_per_step": ms64 / args.steps,
+                                 "speedup_fp32_learned": ms64 / ms32},
+            "accuracy": {f"rel_l2_density_fp32_vs_fp64_after_{args.steps}_steps": rho_err},
+            "sensor": {"training_s": train_s, "ood_fraction": float(out32[:, 2].mean()),
+                       "troubled_fraction": float((out32[:, 3] > 0.5).mean()),
+                       "disagreement_vs_modal": S.disagreement(out32[:, 0], out32[:, 3])},
+            "clocks": clk}
+    if rank == 0 and not args.no_cpu_baseline:
+        rate, cores, sample = CpuArm("kh").sample(12.0)
+        line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    for c in c32 + c64:
+        c["g"].close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -509,6 +633,7 @@ def main():
     ap.add_argument("--config", default="cylinder", choices=CONFIGS)
     ap.add_argument("--precision", default=None, choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kh-n", type=int, default=1024, help="elements per side of the kh workload")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -524,6 +649,8 @@ def main():
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     if args.config == "shock":
         return run_shock(args, rank, world, local, dist)
+    if args.config == "kh":
+        return run_kh(args, rank, world, local, dist)
     precision = args.precision or ("fp32" if args.config == "ensemble" else "fp64")
     prec = hg.PREC_FP32 if precision == "fp32" else hg.PREC_FP64
     parts = build_parts(args.config)

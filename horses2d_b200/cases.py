@@ -33,3 +33,26 @@ def uniform_state(n, *, mach, angle_deg=0.0, gamma=1.4):
     v = np.sqrt(gamma) * mach * np.sin(th)
     q = np.array([1.0, u, v, 1.0 / (gamma - 1.0) + 0.5 * (u * u + v * v)])
     return np.tile(q, (n, 1))
+
+
+def kelvin_helmholtz(x, y, *, mach=0.3, delta=0.01, eps=1e-2, n_modes=4, seed=0, drho=0.0, gamma=1.4):
+    """Doubly periodic shear layer on [0,1]^2 (p = 1): u = U tanh((y - 1/4)/delta) below y = 1/2 and
+    U tanh((3/4 - y)/delta) above, U = sqrt(gamma) M, so that both layers are periodic; the transverse
+    velocity carries a seeded multi-mode perturbation eps U sum_m a_m sin(2 pi m x + phi_m), damped away
+    from the layers by exp(-(d/(4 delta))^2).  Density 1, or with drho > 0 a stream of density 1 + drho
+    between the layers (same tanh profile).  Returns Q [n, 4] in the reference's dimensionless variables.
+    """
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.5, 1.0, n_modes)
+    amp /= amp.sum()
+    phase = rng.uniform(0.0, 2.0 * np.pi, n_modes)
+    U = np.sqrt(gamma) * mach
+    u = np.where(y < 0.5, U * np.tanh((y - 0.25) / delta), U * np.tanh((0.75 - y) / delta))
+    d = np.minimum(np.abs(y - 0.25), np.abs(y - 0.75))
+    pert = np.zeros_like(x)
+    for m in range(n_modes):
+        pert += amp[m] * np.sin(2.0 * np.pi * (m + 1) * x + phase[m])
+    v = eps * U * pert * np.exp(-(d / (4.0 * delta)) ** 2)
+    rho = 1.0 + 0.5 * drho * (1.0 - np.where(y < 0.5, np.tanh((y - 0.25) / delta), np.tanh((0.75 - y) / delta)))
+    p = np.ones_like(x)
+    return np.stack([rho, rho * u, rho * v, p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v)], 1)

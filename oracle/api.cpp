@@ -94,6 +94,7 @@ extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
     const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
     const double cm[3] = {0.0, 1.0 / 3.0, 3.0 / 4.0};
     for (int m = 0; m < 3; ++m) {
+      o.av_hold = m > 0;
       time_derivative(o, t + dt * cm[m]);
       if (m == 0) for (int64_t i = 0; i < n; ++i) G[i] = QD[i];
       else for (int64_t i = 0; i < n; ++i) G[i] = am[m] * G[i] + QD[i];
@@ -104,6 +105,7 @@ extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
     const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
     const double cm[5] = {0.0, 0.1496590219993, 0.3704009573644, 0.6222557631345, 0.9582821306748};
     for (int m = 0; m < 5; ++m) {
+      o.av_hold = m > 0;
       time_derivative(o, t + dt * cm[m]);
       if (m == 0) {
         for (int64_t i = 0; i < n; ++i) G[i] = dt * QD[i];
@@ -116,6 +118,7 @@ extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
       }
     }
   }
+  o.av_hold = false;
 }
 
 extern "C" double or_estimate_dt(void* h, double cfl, double dt_cap) {

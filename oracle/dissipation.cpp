@@ -14,7 +14,9 @@
  * methods", AIAA 2006-112): s = max over rho and p of log10(E_N/E), E the energy of the element's
  * modal coefficients in the orthonormal Legendre basis of [0,1] and E_N that of the modes whose higher
  * index is N, G = the reference's sine ramp around s0 of half width kappa; and an external G per
- * element (the library's learned sensor, checked through it).
+ * element (the library's learned sensor, checked through it).  These two are evaluated on the first
+ * stage of each time step and held for its other stages (the library's rule for its sensors); the
+ * reference's jumps indicator is evaluated at every residual, as in the reference.
  */
 #include "oracle_internal.h"
 #include "viscous.h"
@@ -182,6 +184,7 @@ double modal_indicator(const Oracle& o, const Element& e) {
 }
 
 void compute_av_viscosity(Oracle& o) {
+  if (o.av_hold && o.cas.av_indicator != OR_IND_JUMPS && o.av_mu.size() == o.el.size()) return;
   o.av_mu.assign(o.el.size(), 0.0);
   if (!o.cas.navier_stokes || o.cas.av_type == OR_AV_NONE) return;
 #pragma omp parallel for schedule(static)

@@ -133,6 +133,7 @@ struct Oracle {
   std::vector<double> Q, QDot, dQ, G;
   std::vector<double> av_mu;                          // element artificial viscosity of the current state
   std::vector<double> av_g_ext;                       // externally supplied indicator G (OR_IND_EXTERNAL)
+  bool av_hold = false;                               // later RK stages: keep the modal / external viscosity
   int64_t ndof = 0;
   // EstimateTimeStep SAVE variables (DGTimeIntegrator.f90:471-473)
   double save_umax = 0.0, save_amax = 0.0;

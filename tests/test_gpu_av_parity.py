@@ -89,3 +89,40 @@ def test_newdirichlet_total_pressure_mode():
     g = hg.GpuDGSEM(orc2.export_mesh(), **gkw)
     g.set_state(Qs)
     assert rel_l2(g.compute_time_derivative(0.0), ref) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", [hg.PREC_FP64, hg.PREC_FP32])
+def test_shear_layer_n7_sipg_modal_dissipation(precision):
+    """The Kelvin-Helmholtz workload's physics at a small size: periodic 8 x 8, N = 7, Re 1e4, M 0.3,
+    SIPG (sigma0 10), Roe, Laplacian artificial viscosity driven by the modal indicator (a density
+    contrast across thin layers, so that some elements are flagged); residual and 10 RK3 steps against
+    the oracle, with the workload's step rule dt = min(CFL 0.2 estimate, 0.05 / n^2)."""
+    from horses2d_b200 import mesh as hmesh, cases
+    m = hmesh.cartesian(8, 8, 0.0, 1.0, 0.0, 1.0)
+    orc = O.Oracle(m, 7, nodes=O.LG, riemann=O.ROE, mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=O.IP,
+                   ip_method=0, sigma0_ip=10.0, bcs=hmesh.periodic_bcs_cartesian(), av_type=O.AV_LAPLACIAN,
+                   av_intensity=1.0, av_indicator=O.IND_MODAL)
+    X = orc.coords()
+    Q = cases.kelvin_helmholtz(X[:, 0], X[:, 1], delta=0.005, eps=0.05, seed=5, drho=2.0).ravel()
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    assert np.max(orc.av_viscosity()) > 0.0
+    g = hg.GpuDGSEM(orc.export_mesh(), precision=precision, mach=0.3, reynolds=1.0e4, navier_stokes=1,
+                    viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.ROE,
+                    av_type=hg.AV_LAPLACIAN, av_intensity=1.0, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    g.set_sensor(hg.SENSOR_MODAL)
+    g.set_state(Q)
+    fp64 = precision == hg.PREC_FP64
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= (1e-12 if fp64 else 1e-4)
+    np.testing.assert_allclose(g.element_viscosity(), orc.av_viscosity(), rtol=1e-12 if fp64 else 1e-4, atol=1e-300)
+    dt = min(orc.estimate_dt(0.2, 1.0), 0.05 / 8 ** 2)
+    for s in range(10):
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, 10, 0.0, dt)
+    if fp64:
+        assert rel_l2(g.state(), orc.state()) <= 1e-10
+    else:
+        # this 8 x 8 case is under-resolved on purpose (the layers must trip the indicator) and its
+        # residual grows ~20x over the 10 steps, which amplifies FP32 rounding: 5e-5 here; the
+        # workload-size FP32 density error is reported by bench.py
+        assert rel_l2(g.state()[0::4], orc.state()[0::4]) <= 5e-5
