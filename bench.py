@@ -331,8 +331,16 @@ def make_contexts(parts, prec, stream):
         g.set_stream(stream.cuda_stream)
         Qh = torch.from_numpy(Q0).pin_memory()
         g.set_state(Qh.numpy())
-        ctxs.append(dict(g=g, Qh=Qh, N=N, ninst=ninst, cfl=cfl))
+        tune = g.autotune(trials=10)     # elements-per-CTA variant, timed on this workload's state
+        ctxs.append(dict(g=g, Qh=Qh, N=N, ninst=ninst, cfl=cfl, tune=tune))
     return ctxs
+
+
+def tiling_summary(ctxs):
+    """Autotuner outcome per context: elements per CTA chosen and ms per residual of each variant."""
+    return [{"N": c["N"], "elements_per_cta": c["tune"]["tiling"]["elements_per_cta"],
+             "threads_per_cta": c["tune"]["tiling"]["threads_per_cta"],
+             "ms_per_variant": [round(x, 5) for x in c["tune"]["ms"]]} for c in ctxs]
 
 
 class L2Flush:
@@ -441,6 +449,7 @@ def run_shock(args, rank, world, local, dist):
             c[0]["g"].set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
         else:
             c[0]["g"].set_sensor(hg.SENSOR_MODAL)
+        c[0]["tune"] = c[0]["g"].autotune(trials=10)    # again, with the sensor that will run
         return c
 
     c32, c64 = ctx(hg.PREC_FP32, True), ctx(hg.PREC_FP64, False)
@@ -490,6 +499,7 @@ def run_shock(args, rank, world, local, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
             "config": {"workload": "shock", "ndof": ndof, "mesh": f"{nx}x{ny}", "N": N, "precision": "fp32",
+                       "tiling": tiling_summary(c32),
                        "sensor": "learned (MLP 16-32-32-1) with modal fallback", "scheme": "Williamson RK3",
                        "l2": ("256 MB buffer written between timed steps (outside the step events)"
                               if flush.buf is not None else "inputs larger than L2"),
@@ -541,8 +551,10 @@ def run_kh(args, rank, world, local, dist):
     parts = [(desc, Q0, N, 1, kw, 0.2)]
     c32 = make_contexts(parts, hg.PREC_FP32, stream)
     c32[0]["g"].set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
+    c32[0]["tune"] = c32[0]["g"].autotune(trials=10)    # again, with the sensor that will run
     c64 = make_contexts(parts, hg.PREC_FP64, stream)
     c64[0]["g"].set_sensor(hg.SENSOR_MODAL)
+    c64[0]["tune"] = c64[0]["g"].autotune(trials=10)
     del desc
     g32, g64 = c32[0]["g"], c64[0]["g"]
     ndof = g32.ndof
@@ -591,6 +603,7 @@ def run_kh(args, rank, world, local, dist):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
             "config": {"workload": "kh", "ndof": ndof, "mesh": f"{n}x{n}", "N": N, "precision": "fp32",
+                       "tiling": tiling_summary(c32),
                        "physics": "NS Re 1e4 M 0.3, SIPG (sigma0 10), Roe, Laplacian artificial viscosity",
                        "dt": dt,
                        "sensor": "learned (MLP 16-32-32-1, trained on the shock workload's snapshots at N=3) "
@@ -720,6 +733,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": args.config, "ndof": ndof, "precision": precision,
                        "orders": [c["N"] for c in ctxs], "instances": sum(c["ninst"] for c in ctxs),
+                       "tiling": tiling_summary(ctxs),
                        "scheme": "Williamson RK3",
                        "l2": ("256 MB buffer written between timed steps (outside the step events)"
                               if flush.buf is not None else "inputs larger than L2"),

@@ -50,11 +50,13 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
             "hg_time_derivative", "hg_time_step", "hg_time_steps", "hg_residuals", "hg_estimate_dt",
             "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info",
             "hg_profile", "hg_kernel_times", "hg_residuals_noalloc", "hg_set_sensor", "hg_sensor_eval",
-            "hg_element_viscosity", "hg_mlp_forward", "hg_mlp_grad", "hg_mlp_train", "hg_set_boundary_state")
+            "hg_element_viscosity", "hg_mlp_forward", "hg_mlp_grad", "hg_mlp_train", "hg_set_boundary_state",
+            "hg_autotune", "hg_set_tiling", "hg_get_tiling")
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
 KERNEL_KINDS = ("stage", "gradient", "trace", "reduce", "speed", "face_flux")
+TILINGS = 2
 
 
 def load():
@@ -97,6 +99,9 @@ def load():
     L.hg_sensor_eval.argtypes = [vp, f32p, F64P]
     L.hg_element_viscosity.argtypes = [vp, F64P]
     L.hg_set_boundary_state.argtypes = [vp, C.c_int32, F64P, C.c_int64]
+    L.hg_autotune.argtypes = [vp, C.c_int32, I32P, F64P]
+    L.hg_set_tiling.argtypes = [vp, C.c_int32]
+    L.hg_get_tiling.argtypes = [vp, I32P]
     L.hg_mlp_forward.argtypes = [f32p, f32p, C.c_int64, f32p]
     L.hg_mlp_grad.argtypes = [f32p, f32p, f32p, f32p, C.c_int64, F64P, f32p]
     L.hg_mlp_train.argtypes = [f32p, f32p, f32p, f32p, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64, F64P]

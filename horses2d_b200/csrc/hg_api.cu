@@ -45,8 +45,16 @@ static void free_ctx(hg_ctx* c) {
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
 
+static int epb_of(const hg_ctx* c, int variant) {
+  return c->ns ? epb_ns_of(c->P, variant) : epb_stage(c->P, variant);
+}
 static int grid_for(const hg_ctx* c) {
-  const int epb = c->ns ? epb_ns(c->P) : epb_for(c->P);
+  const int epb = epb_of(c, c->tiling);
+  return (c->n_el + epb - 1) / epb;
+}
+// per-CTA residual partials: room for the tiling variant with the most CTAs
+static int max_grid(const hg_ctx* c) {
+  const int epb = std::min(epb_of(c, 0), epb_of(c, 1));
   return (c->n_el + epb - 1) / epb;
 }
 
@@ -65,6 +73,17 @@ static int grid_for(const hg_ctx* c) {
 
 template <typename real>
 static void run_trace(hg_ctx* c) { HG_DISPATCH_P(c->P, launch_trace_P, c); }
+
+template <int P, typename real>
+static void ns_dispatch(hg_ctx* c, const NSArgs<real>& a) {
+  if (c->tiling) launch_ns_PV<P, real, 1>(c, a);
+  else launch_ns_PV<P, real, 0>(c, a);
+}
+template <int P, typename real>
+static void stage_dispatch(hg_ctx* c, const StageArgs<real>& a) {
+  if (c->tiling) launch_stage_PV<P, real, 1>(c, a);
+  else launch_stage_PV<P, real, 0>(c, a);
+}
 
 template <typename real>
 static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
@@ -107,7 +126,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.mu_av = c->d_mu_av;
   a.sensor = sensor_args(c);
   if (c->exact) launch_exact_flux<real>(c);
-  HG_DISPATCH_P(c->P, launch_ns_P, c, a);
+  HG_DISPATCH_P(c->P, ns_dispatch, c, a);
   if (update) c->cur ^= 1;
 }
 
@@ -135,7 +154,7 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.riemann = c->riemann;
   a.pc = c->pc;
   if (c->exact) launch_exact_flux<real>(c);
-  HG_DISPATCH_P(c->P, launch_stage_P, c, a);
+  HG_DISPATCH_P(c->P, stage_dispatch, c, a);
   if (update) c->cur ^= 1;
 }
 
@@ -392,7 +411,7 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   c->d_T[0] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_T[1] = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
   c->d_QDot = dalloc<double>(c->ndof);
-  c->d_resid = dalloc<double>(size_t(grid_for(c)) * 4);
+  c->d_resid = dalloc<double>(size_t(max_grid(c)) * 4);
   c->d_resid_out = dalloc<double>(4);
   c->d_elmax = dalloc<double>(size_t(E) * 2);
   if (c->av != HG_AV_NONE) {
@@ -435,7 +454,7 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_zones, zones.data(), zones.size() * sizeof(Zone), cudaMemcpyHostToDevice));
-  HG_CUDA(cudaMemset(c->d_resid, 0, size_t(grid_for(c)) * 4 * sizeof(double)));
+  HG_CUDA(cudaMemset(c->d_resid, 0, size_t(max_grid(c)) * 4 * sizeof(double)));
 }
 
 extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, const hg_bc_desc* bcs, int32_t n_bcs,
@@ -755,6 +774,71 @@ extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, 
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+// ------------------------------------------------------------------ elements-per-CTA autotuner
+extern "C" int hg_set_tiling(hg_ctx* c, int32_t variant) {
+  try {
+    if (variant < 0 || variant >= HG_TILINGS) throw std::runtime_error("unknown tiling variant");
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    if (variant != c->tiling) drop_graph(c);
+    c->tiling = variant;
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_get_tiling(const hg_ctx* c, int32_t out[3]) {
+  if (!c || !out) return 1;
+  const int epb = epb_of(c, c->tiling);
+  out[0] = c->tiling;
+  out[1] = epb;
+  out[2] = block_of(c->P, epb);
+  return 0;
+}
+
+extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* ms_per_variant) {
+  if (!c) return 1;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  const bool prof = c->prof;
+  try {
+    require_state(c);
+    if (trials < 1) throw std::runtime_error("autotune needs at least one trial");
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    drop_graph(c);
+    c->prof = false;
+    HG_CUDA(cudaEventCreate(&ev[0]));
+    HG_CUDA(cudaEventCreate(&ev[1]));
+    double best = 0.0;
+    int best_v = 0;
+    for (int v = 0; v < HG_TILINGS; ++v) {
+      c->tiling = v;
+      // residual launches of the resident state (no update): the stage's full arithmetic and loads
+      for (int w = 0; w < 2; ++w) stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, false);
+      HG_CUDA(cudaEventRecord(ev[0], c->stream));
+      for (int k = 0; k < trials; ++k) stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, false);
+      HG_CUDA(cudaEventRecord(ev[1], c->stream));
+      HG_CUDA(cudaEventSynchronize(ev[1]));
+      float ms = 0.f;
+      HG_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      const double per = double(ms) / trials;
+      if (ms_per_variant) ms_per_variant[v] = per;
+      if (v == 0 || per < best) { best = per; best_v = v; }
+    }
+    c->tiling = best_v;
+    // leave the residual partials of the resident state in the chosen layout (as hg_time_derivative)
+    stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, true);
+    HG_CUDA(cudaGetLastError());
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    c->prof = prof;
+    if (chosen) *chosen = best_v;
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return 0;
+  } catch (const std::exception& ex) {
+    for (cudaEvent_t e : ev) if (e) cudaEventDestroy(e);
+    c->prof = prof;
+    return fail(c, ex);
+  }
 }
 
 extern "C" int hg_info(const hg_ctx* c, int32_t out[4]) {

@@ -51,6 +51,7 @@ struct hg_ctx {
   void* d_jac = nullptr;          // [n_el][NP] J (curved meshes), context precision
   void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
   void* d_dQ = nullptr;           // element gradients [n_el][2][4][NP] (Navier-Stokes)
+  int tiling = 0;                 // elements-per-CTA variant of the stage kernels (hg_autotune / hg_set_tiling)
   bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
   void* d_FX = nullptr;           // its face fluxes of the current stage [n_el*4][P][4], context precision
   // zones fed per node (hg_set_boundary_state): state rows [rows][P][4] indexed by side.w
@@ -127,10 +128,11 @@ inline void max_carveout(K kernel) {
                                int(cudaSharedmemCarveoutMaxShared)));
 }
 
-// Per-order launches, explicitly instantiated in hg_inst_*.cu.
-template <int P, typename real> void launch_stage_P(hg_ctx* c, const StageArgs<real>& a);
+// Per-order launches, explicitly instantiated in hg_inst_*.cu (V = tiling variant: 0 in the plain
+// units, 1 in the *_t1 units).
+template <int P, typename real, int V> void launch_stage_PV(hg_ctx* c, const StageArgs<real>& a);
 template <int P, typename real> void launch_trace_P(hg_ctx* c);
-template <int P, typename real> void launch_ns_P(hg_ctx* c, const NSArgs<real>& a);
+template <int P, typename real, int V> void launch_ns_PV(hg_ctx* c, const NSArgs<real>& a);
 template <int P, typename real> void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out);
 template <typename real> void launch_exact_flux(hg_ctx* c);
 

@@ -1,5 +1,5 @@
 // hg_inst_ns32c.cu -- explicit instantiations: Navier-Stokes kernels, P = 6, 7, float.
 #include "hg_launch.cuh"
 
-template void launch_ns_P<6, float>(hg_ctx*, const NSArgs<float>&);
-template void launch_ns_P<7, float>(hg_ctx*, const NSArgs<float>&);
+template void launch_ns_PV<6, float, 0>(hg_ctx*, const NSArgs<float>&);
+template void launch_ns_PV<7, float, 0>(hg_ctx*, const NSArgs<float>&);

@@ -1,5 +1,5 @@
 // hg_inst_ns32d.cu -- explicit instantiations: Navier-Stokes kernels, P = 8, 9, float.
 #include "hg_launch.cuh"
 
-template void launch_ns_P<8, float>(hg_ctx*, const NSArgs<float>&);
-template void launch_ns_P<9, float>(hg_ctx*, const NSArgs<float>&);
+template void launch_ns_PV<8, float, 0>(hg_ctx*, const NSArgs<float>&);
+template void launch_ns_PV<9, float, 0>(hg_ctx*, const NSArgs<float>&);

@@ -1,5 +1,5 @@
 // hg_inst_ns64a.cu -- explicit instantiations: Navier-Stokes kernels, P = 2, 3, double.
 #include "hg_launch.cuh"
 
-template void launch_ns_P<2, double>(hg_ctx*, const NSArgs<double>&);
-template void launch_ns_P<3, double>(hg_ctx*, const NSArgs<double>&);
+template void launch_ns_PV<2, double, 0>(hg_ctx*, const NSArgs<double>&);
+template void launch_ns_PV<3, double, 0>(hg_ctx*, const NSArgs<double>&);

@@ -3,9 +3,10 @@
 #pragma once
 #include "hg_ctx.h"
 
-template <int P, typename real>
-void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
-  constexpr int EPB = epb_for(P);
+template <int P, typename real, int V>
+void launch_stage_PV(hg_ctx* c, const StageArgs<real>& a) {
+  constexpr int EPB = epb_stage(P, V);
+  constexpr int BLK = block_of(P, EPB);
   const int grid = (a.n_el + EPB - 1) / EPB;
   static bool attr = false;
   if (!attr) {
@@ -18,11 +19,11 @@ void launch_stage_P(hg_ctx* c, const StageArgs<real>& a) {
   const bool lgl = c->node_type == HG_NODES_LGL;
   timed(c, HG_KERNEL_STAGE, [&] {
     if (c->affine) {
-      if (lgl) stage_kernel<P, EPB, real, true, true><<<grid, block_for(P), 0, c->stream>>>(a);
-      else stage_kernel<P, EPB, real, true, false><<<grid, block_for(P), 0, c->stream>>>(a);
+      if (lgl) stage_kernel<P, EPB, real, true, true><<<grid, BLK, 0, c->stream>>>(a);
+      else stage_kernel<P, EPB, real, true, false><<<grid, BLK, 0, c->stream>>>(a);
     } else {
-      if (lgl) stage_kernel<P, EPB, real, false, true><<<grid, block_for(P), 0, c->stream>>>(a);
-      else stage_kernel<P, EPB, real, false, false><<<grid, block_for(P), 0, c->stream>>>(a);
+      if (lgl) stage_kernel<P, EPB, real, false, true><<<grid, BLK, 0, c->stream>>>(a);
+      else stage_kernel<P, EPB, real, false, false><<<grid, BLK, 0, c->stream>>>(a);
     }
   });
   ++c->launches;
@@ -39,9 +40,10 @@ void launch_trace_P(hg_ctx* c) {
   ++c->launches;
 }
 
-template <int P, typename real, bool AFFINE, bool IP, bool AV>
+template <int P, typename real, int V, bool AFFINE, bool IP, bool AV>
 static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
-  constexpr int EPB = epb_ns(P);
+  constexpr int EPB = epb_ns_of(P, V);
+  constexpr int BLK = block_of(P, EPB);
   const int grid = (a.n_el + EPB - 1) / EPB;
   static bool attr = false;
   if (!attr) {
@@ -51,28 +53,28 @@ static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
   }
   if (a.run_gradient) {
     timed(c, HG_KERNEL_GRADIENT,
-          [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, block_ns(P), 0, c->stream>>>(a); });
+          [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, BLK, 0, c->stream>>>(a); });
     ++c->launches;
   }
   timed(c, HG_KERNEL_STAGE,
-        [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, block_ns(P), 0, c->stream>>>(a); });
+        [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, BLK, 0, c->stream>>>(a); });
   ++c->launches;
 }
 
-template <int P, typename real>
-void launch_ns_P(hg_ctx* c, const NSArgs<real>& a) {
+template <int P, typename real, int V>
+void launch_ns_PV(hg_ctx* c, const NSArgs<real>& a) {
   // artificial dissipation is a template switch so that the plain kernels keep their register budget
   if (c->av) {
     if (c->affine) {
-      if (c->ip) launch_ns_PAI<P, real, true, true, true>(c, a); else launch_ns_PAI<P, real, true, false, true>(c, a);
+      if (c->ip) launch_ns_PAI<P, real, V, true, true, true>(c, a); else launch_ns_PAI<P, real, V, true, false, true>(c, a);
     } else {
-      if (c->ip) launch_ns_PAI<P, real, false, true, true>(c, a); else launch_ns_PAI<P, real, false, false, true>(c, a);
+      if (c->ip) launch_ns_PAI<P, real, V, false, true, true>(c, a); else launch_ns_PAI<P, real, V, false, false, true>(c, a);
     }
   } else {
     if (c->affine) {
-      if (c->ip) launch_ns_PAI<P, real, true, true, false>(c, a); else launch_ns_PAI<P, real, true, false, false>(c, a);
+      if (c->ip) launch_ns_PAI<P, real, V, true, true, false>(c, a); else launch_ns_PAI<P, real, V, true, false, false>(c, a);
     } else {
-      if (c->ip) launch_ns_PAI<P, real, false, true, false>(c, a); else launch_ns_PAI<P, real, false, false, false>(c, a);
+      if (c->ip) launch_ns_PAI<P, real, V, false, true, false>(c, a); else launch_ns_PAI<P, real, V, false, false, false>(c, a);
     }
   }
 }

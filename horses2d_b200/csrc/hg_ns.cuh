@@ -63,6 +63,10 @@ struct NSArgs {
 __host__ __device__ constexpr int epb_ns(int P) {
   return P == 2 ? 16 : P == 3 ? 7 : P == 4 ? 8 : P == 5 ? 5 : P == 6 ? 4 : P == 7 ? 3 : 2;
 }
+__host__ __device__ constexpr int epb_ns_small(int P) {
+  return P == 2 ? 4 : P == 3 ? 2 : P == 4 ? 2 : 1;
+}
+__host__ __device__ constexpr int epb_ns_of(int P, int variant) { return variant ? epb_ns_small(P) : epb_ns(P); }
 __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) + 31) / 32) * 32; }
 
 // Shared tiles of one CTA.
@@ -325,7 +329,7 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
 }
 
 template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
-__global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a) {
+__global__ void __launch_bounds__(block_of(P, EPB)) ns_gradient_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
   __shared__ NSTiles<P, EPB, real, AFFINE> s;
   const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
@@ -363,9 +367,9 @@ __global__ void __launch_bounds__(block_ns(P)) ns_gradient_kernel(NSArgs<real> a
 }
 
 template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
-__global__ void __launch_bounds__(block_ns(P)) ns_stage_kernel(NSArgs<real> a) {
+__global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
-  constexpr int NW = block_ns(P) / 32;
+  constexpr int NW = block_of(P, EPB) / 32;
   __shared__ NSTiles<P, EPB, real, AFFINE> s;
   const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
   const int e = blockIdx.x * EPB + le;

@@ -57,10 +57,17 @@ struct StageArgs {
   PhysConst pc;
 };
 
+// Elements per CTA: tiling variant 0 (default, large CTAs) and variant 1 (small CTAs: more CTAs in
+// flight on small meshes); hg_autotune times both on the resident state and keeps the faster.
 __host__ __device__ constexpr int epb_for(int P) {
   return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : 3;
 }
-__host__ __device__ constexpr int block_for(int P) { return ((P * P * epb_for(P) + 31) / 32) * 32; }
+__host__ __device__ constexpr int epb_small_for(int P) {
+  return P == 2 ? 8 : P == 3 ? 4 : P == 4 ? 4 : P == 5 ? 2 : P == 6 ? 2 : P == 7 ? 2 : 1;
+}
+__host__ __device__ constexpr int epb_stage(int P, int variant) { return variant ? epb_small_for(P) : epb_for(P); }
+__host__ __device__ constexpr int block_of(int P, int EPB) { return ((P * P * EPB + 31) / 32) * 32; }
+__host__ __device__ constexpr int block_for(int P) { return block_of(P, epb_for(P)); }
 
 // max that keeps NaN (a residual that is NaN must stay visible)
 __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
@@ -75,10 +82,10 @@ __host__ __device__ constexpr int face_node(int P, int side, int l, int kk) {
 }
 
 template <int P, int EPB, typename real, bool AFFINE, bool LGL>
-__global__ void __launch_bounds__(block_for(P)) stage_kernel(StageArgs<real> a) {
+__global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real> a) {
   constexpr int NP = P * P;
   constexpr int FT = 4 * P;
-  constexpr int NW = block_for(P) / 32;
+  constexpr int NW = block_of(P, EPB) / 32;
   __shared__ real s_mat[NP + 4 * P];
   __shared__ real s_Fc[4][EPB][NP];
   __shared__ real s_Gc[4][EPB][NP];

@@ -198,6 +198,23 @@ class GpuDGSEM:
         uB = np.ascontiguousarray(uB, dtype=np.float64).ravel()
         self._check(self._lib.hg_set_boundary_state(self._h, int(zone), uB.ctypes.data_as(L.F64P), uB.size))
 
+    def autotune(self, trials=10):
+        """Time the elements-per-CTA variants on the resident state and keep the fastest:
+        {"chosen": variant, "ms": [ms per residual evaluation per variant], "tiling": get_tiling()}."""
+        ch = C.c_int32(0)
+        ms = np.zeros(L.TILINGS)
+        self._check(self._lib.hg_autotune(self._h, int(trials), C.byref(ch), ms.ctypes.data_as(L.F64P)))
+        return {"chosen": ch.value, "ms": ms.tolist(), "tiling": self.get_tiling()}
+
+    def set_tiling(self, variant):
+        self._check(self._lib.hg_set_tiling(self._h, int(variant)))
+
+    def get_tiling(self):
+        """{variant, elements per CTA, threads per CTA} of the stage kernels."""
+        out = (C.c_int32 * 3)()
+        self._check(self._lib.hg_get_tiling(self._h, out))
+        return dict(variant=out[0], elements_per_cta=out[1], threads_per_cta=out[2])
+
     def element_viscosity(self):
         n = self.info()["n_elements"]
         mu = np.zeros(n)

@@ -193,6 +193,19 @@ int  hg_mlp_grad(const float* params, const float* X, const float* t, const floa
                  float* grad);
 int  hg_mlp_train(float* params, const float* X, const float* t, const float* w, int64_t n, int32_t epochs,
                   int32_t batch, double lr, uint64_t seed, double* epoch_loss);
+/* Elements-per-CTA autotuner (no reference counterpart).  The stage kernels exist in
+ * HG_TILINGS tilings: variant 0 packs several elements per CTA (fewer, larger CTAs), variant 1
+ * one or two (more CTAs in flight: small meshes, the smaller buckets of an ensemble).
+ * hg_autotune times `trials` residual evaluations of the resident state in each variant with
+ * CUDA events on the context's stream, keeps the faster one (chosen, and ms per evaluation
+ * for each variant in ms_per_variant[HG_TILINGS], both may be NULL), and leaves the residual
+ * of the resident state for hg_residuals as hg_time_derivative does; the state is not changed.
+ * hg_set_tiling forces a variant; hg_get_tiling: out = {variant, elements per CTA, threads
+ * per CTA}.  Results are the same in every variant to rounding of the per-CTA reductions. */
+#define HG_TILINGS 2
+int  hg_autotune(hg_ctx* ctx, int32_t trials, int32_t* chosen, double* ms_per_variant);
+int  hg_set_tiling(hg_ctx* ctx, int32_t variant);
+int  hg_get_tiling(const hg_ctx* ctx, int32_t out[3]);
 /* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
 int  hg_info(const hg_ctx* ctx, int32_t out[4]);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N
