@@ -51,7 +51,8 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
             "hg_set_stream", "hg_synchronize", "hg_device_state", "hg_launch_count", "hg_nodes", "hg_info",
             "hg_profile", "hg_kernel_times", "hg_residuals_noalloc", "hg_set_sensor", "hg_sensor_eval",
             "hg_element_viscosity", "hg_mlp_forward", "hg_mlp_grad", "hg_mlp_train", "hg_set_boundary_state",
-            "hg_autotune", "hg_set_tiling", "hg_get_tiling")
+            "hg_autotune", "hg_set_tiling", "hg_get_tiling", "hg_group_create", "hg_group_destroy",
+            "hg_group_time_steps", "hg_group_last_error")
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
@@ -102,6 +103,12 @@ def load():
     L.hg_autotune.argtypes = [vp, C.c_int32, I32P, F64P]
     L.hg_set_tiling.argtypes = [vp, C.c_int32]
     L.hg_get_tiling.argtypes = [vp, I32P]
+    L.hg_group_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]
+    L.hg_group_destroy.argtypes = [vp]
+    L.hg_group_destroy.restype = None
+    L.hg_group_time_steps.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double]
+    L.hg_group_last_error.argtypes = [vp]
+    L.hg_group_last_error.restype = C.c_char_p
     L.hg_mlp_forward.argtypes = [f32p, f32p, C.c_int64, f32p]
     L.hg_mlp_grad.argtypes = [f32p, f32p, f32p, f32p, C.c_int64, F64P, f32p]
     L.hg_mlp_train.argtypes = [f32p, f32p, f32p, f32p, C.c_int64, C.c_int32, C.c_int32, C.c_double, C.c_uint64, F64P]

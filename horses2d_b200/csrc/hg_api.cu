@@ -28,9 +28,12 @@ static T* dalloc(size_t n) {
 }
 
 static void drop_graph(hg_ctx* c) {
-  if (c->gexec) cudaGraphExecDestroy(c->gexec);
-  c->gexec = nullptr;
+  for (auto& x : c->gexec) {
+    if (x) cudaGraphExecDestroy(x);
+    x = nullptr;
+  }
   c->g_scheme = -1;
+  ++c->gen;
 }
 
 static void free_ctx(hg_ctx* c) {
@@ -547,10 +550,12 @@ extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
 // dt only, the stepping time t enters no kernel).
 static void graph_steps(hg_ctx* c, int scheme, int n_steps, double t0, double dt) {
   int s = 0;
-  one_step(c, scheme, t0, dt);   // first launches set kernel attributes outside any capture
-  ++s;
-  if (!c->gexec || c->g_scheme != scheme || c->g_dt != dt || c->g_cur != c->cur) {
-    drop_graph(c);
+  if (c->g_scheme != scheme || c->g_dt != dt) drop_graph(c);
+  if (!c->gexec[c->cur]) {
+    one_step(c, scheme, t0, dt);   // first launches set kernel attributes outside any capture
+    ++s;
+  }
+  if (!c->gexec[c->cur]) {
     const int64_t l0 = c->launches;
     const int cur0 = c->cur;
     HG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
@@ -566,20 +571,20 @@ static void graph_steps(hg_ctx* c, int scheme, int n_steps, double t0, double dt
       throw;
     }
     cudaGraph_t g = nullptr;
-    HG_CUDA(cudaStreamEndCapture(c->stream, &g));
-    const cudaError_t ie = cudaGraphInstantiate(&c->gexec, g, 0);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    c->g_launches[cur0] = c->launches - l0;
+    c->launches = l0;
+    c->cur = cur0;   // two steps flip the parity an even number of times; the capture ran nothing
+    HG_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&c->gexec[cur0], g, 0);
     cudaGraphDestroy(g);
     HG_CUDA(ie);
-    c->g_launches = c->launches - l0;
-    c->launches = l0;
-    c->cur = cur0;
     c->g_scheme = scheme;
     c->g_dt = dt;
-    c->g_cur = c->cur;
   }
   for (; s + 2 <= n_steps; s += 2) {
-    HG_CUDA(cudaGraphLaunch(c->gexec, c->stream));
-    c->launches += c->g_launches;
+    HG_CUDA(cudaGraphLaunch(c->gexec[c->cur], c->stream));
+    c->launches += c->g_launches[c->cur];
   }
   for (; s < n_steps; ++s) one_step(c, scheme, t0 + s * dt, dt);
 }
@@ -774,6 +779,159 @@ extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, 
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+// ------------------------------------------------------------------ context groups
+// Independent contexts (an ensemble packed by polynomial order, one context per order) stepped by
+// one CUDA graph: each member's launches are captured on a stream of its own, forked from and joined
+// back to the members' common stream, so the members' kernels run concurrently and one graph launch
+// advances all of them by two steps.
+struct hg_group {
+  std::vector<hg_ctx*> m;
+  std::vector<cudaStream_t> fork;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t start = nullptr;
+  // one graph per trace-buffer parity of the first member; the members' parities relative to it and
+  // their set-up generations must match the capture
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int scheme = -1;
+  double dt = 0.0;
+  std::vector<int> rel;
+  std::vector<int64_t> gen, per_launches[2];
+  std::string err;
+};
+
+static void group_drop(hg_group* g) {
+  for (auto& x : g->exec) {
+    if (x) cudaGraphExecDestroy(x);
+    x = nullptr;
+  }
+}
+
+static void group_free(hg_group* g) {
+  group_drop(g);
+  for (cudaStream_t s : g->fork) if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t e : g->join) if (e) cudaEventDestroy(e);
+  if (g->start) cudaEventDestroy(g->start);
+}
+
+extern "C" int hg_group_create(hg_ctx* const* ctxs, int32_t n, hg_group** out) {
+  if (!out) return 1;
+  *out = nullptr;
+  hg_group* g = new hg_group();
+  try {
+    if (!ctxs || n < 1) throw std::runtime_error("a group needs at least one context");
+    for (int i = 0; i < n; ++i) {
+      if (!ctxs[i]) throw std::runtime_error("null context in group");
+      if (ctxs[i]->stream != ctxs[0]->stream) throw std::runtime_error("group members must share one stream");
+      for (int j = 0; j < i; ++j) if (ctxs[j] == ctxs[i]) throw std::runtime_error("context listed twice");
+      g->m.push_back(ctxs[i]);
+    }
+    g->fork.assign(n, nullptr);
+    g->join.assign(n, nullptr);
+    for (int i = 0; i < n; ++i) {
+      HG_CUDA(cudaStreamCreateWithFlags(&g->fork[i], cudaStreamNonBlocking));
+      HG_CUDA(cudaEventCreateWithFlags(&g->join[i], cudaEventDisableTiming));
+    }
+    HG_CUDA(cudaEventCreateWithFlags(&g->start, cudaEventDisableTiming));
+  } catch (const std::exception& ex) {
+    g_create_err = ex.what();
+    group_free(g);
+    delete g;
+    return 1;
+  }
+  *out = g;
+  return 0;
+}
+
+extern "C" void hg_group_destroy(hg_group* g) {
+  if (!g) return;
+  group_free(g);
+  delete g;
+}
+
+extern "C" const char* hg_group_last_error(const hg_group* g) { return g ? g->err.c_str() : g_create_err.c_str(); }
+
+extern "C" int hg_group_time_steps(hg_group* g, int32_t scheme, int32_t n_steps, double t0, double dt) {
+  if (!g) return 1;
+  const size_t n = g->m.size();
+  std::vector<cudaStream_t> own(n);
+  for (size_t i = 0; i < n; ++i) own[i] = g->m[i]->stream;
+  try {
+    for (hg_ctx* c : g->m) {
+      require_state(c);
+      if (c->prof) throw std::runtime_error("group stepping with kernel timing on: step the members instead");
+      if (c->stream != g->m[0]->stream) throw std::runtime_error("group members must share one stream");
+    }
+    cudaStream_t main = g->m[0]->stream;
+    int s = 0;
+    if (n_steps >= 3) {
+      bool valid = g->scheme == scheme && g->dt == dt && g->rel.size() == n;
+      for (size_t i = 0; valid && i < n; ++i)
+        valid = g->rel[i] == (g->m[i]->cur ^ g->m[0]->cur) && g->gen[i] == g->m[i]->gen;
+      if (!valid) {
+        group_drop(g);
+        g->rel.assign(n, 0);
+        g->gen.assign(n, 0);
+        for (size_t i = 0; i < n; ++i) { g->rel[i] = g->m[i]->cur ^ g->m[0]->cur; g->gen[i] = g->m[i]->gen; }
+        g->scheme = scheme;
+        g->dt = dt;
+      }
+      if (!g->exec[g->m[0]->cur]) {
+        for (hg_ctx* c : g->m) one_step(c, scheme, t0, dt);   // kernel attributes are set outside any capture
+        ++s;
+      }
+      const int p = g->m[0]->cur;
+      if (!g->exec[p]) {
+        std::vector<int> cur0(n);
+        std::vector<int64_t> l0(n);
+        for (size_t i = 0; i < n; ++i) { cur0[i] = g->m[i]->cur; l0[i] = g->m[i]->launches; }
+        HG_CUDA(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+        try {
+          HG_CUDA(cudaEventRecord(g->start, main));
+          for (size_t i = 0; i < n; ++i) {
+            HG_CUDA(cudaStreamWaitEvent(g->fork[i], g->start, 0));
+            g->m[i]->stream = g->fork[i];
+            one_step(g->m[i], scheme, t0, dt);
+            one_step(g->m[i], scheme, t0, dt);
+            g->m[i]->stream = own[i];
+            HG_CUDA(cudaEventRecord(g->join[i], g->fork[i]));
+            HG_CUDA(cudaStreamWaitEvent(main, g->join[i], 0));
+          }
+        } catch (...) {
+          for (size_t i = 0; i < n; ++i) { g->m[i]->stream = own[i]; g->m[i]->cur = cur0[i]; g->m[i]->launches = l0[i]; }
+          cudaGraph_t g0 = nullptr;
+          cudaStreamEndCapture(main, &g0);
+          if (g0) cudaGraphDestroy(g0);
+          throw;
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(main, &graph);
+        g->per_launches[p].assign(n, 0);
+        for (size_t i = 0; i < n; ++i) {
+          g->per_launches[p][i] = g->m[i]->launches - l0[i];
+          g->m[i]->launches = l0[i];
+          g->m[i]->cur = cur0[i];
+        }
+        HG_CUDA(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&g->exec[p], graph, 0);
+        cudaGraphDestroy(graph);
+        HG_CUDA(ie);
+      }
+      for (; s + 2 <= n_steps; s += 2) {
+        HG_CUDA(cudaGraphLaunch(g->exec[p], main));
+        for (size_t i = 0; i < n; ++i) g->m[i]->launches += g->per_launches[p][i];
+      }
+    }
+    for (; s < n_steps; ++s)
+      for (hg_ctx* c : g->m) one_step(c, scheme, t0 + s * dt, dt);
+    HG_CUDA(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& ex) {
+    for (size_t i = 0; i < n; ++i) g->m[i]->stream = own[i];
+    g->err = ex.what();
+    return 1;
+  }
 }
 
 // ------------------------------------------------------------------ elements-per-CTA autotuner

@@ -65,11 +65,13 @@ struct hg_ctx {
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
   double save_umax = 0.0, save_amax = 0.0;
-  // CUDA graph of two time steps (hg_time_steps): valid for one scheme, dt and trace-buffer parity
-  cudaGraphExec_t gexec = nullptr;
-  int g_scheme = -1, g_cur = -1;
+  // CUDA graphs of two time steps (hg_time_steps), one per trace-buffer parity at their start (a
+  // step flips the parity once per stage): valid for one scheme and dt
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int g_scheme = -1;
+  int64_t gen = 0;                // bumped whenever captured launches go stale (context groups check it)
   double g_dt = 0.0;
-  int64_t g_launches = 0;
+  int64_t g_launches[2] = {0, 0};
   // per-kernel timing (hg_profile): event pairs recorded around each launch
   bool prof = false;
   std::vector<cudaEvent_t> prof_pool;

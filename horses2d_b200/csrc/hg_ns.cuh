@@ -64,7 +64,7 @@ __host__ __device__ constexpr int epb_ns(int P) {
   return P == 2 ? 16 : P == 3 ? 7 : P == 4 ? 8 : P == 5 ? 5 : P == 6 ? 4 : P == 7 ? 3 : 2;
 }
 __host__ __device__ constexpr int epb_ns_small(int P) {
-  return P == 2 ? 4 : P == 3 ? 2 : P == 4 ? 2 : 1;
+  return P == 2 ? 4 : P <= 6 ? 2 : 1;
 }
 __host__ __device__ constexpr int epb_ns_of(int P, int variant) { return variant ? epb_ns_small(P) : epb_ns(P); }
 __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) + 31) / 32) * 32; }

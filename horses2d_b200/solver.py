@@ -226,3 +226,29 @@ class GpuDGSEM:
         out = (C.c_int32 * 4)()
         self._check(self._lib.hg_info(self._h, out))
         return dict(N=out[0], n_elements=out[1], affine=bool(out[2]), precision=out[3])
+
+
+class GpuGroup:
+    """Independent contexts stepped together by one CUDA graph (hg_group_*): an ensemble packed into
+    one GpuDGSEM per polynomial order.  The members must share one stream and have their state set."""
+
+    def __init__(self, members):
+        self.members = list(members)   # keeps the contexts alive while the group exists
+        lib = L.load()
+        arr = (C.c_void_p * len(self.members))(*[m._h.value for m in self.members])
+        h = C.c_void_p()
+        if lib.hg_group_create(arr, len(self.members), C.byref(h)) != 0:
+            raise HorsesGpuError(lib.hg_group_last_error(None).decode())
+        self._h = h
+        self._lib = lib
+
+    def time_steps(self, scheme, n_steps, t0, dt):
+        if self._lib.hg_group_time_steps(self._h, int(scheme), int(n_steps), float(t0), float(dt)) != 0:
+            raise HorsesGpuError(self._lib.hg_group_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.hg_group_destroy(self._h)
+            self._h = None
+
+    __del__ = close

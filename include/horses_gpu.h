@@ -193,6 +193,21 @@ int  hg_mlp_grad(const float* params, const float* X, const float* t, const floa
                  float* grad);
 int  hg_mlp_train(float* params, const float* X, const float* t, const float* w, int64_t n, int32_t epochs,
                   int32_t batch, double lr, uint64_t seed, double* epoch_loss);
+/* Context groups (no reference counterpart): independent contexts -- an ensemble of cases,
+ * packed into one context per polynomial order -- advanced together.  hg_group_time_steps
+ * runs n_steps steps of every member; from three steps on, it captures two steps of all
+ * members into one CUDA graph in which each member's launches run on a stream of their own
+ * (forked from and joined back to the members' common stream), so the members' kernels
+ * overlap and one graph launch advances the whole ensemble by two steps.  Members must share
+ * one stream (hg_set_stream) and have their state set; kernel timing must be off.  The graph
+ * is rebuilt when the scheme, dt or a member's set-up changes.  The group holds no data of
+ * its own: destroying it leaves the members as they are. */
+typedef struct hg_group hg_group;
+int  hg_group_create(hg_ctx* const* ctxs, int32_t n, hg_group** out);
+void hg_group_destroy(hg_group* group);
+int  hg_group_time_steps(hg_group* group, int32_t scheme, int32_t n_steps, double t0, double dt);
+const char* hg_group_last_error(const hg_group* group);   /* group may be NULL: last hg_group_create error */
+
 /* Elements-per-CTA autotuner (no reference counterpart).  The stage kernels exist in
  * HG_TILINGS tilings: variant 0 packs several elements per CTA (fewer, larger CTAs), variant 1
  * one or two (more CTAs in flight: small meshes, the smaller buckets of an ensemble).
