@@ -91,6 +91,8 @@ def lib():
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
         L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
+        L.or_surface_integrals.restype = i
+        L.or_surface_integrals.argtypes = [vp, i, dp]
         L.or_zone_edge_nodes.restype = i
         L.or_zone_edge_nodes.argtypes = [vp, i, dp]
         L.or_set_zone_state.argtypes = [vp, i, dp]
@@ -246,6 +248,15 @@ class Oracle:
         X = np.zeros((n, 2))
         lib().or_zone_edge_nodes(self.h, zone, _p(X, C.c_double))
         return X
+
+    def surface_integrals(self, zone):
+        """Dimensionless surface integrals of zone `zone` over the traces of the last residual
+        evaluation: dict(surface, pressure, pressure_force (2), viscous_force (2), mass_flow, flow)."""
+        out = np.zeros(8)
+        if lib().or_surface_integrals(self.h, zone, _p(out, C.c_double)) != 0:
+            raise ValueError(f"unknown zone {zone}")
+        return dict(surface=out[0], pressure=out[1], pressure_force=out[2:4].copy(), viscous_force=out[4:6].copy(),
+                    mass_flow=out[6], flow=out[7])
 
     def set_zone_state(self, zone, uB):
         uB = np.ascontiguousarray(uB, dtype=np.float64)

@@ -117,6 +117,10 @@ int     or_edge_count_by_type(void* h, int type);
  * BoundaryConditions/BoundaryConditionFunctionDrivers.incf): or_zone_edge_nodes returns the
  * number of edge nodes of a zone and (if X != NULL) their coordinates [n][2], edges in
  * mesh order; or_set_zone_state sets the zone's boundary state uB [n][4] at those nodes. */
+/* Surface integrals of zone (marker) `zone` over the traces of the last residual evaluation
+ * (Mesh/QuadMesh_Integrals.incf), dimensionless: out = {surface, pressure, pressure force x, y,
+ * viscous-tensor force x, y, mass flow, volume flow}.  Returns 0, or -1 for an unknown zone. */
+int     or_surface_integrals(void* h, int zone, double out[8]);
 int     or_zone_edge_nodes(void* h, int zone, double* X);
 void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,

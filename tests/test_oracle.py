@@ -18,6 +18,8 @@
   0.1), Euler walls and two newDirichlet zones, Mach 2, N = 3, Legendre-Gauss,
   steady RK5 (CFL 0.1, dt cap 2, residual 1e-8); the reference asserts
   iteration 9884 and the four final residuals to 1e-11.
+* CylinderRe100 benchmark: exact Riemann solver on every zone, p-refinement, BR1, steady RK5; final
+  residuals (1e-11) and the wall's lift and drag coefficients (surface integrals, 1e-12).
 * Spectral building blocks: exactness of the nodal derivative and quadrature.
 * Free-stream preservation on curved meshes, conservation on periodic meshes.
 """
@@ -162,6 +164,40 @@ def test_ns_freestream_preservation_curved():
         q = np.array([1.0, 0.3 * np.sqrt(1.4), 0.0, 2.5 + 0.5 * 0.09 * 1.4])
         orc.set_state(np.tile(q, orc.ndof // 4))
         assert np.abs(orc.time_derivative(0.0)).max() <= 1e-8
+
+
+def test_cylinder_re100_benchmark_golden():
+    """CylinderRe100 (TestCases/Benchmark/Simulations/CylinderRe100): Navier-Stokes, Re 100, M 0.1, BR1,
+    HLL inside and the exact Riemann solver on every zone (three Dirichlet zones, a partially
+    non-reflective pressure outlet, an adiabatic wall), p-refinement zones of orders 2/8/6/4 on
+    Legendre-Gauss nodes (mortars of the projection types 3-6), steady RK5 for 250 iterations at
+    CFL 0.1, dt cap 1e-2.  The reference asserts the final residuals to 1e-11 and the lift and drag
+    coefficients of the wall -- surface integrals of pressure and of the viscous tensor over the
+    last stage's traces (Monitors.f90:1130-1138) -- to 1e-12."""
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["CylinderRe100"]
+    m = load_mesh("CylinderBench")
+    porder = np.array([8, 2, 8, 6, 4])[m["p_zones"]]     # zone 0 would take the default order 8
+    ex = O.EXACT
+    bcs = [dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_DIRICHLET, riemann=ex),
+           dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2, riemann=ex),
+           dict(type=O.BC_VISCOUSWALL, wall_type=2, riemann=ex)]
+    orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.HLL, mach=0.1, reynolds=100.0, prandtl=0.72, navier_stokes=1,
+                   viscous=O.BR1, bcs=bcs)
+    r = orc.ref
+    cv = 287.15 * 2.5   # UniformInitialCondition, dimensional
+    q = np.array([r["rho"], r["rho"] * r["V"], 0.0, cv * r["rho"] * r["T"] + 0.5 * r["rho"] * r["V"] * r["V"]])
+    q = q / np.array([r["rho"], r["rho"] * r["a"], r["rho"] * r["a"], r["p"]])
+    orc.set_state(np.tile(q, orc.ndof // 4))
+    it, _ = orc.integrate(O.RK5, transient=False, t0=0.0, t_end=1e9, max_iter=250, cfl=0.1, dt_cap=1e-2,
+                          residual_target=1e-14)
+    assert it == 250
+    assert np.max(np.abs(orc.residuals() - np.array(golden["residuals"]))) <= 1e-11
+    # lift / drag surface monitors: (pressure force - sqrt(gamma) M viscous force) p_ref L / (rho V^2 S / 2)
+    si = orc.surface_integrals(5)
+    dyn = 0.5 * r["rho"] * r["V"] * r["V"] * 1.0
+    force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
+    assert abs(force[1] / dyn - golden["cl"]) <= 1e-12
+    assert abs(force[0] / dyn - golden["cd"]) <= 1e-12
 
 
 def test_ramp_benchmark_golden():
