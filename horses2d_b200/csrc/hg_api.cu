@@ -43,7 +43,8 @@ static void free_ctx(hg_ctx* c) {
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
                   c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
-                  c->d_FX, c->d_bq};
+                  c->d_FX, c->d_bq, c->d_si_out};
+  for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
 }
@@ -130,6 +131,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.sensor = sensor_args(c);
   if (c->exact) launch_exact_flux<real>(c);
   HG_DISPATCH_P(c->P, ns_dispatch, c, a);
+  c->last_T = c->cur;   // trace buffer of the state this stage evaluated (surface integrals read it)
   if (update) c->cur ^= 1;
 }
 
@@ -158,6 +160,7 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.pc = c->pc;
   if (c->exact) launch_exact_flux<real>(c);
   HG_DISPATCH_P(c->P, stage_dispatch, c, a);
+  c->last_T = c->cur;   // trace buffer of the state this stage evaluated (surface integrals read it)
   if (update) c->cur ^= 1;
 }
 
@@ -776,6 +779,34 @@ extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, 
     }
     HG_CUDA(cudaMemcpyAsync(c->d_bq + size_t(c->zone_row0[z]) * c->P * 4, uB, size_t(expect) * sizeof(double),
                             cudaMemcpyHostToDevice, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+// ------------------------------------------------------------------ surface integrals
+extern "C" int hg_surface_integrals(hg_ctx* c, int32_t zone, double out[8]) {
+  try {
+    require_state(c);
+    if (!out) throw std::runtime_error("null output");
+    if (zone < 1 || zone > int(c->zone_type.size()) || c->zone_type[zone - 1] < 0)
+      throw std::runtime_error("unknown zone " + std::to_string(zone));
+    const int z = zone - 1;
+    if (c->d_zone_sides.size() < c->zone_sides.size()) c->d_zone_sides.resize(c->zone_sides.size(), nullptr);
+    const std::vector<int>& sides = c->zone_sides[z];
+    if (sides.empty()) {
+      for (int k = 0; k < 8; ++k) out[k] = 0.0;
+      return 0;
+    }
+    if (!c->d_zone_sides[z]) {
+      c->d_zone_sides[z] = dalloc<int>(sides.size());
+      HG_CUDA(cudaMemcpy(c->d_zone_sides[z], sides.data(), sides.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (!c->d_si_out) c->d_si_out = dalloc<double>(8);
+    if (c->precision == HG_PREC_FP32) launch_surface_integrals<float>(c, zone, c->d_si_out);
+    else launch_surface_integrals<double>(c, zone, c->d_si_out);
+    HG_CUDA(cudaGetLastError());
+    HG_CUDA(cudaMemcpyAsync(out, c->d_si_out, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }

@@ -61,6 +61,9 @@ struct hg_ctx {
   std::vector<int> zone_type;                 // per zone: HG_BC_*
   std::vector<int> zone_row0;                 // per zone: first state row, -1 until fed per node
   std::vector<int4> h_side;                   // host copy of the side table
+  std::vector<int*> d_zone_sides;             // per zone: its sides on the device (surface integrals), lazily
+  double* d_si_out = nullptr;                 // surface-integral results [8]
+  int last_T = 0;                             // trace buffer of the last residual evaluation's state
   bool state_set = false;
   int64_t launches = 0;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
@@ -137,6 +140,7 @@ template <int P, typename real> void launch_trace_P(hg_ctx* c);
 template <int P, typename real, int V> void launch_ns_PV(hg_ctx* c, const NSArgs<real>& a);
 template <int P, typename real> void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out);
 template <typename real> void launch_exact_flux(hg_ctx* c);
+template <typename real> void launch_surface_integrals(hg_ctx* c, int zone, double* d_out);
 
 inline SensorArgs sensor_args(const hg_ctx* c) {
   SensorArgs s;

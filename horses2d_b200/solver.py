@@ -198,6 +198,14 @@ class GpuDGSEM:
         uB = np.ascontiguousarray(uB, dtype=np.float64).ravel()
         self._check(self._lib.hg_set_boundary_state(self._h, int(zone), uB.ctypes.data_as(L.F64P), uB.size))
 
+    def surface_integrals(self, zone):
+        """Dimensionless surface integrals of zone `zone` over the traces of the last residual evaluation:
+        dict(surface, pressure, pressure_force (2), viscous_force (2), mass_flow, flow)."""
+        out = np.zeros(8)
+        self._check(self._lib.hg_surface_integrals(self._h, int(zone), out.ctypes.data_as(L.F64P)))
+        return dict(surface=out[0], pressure=out[1], pressure_force=out[2:4].copy(), viscous_force=out[4:6].copy(),
+                    mass_flow=out[6], flow=out[7])
+
     def autotune(self, trials=10):
         """Time the elements-per-CTA variants on the resident state and keep the fastest:
         {"chosen": variant, "ms": [ms per residual evaluation per variant], "tiling": get_tiling()}."""

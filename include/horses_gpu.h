@@ -131,6 +131,17 @@ int  hg_estimate_dt(hg_ctx* ctx, double cfl, double dt_cap, double* dt);
  * kinds recompute their ghost state from the zone state each stage and are rejected. */
 int  hg_set_boundary_state(hg_ctx* ctx, int32_t zone, const double* uB, int64_t n_values);
 
+/* == the mesh functions of the surface monitors (Mesh/QuadMesh_Integrals.incf:67-346:
+ * ScalarScalar "Surface" and "pressure", ScalarVector "pressure", VectorVector "mass-flow" and
+ * "flow", TensorVector "viscous" with ComputeViscousTensor, Physics/ViscousFluxes.f90:416-461),
+ * over zone `zone` (1-based marker) and the traces of the state of the last residual evaluation:
+ * after hg_time_derivative the resident state, after a time step its last stage's input state,
+ * as the reference's monitors (updated after TimeStep) read them.  Dimensionless, as the mesh
+ * functions return them: out = {surface, pressure, pressure force x, y, viscous-tensor force
+ * x, y (0 without viscosity), mass flow, volume flow}.  Lift / drag: (pressure force - sqrt(gamma)
+ * M viscous force) p_ref L / (rho_ref V_ref^2 S / 2) (Monitors.f90:1130-1138). */
+int  hg_surface_integrals(hg_ctx* ctx, int32_t zone, double out[8]);
+
 /* Stream control: run on the caller's stream (e.g. a framework's current stream). */
 int  hg_set_stream(hg_ctx* ctx, void* cuda_stream);
 int  hg_synchronize(hg_ctx* ctx);
