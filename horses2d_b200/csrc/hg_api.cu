@@ -264,6 +264,8 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   mats.insert(mats.end(), ops.dlbw1.begin(), ops.dlbw1.end());
   mats.insert(mats.end(), ops.w.begin(), ops.w.end());
   mats.insert(mats.end(), ops.Vinv.begin(), ops.Vinv.end());
+  mats.insert(mats.end(), ops.xi.begin(), ops.xi.end());   // probes: nodes and barycentric weights
+  mats.insert(mats.end(), ops.wb.begin(), ops.wb.end());
   c->sensor_s0 = std::log10(1.0 / std::pow(double(N + 1), 4.0));   // modal ramp defaults
   c->sensor_kappa = 1.0;
 
@@ -810,6 +812,41 @@ extern "C" int hg_surface_integrals(hg_ctx* c, int32_t zone, double out[8]) {
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_probes(hg_ctx* c, int32_t n, const int32_t* elements, const double* xi_eta, double* out) {
+  int* d_el = nullptr;
+  double* d_x = nullptr;
+  double* d_o = nullptr;
+  try {
+    require_state(c);
+    if (n < 0 || (n > 0 && (!elements || !xi_eta || !out))) throw std::runtime_error("bad probe arguments");
+    for (int k = 0; k < n; ++k) {
+      if (elements[k] < 0 || elements[k] >= c->n_el) throw std::runtime_error("probe element out of range");
+      for (int d = 0; d < 2; ++d)
+        if (!(xi_eta[2 * k + d] >= 0.0 && xi_eta[2 * k + d] <= 1.0))
+          throw std::runtime_error("probe reference coordinates must lie in [0,1]");
+    }
+    if (n == 0) return 0;
+    d_el = dalloc<int>(n);
+    d_x = dalloc<double>(size_t(n) * 2);
+    d_o = dalloc<double>(size_t(n) * 4);
+    HG_CUDA(cudaMemcpyAsync(d_el, elements, size_t(n) * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    HG_CUDA(cudaMemcpyAsync(d_x, xi_eta, size_t(n) * 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    launch_probes(c, n, d_el, d_x, d_o);
+    HG_CUDA(cudaGetLastError());
+    HG_CUDA(cudaMemcpyAsync(out, d_o, size_t(n) * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(d_el);
+    cudaFree(d_x);
+    cudaFree(d_o);
+    return 0;
+  } catch (const std::exception& ex) {
+    if (d_el) cudaFree(d_el);
+    if (d_x) cudaFree(d_x);
+    if (d_o) cudaFree(d_o);
+    return fail(c, ex);
+  }
 }
 
 // ------------------------------------------------------------------ context groups

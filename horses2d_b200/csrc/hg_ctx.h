@@ -141,6 +141,7 @@ template <int P, typename real, int V> void launch_ns_PV(hg_ctx* c, const NSArgs
 template <int P, typename real> void launch_sensor_eval_P(hg_ctx* c, float* feat, double* out);
 template <typename real> void launch_exact_flux(hg_ctx* c);
 template <typename real> void launch_surface_integrals(hg_ctx* c, int zone, double* d_out);
+void launch_probes(hg_ctx* c, int n, const int* d_elements, const double* d_xi_eta, double* d_out);
 
 inline SensorArgs sensor_args(const hg_ctx* c) {
   SensorArgs s;

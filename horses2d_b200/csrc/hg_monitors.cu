@@ -8,6 +8,7 @@
 // fixed subset of the zone's side nodes, then a fixed-order tree sums the eight values, so repeated
 // calls give identical results.
 #include "hg_ctx.h"
+#include <cfloat>
 
 namespace hg {
 
@@ -63,7 +64,52 @@ __global__ void __launch_bounds__(SI_THREADS) surface_integral_kernel(int n_side
   if (threadIdx.x < 8) out[threadIdx.x] = red[threadIdx.x][0];
 }
 
+// Probes (Monitors.f90:740-830): the resident state at reference coordinates (xi, eta) of an element,
+// BilinearForm(Q, l_xi, l_eta) = sum_i l_xi(i) sum_j Q(i,j) l_eta(j) (Generic/MatrixOperations.f90:185-209)
+// with the barycentric Lagrange basis of the element's nodes (exact at the nodes).  One thread per probe.
+__device__ __forceinline__ void lagrange_at(double x, int P, const double* nodes, const double* wb, double* l) {
+  bool match = false;
+  for (int j = 0; j < P; ++j) {
+    const double a = x, b = nodes[j];
+    const bool eq = (a == 0.0 || b == 0.0) ? fabs(a - b) <= 2.0 * DBL_EPSILON
+                                           : fabs(b - a) <= 2.0 * DBL_EPSILON * fmax(fabs(a), fabs(b));
+    l[j] = eq ? 1.0 : 0.0;
+    match = match || eq;
+  }
+  if (match) return;
+  double d = 0.0;
+  for (int j = 0; j < P; ++j) { const double t = wb[j] / (x - nodes[j]); l[j] = t; d += t; }
+  for (int j = 0; j < P; ++j) l[j] /= d;
+}
+
+__global__ void probe_kernel(int n, const int* elements, const double* xi_eta, const double* nodes, const double* wb,
+                             int P, const double* Q, double* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double lx[10], ly[10];
+  lagrange_at(xi_eta[2 * k], P, nodes, wb, lx);
+  lagrange_at(xi_eta[2 * k + 1], P, nodes, wb, ly);
+  const double* q = Q + size_t(elements[k]) * P * P * 4;
+  for (int v = 0; v < 4; ++v) {
+    double b = 0.0;
+    for (int i = 0; i < P; ++i) {
+      double t = 0.0;
+      for (int j = 0; j < P; ++j) t += q[(j * P + i) * 4 + v] * ly[j];
+      b += lx[i] * t;
+    }
+    out[4 * k + v] = b;
+  }
+}
+
 }  // namespace hg
+
+void launch_probes(hg_ctx* c, int n, const int* d_elements, const double* d_xi_eta, double* d_out) {
+  const int NP = c->P * c->P;
+  const double* nodes = c->d_mats + 3 * NP + 7 * c->P;   // after hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w Vinv
+  probe_kernel<<<(n + 127) / 128, 128, 0, c->stream>>>(n, d_elements, d_xi_eta, nodes, nodes + c->P, c->P, c->d_Q,
+                                                      d_out);
+  ++c->launches;
+}
 
 template <typename real>
 void launch_surface_integrals(hg_ctx* c, int zone, double* d_out) {

@@ -363,3 +363,61 @@ def ogrid(n_radial, n_azimuthal, r0, r1, stretch, np1=11):
     return dict(points=points.astype(np.float64), quads=quads.astype(np.int32), bdry_edges=be.astype(np.int32),
                 bdry_marker=bm.astype(np.int32), marker_names=np.array(["wall", "farfield"]),
                 curved_edges=np.array(ce, np.int32), curve_x=np.array(cx), curve_y=np.array(cy))
+
+
+def locate(desc, points, node_type, tol=1e-12, max_iter=30):
+    """Element (0-based) and reference coordinates (xi, eta) in [0,1]^2 of physical points, for probes
+    (the reference locates a probe once, at monitor construction).  The element map is the degree-N
+    interpolant of the descriptor's node coordinates (the transfinite map itself on straight-sided
+    elements); candidates are the elements whose bounding box (nodes and vertices, widened by a tenth)
+    holds the point, and the map is inverted by Newton's method.  Returns (elements [n] int32, xi_eta [n, 2]); raises ValueError for a
+    point outside the mesh."""
+    from ._lib import nodes as lib_nodes
+    pts = np.asarray(points, dtype=float).reshape(-1, 2)
+    N = int(np.asarray(desc["N"])[0])
+    P = N + 1
+    xi, _ = lib_nodes(N, node_type)
+    bw = np.array([1.0 / np.prod([xi[j] - xi[k] for k in range(P) if k != j]) for j in range(P)])
+    X = np.asarray(desc["x"], dtype=float).reshape(-1, P * P, 2)
+    V = np.asarray(desc["vertices"], dtype=float).reshape(-1, 4, 2)
+    lo, hi = np.minimum(X.min(1), V.min(1)), np.maximum(X.max(1), V.max(1))
+    pad = 0.1 * (hi - lo).max(1, keepdims=True)     # curved sides may bulge past nodes and vertices
+
+    def basis(x):
+        d = x - xi
+        hit = np.abs(d) <= 1e-15
+        if hit.any():
+            l = hit.astype(float)
+            # derivative at a node: l_j'(x_i) = D(i, j)
+            i = int(np.argmax(hit))
+            dl = np.array([(bw[j] / bw[i]) / (xi[i] - xi[j]) if j != i else 0.0 for j in range(P)])
+            dl[i] = -dl.sum()
+            return l, dl
+        t = bw / d
+        s = t.sum()
+        l = t / s
+        dt = -bw / d ** 2
+        dl = (dt * s - t * dt.sum()) / s ** 2
+        return l, dl
+
+    elements, coords = np.zeros(len(pts), np.int32), np.zeros((len(pts), 2))
+    for k, p in enumerate(pts):
+        cand = np.nonzero(np.all(lo - pad <= p, 1) & np.all(p <= hi + pad, 1))[0]
+        for e in cand:
+            G = X[e].reshape(P, P, 2)          # [eta][xi][d]
+            s = np.array([0.5, 0.5])
+            for _ in range(max_iter):
+                lx, dlx = basis(s[0])
+                ly, dly = basis(s[1])
+                f = np.einsum("j,i,jid->d", ly, lx, G) - p
+                J = np.stack([np.einsum("j,i,jid->d", ly, dlx, G), np.einsum("j,i,jid->d", dly, lx, G)], 1)
+                ds = np.linalg.solve(J, -f)
+                s = np.clip(s + ds, -0.5, 1.5)
+                if np.abs(ds).max() < tol:
+                    break
+            if np.all(s >= -1e-10) and np.all(s <= 1.0 + 1e-10):
+                elements[k], coords[k] = e, np.clip(s, 0.0, 1.0)
+                break
+        else:
+            raise ValueError(f"point {tuple(p)} is outside the mesh")
+    return elements, coords

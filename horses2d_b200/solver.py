@@ -206,6 +206,18 @@ class GpuDGSEM:
         return dict(surface=out[0], pressure=out[1], pressure_force=out[2:4].copy(), viscous_force=out[4:6].copy(),
                     mass_flow=out[6], flow=out[7])
 
+    def probes(self, elements, xi_eta):
+        """Resident state [n, 4] at probe points given by element (0-based) and reference coordinates [n, 2]
+        in [0,1] (mesh.locate turns physical points into these)."""
+        el = np.ascontiguousarray(elements, dtype=np.int32).ravel()
+        xe = np.ascontiguousarray(xi_eta, dtype=np.float64).reshape(-1, 2)
+        if xe.shape[0] != el.size:
+            raise HorsesGpuError("one (xi, eta) pair per probe")
+        out = np.zeros((el.size, 4))
+        self._check(self._lib.hg_probes(self._h, el.size, el.ctypes.data_as(L.I32P), xe.ctypes.data_as(L.F64P),
+                                        out.ctypes.data_as(L.F64P)))
+        return out
+
     def autotune(self, trials=10):
         """Time the elements-per-CTA variants on the resident state and keep the fastest:
         {"chosen": variant, "ms": [ms per residual evaluation per variant], "tiling": get_tiling()}."""

@@ -141,6 +141,12 @@ int  hg_set_boundary_state(hg_ctx* ctx, int32_t zone, const double* uB, int64_t 
  * x, y (0 without viscosity), mass flow, volume flow}.  Lift / drag: (pressure force - sqrt(gamma)
  * M viscous force) p_ref L / (rho_ref V_ref^2 S / 2) (Monitors.f90:1130-1138). */
 int  hg_surface_integrals(hg_ctx* ctx, int32_t zone, double out[8]);
+/* == Probe_t update (Monitors.f90:740-830): the resident state at n probe points, each given as an
+ * element (0-based) and its reference coordinates xi_eta[2k], xi_eta[2k+1] in [0,1] (the reference
+ * locates them once at construction); out[n][4] = the conservative dimensionless state
+ * sum_i l_xi(i) sum_j Q(i,j) l_eta(j) (BilinearForm, Generic/MatrixOperations.f90:185-209).  The
+ * derived probe variables (u, v, p, Mach) and reference-value factors are the caller's. */
+int  hg_probes(hg_ctx* ctx, int32_t n, const int32_t* elements, const double* xi_eta, double* out);
 
 /* Stream control: run on the caller's stream (e.g. a framework's current stream). */
 int  hg_set_stream(hg_ctx* ctx, void* cuda_stream);

@@ -71,6 +71,27 @@ void surface_integrals(const Oracle& o, int zone, double out[8]) {
 
 }  // namespace orc
 
+extern "C" int or_probe(void* h, int e, double xi, double eta, double out[4]) {
+  // Probe_t update (Monitors.f90:740-830): BilinearForm(Q, l_xi, l_eta) = dot_product(l_xi, Q l_eta)
+  // (Generic/MatrixOperations.f90:185-209), with the element's Lagrange basis at (xi, eta)
+  orc::Oracle& o = *static_cast<orc::Oracle*>(h);
+  if (e < 0 || e >= int(o.el.size())) return -1;
+  const orc::Element& E = o.el[e];
+  const int P = E.P;
+  const std::vector<double> lx = E.sp->lj(xi), ly = E.sp->lj(eta);
+  const double* Q = &o.Q[E.offset];
+  for (int v = 0; v < 4; ++v) {
+    double b = 0.0;
+    for (int i = 0; i < P; ++i) {
+      double t = 0.0;
+      for (int j = 0; j < P; ++j) t += Q[(j * P + i) * 4 + v] * ly[j];
+      b += lx[i] * t;
+    }
+    out[v] = b;
+  }
+  return 0;
+}
+
 extern "C" int or_surface_integrals(void* h, int zone, double out[8]) {
   orc::Oracle& o = *static_cast<orc::Oracle*>(h);
   if (zone < 1 || zone >= int(o.zones.size())) return -1;

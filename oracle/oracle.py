@@ -91,6 +91,8 @@ def lib():
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
         L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
+        L.or_probe.restype = i
+        L.or_probe.argtypes = [vp, i, C.c_double, C.c_double, dp]
         L.or_surface_integrals.restype = i
         L.or_surface_integrals.argtypes = [vp, i, dp]
         L.or_zone_edge_nodes.restype = i
@@ -257,6 +259,12 @@ class Oracle:
             raise ValueError(f"unknown zone {zone}")
         return dict(surface=out[0], pressure=out[1], pressure_force=out[2:4].copy(), viscous_force=out[4:6].copy(),
                     mass_flow=out[6], flow=out[7])
+
+    def probe(self, e, xi, eta):
+        out = np.zeros(4)
+        if lib().or_probe(self.h, int(e), float(xi), float(eta), _p(out, C.c_double)) != 0:
+            raise ValueError(f"unknown element {e}")
+        return out
 
     def set_zone_state(self, zone, uB):
         uB = np.ascontiguousarray(uB, dtype=np.float64)

@@ -121,6 +121,8 @@ int     or_edge_count_by_type(void* h, int type);
  * (Mesh/QuadMesh_Integrals.incf), dimensionless: out = {surface, pressure, pressure force x, y,
  * viscous-tensor force x, y, mass flow, volume flow}.  Returns 0, or -1 for an unknown zone. */
 int     or_surface_integrals(void* h, int zone, double out[8]);
+/* Probe (Monitors.f90:740-830): the state at reference coordinates (xi, eta) of element e (0-based). */
+int     or_probe(void* h, int e, double xi, double eta, double out[4]);
 int     or_zone_edge_nodes(void* h, int zone, double* X);
 void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,

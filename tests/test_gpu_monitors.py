@@ -57,3 +57,27 @@ def test_cylinder_surface_integrals_fp32():
     g.set_state(Q)
     g.compute_time_derivative(0.0)
     compare(g, orc, 1e-5)
+
+
+def test_probes_match_oracle():
+    """Probes (element + reference coordinates, located by mesh.locate on the cylinder O-grid) of the
+    resident state: BilinearForm of the element's nodal values, against the oracle's, to 1e-13;
+    a probe placed on a node returns the node's value."""
+    from horses2d_b200 import mesh as hmesh
+    orc, kw, Q0 = cylinder_ns(4, O.LG, O.BR1)
+    Q = perturbed(Q0, 0.02, seed=43)
+    orc.set_state(Q)
+    desc = orc.export_mesh()
+    g = hg.GpuDGSEM(desc, **kw)
+    g.set_state(Q)
+    pts = np.array([[0.75, 0.0], [0.6, 0.3], [-1.5, 0.7], [2.0, -1.0]])
+    el, xe = hmesh.locate(desc, pts, hg.NODES_LG)
+    xi, _ = hg.lib.nodes(4, hg.NODES_LG)
+    el = np.append(el, 7)
+    xe = np.vstack([xe, [xi[2], xi[3]]])
+    out = g.probes(el, xe)
+    for k in range(len(el)):
+        np.testing.assert_allclose(out[k], orc.probe(el[k], xe[k, 0], xe[k, 1]), rtol=1e-13, atol=1e-13)
+    np.testing.assert_array_equal(out[-1], Q.reshape(-1, 25, 4)[7, 3 * 5 + 2])
+    with pytest.raises(hg.HorsesGpuError):
+        g.probes([0], [[1.5, 0.5]])

@@ -81,3 +81,27 @@ def test_general_builder_matches_reference_construction(case):
         assert va[:4] == vb[:4], key
         np.testing.assert_allclose(va[4], vb[4], atol=1e-13)
         np.testing.assert_allclose(va[5], vb[5], rtol=1e-13)
+
+
+@pytest.mark.parametrize("kind", ["box", "ogrid"])
+def test_locate_points_for_probes(kind):
+    """mesh.locate recovers element and reference coordinates of points placed at known nodes (Gauss
+    nodes are interior, so the element is unique), on a box and on a curved O-grid."""
+    import horses2d_b200 as hg
+    N = 4
+    if kind == "box":
+        d = hmesh.box_descriptor(5, 4, -1.0, 1.5, 0.0, 2.0, N, hg.NODES_LG)
+    else:
+        d = hmesh.build_descriptor(hmesh.ogrid(4, 12, 0.5, 3.0, 1.2), N, hg.NODES_LG)
+    xi, _ = hg.lib.nodes(N, hg.NODES_LG)
+    X = np.asarray(d["x"]).reshape(-1, (N + 1) ** 2, 2)
+    rng = np.random.default_rng(3)
+    picks = [(int(e), int(i), int(j)) for e, i, j in zip(rng.integers(0, X.shape[0], 12), rng.integers(0, N + 1, 12),
+                                                          rng.integers(0, N + 1, 12))]
+    pts = np.array([X[e, j * (N + 1) + i] for e, i, j in picks])
+    el, xe = hmesh.locate(d, pts, hg.NODES_LG)
+    for (e, i, j), ek, (a, b) in zip(picks, el, xe):
+        assert ek == e
+        assert abs(a - xi[i]) < 1e-10 and abs(b - xi[j]) < 1e-10
+    with pytest.raises(ValueError):
+        hmesh.locate(d, [[100.0, 100.0]], hg.NODES_LG)
