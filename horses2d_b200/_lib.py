@@ -52,7 +52,8 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
             "hg_profile", "hg_kernel_times", "hg_residuals_noalloc", "hg_set_sensor", "hg_sensor_eval",
             "hg_element_viscosity", "hg_mlp_forward", "hg_mlp_grad", "hg_mlp_train", "hg_set_boundary_state",
             "hg_autotune", "hg_set_tiling", "hg_get_tiling", "hg_group_create", "hg_group_destroy",
-            "hg_group_time_steps", "hg_group_last_error", "hg_surface_integrals", "hg_probes")
+            "hg_group_time_steps", "hg_group_last_error", "hg_surface_integrals", "hg_probes",
+            "hg_mesh_connectivity", "hg_mesh_last_error")
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
@@ -103,6 +104,10 @@ def load():
     L.hg_autotune.argtypes = [vp, C.c_int32, I32P, F64P]
     L.hg_surface_integrals.argtypes = [vp, C.c_int32, F64P]
     L.hg_probes.argtypes = [vp, C.c_int32, I32P, F64P, F64P]
+    L.hg_mesh_connectivity.argtypes = [C.c_int32, C.c_int32, I32P, C.c_int32, I32P, I32P, C.c_int32, I32P, C.c_int32,
+                                       I32P, I32P, I32P, I32P, I32P, I32P]
+    L.hg_mesh_last_error.argtypes = []
+    L.hg_mesh_last_error.restype = C.c_char_p
     L.hg_set_tiling.argtypes = [vp, C.c_int32]
     L.hg_get_tiling.argtypes = [vp, I32P]
     L.hg_group_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]

@@ -421,3 +421,31 @@ def locate(desc, points, node_type, tol=1e-12, max_iter=30):
         else:
             raise ValueError(f"point {tuple(p)} is outside the mesh")
     return elements, coords
+
+
+def connectivity(m):
+    """Mesh-file connectivity through the library's O(E) builder (hg_mesh_connectivity), for a mesh dict
+    with points, quads (1-based point ids), bdry_edges, bdry_marker and optional curved_edges: the
+    reference's lists (1-based, list order) as dict(points_of_edges [F,3], elements_of_edges [F,3],
+    edge_marker [F], curved_edges [C], curve_inverted [C])."""
+    import ctypes as C
+    from . import _lib as L
+    lib = L.load()
+    quads = np.ascontiguousarray(m["quads"], dtype=np.int32).reshape(-1, 4)
+    be = np.ascontiguousarray(m["bdry_edges"], dtype=np.int32).reshape(-1, 2)
+    bm = np.ascontiguousarray(m["bdry_marker"], dtype=np.int32).ravel()
+    ce = np.ascontiguousarray(m.get("curved_edges", np.zeros((0, 2))), dtype=np.int32).reshape(-1, 2)
+    n_pts = int(np.asarray(m["points"]).reshape(-1, 2).shape[0])
+    cap = 4 * quads.shape[0]
+    nE = C.c_int32(0)
+    pts, els = np.zeros((cap, 3), np.int32), np.zeros((cap, 3), np.int32)
+    mk = np.zeros(cap, np.int32)
+    cedge, cinv = np.zeros(max(len(ce), 1), np.int32), np.zeros(max(len(ce), 1), np.int32)
+    p = lambda a: a.ctypes.data_as(L.I32P)   # noqa: E731
+    rc = lib.hg_mesh_connectivity(n_pts, quads.shape[0], p(quads), be.shape[0], p(be), p(bm), len(ce), p(ce), cap,
+                                  C.byref(nE), p(pts), p(els), p(mk), p(cedge), p(cinv))
+    if rc != 0:
+        raise ValueError(lib.hg_mesh_last_error().decode())
+    F = nE.value
+    return dict(points_of_edges=pts[:F], elements_of_edges=els[:F], edge_marker=mk[:F],
+                curved_edges=cedge[:len(ce)], curve_inverted=cinv[:len(ce)])

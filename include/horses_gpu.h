@@ -240,6 +240,26 @@ int  hg_set_tiling(hg_ctx* ctx, int32_t variant);
 int  hg_get_tiling(const hg_ctx* ctx, int32_t out[3]);
 /* Context facts: out = {N, n_elements, affine geometry path (0/1), precision}. */
 int  hg_info(const hg_ctx* ctx, int32_t out[4]);
+/* Mesh-file connectivity in O(E) (host code; replaces Mesh/MeshFile.f90:254-267, 287-652:
+ * computeFaces, mergeDividedFaces (twice), computeElementOfEdges, computeFaceMarkers,
+ * computeCurvedEdges, whose linked-list searches make preprocessing O(E^2)).  Same lists, same
+ * order and conventions as the reference; all ids 1-based as in the mesh file.
+ * In:  points_of_quads[E][4], points_of_bdryedges[B][2], bdry_marker[B], curved_edges_points[C][2].
+ * Out (caller-sized for `capacity` edges; 4E always suffices): n_edges;
+ *   points_of_edges[F][3]: the two ends as first listed, and the middle node of a subdivided
+ *     (hanging-node) edge, else 0;
+ *   elements_of_edges[F][3]: LEFT, RIGHT (0 on a boundary) or, for a subdivided edge, the element
+ *     holding both ends, the one holding end 1 and the middle, the one holding end 2 and the middle;
+ *   edge_marker[F]: 0 interior, else the boundary marker;
+ *   curved_edges[C]: the edge of each curve, curve_inverted[C]: 1 when the curve runs from the
+ *     edge's second end to its first (its coordinates are then to be reversed).
+ * Returns 0, or 1 with the reason in hg_mesh_last_error(). */
+int  hg_mesh_connectivity(int32_t n_points, int32_t n_elements, const int32_t* points_of_quads,
+                          int32_t n_bdry_edges, const int32_t* points_of_bdryedges, const int32_t* bdry_marker,
+                          int32_t n_curved, const int32_t* curved_edges_points, int32_t capacity,
+                          int32_t* n_edges, int32_t* points_of_edges, int32_t* elements_of_edges,
+                          int32_t* edge_marker, int32_t* curved_edges, int32_t* curve_inverted);
+const char* hg_mesh_last_error(void);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N
  * (NodesAndWeightsClass.f90:251-332 computeNodesAndWeights).  xi, w: N+1 doubles. */
 int  hg_nodes(int32_t N, int32_t node_type, double* xi, double* w);

@@ -12,6 +12,7 @@
  *                                   DGTimeIntegrator.f90:159-255
  *   Mesh_ComputeResiduals           Mesh/QuadMesh_Auxiliars.incf:22-38
  */
+#include <algorithm>
 #include "oracle_internal.h"
 #include <cstring>
 #include <cstdio>
@@ -296,4 +297,15 @@ extern "C" void or_set_zone_state(void* h, int zone, const double* uB) {
     for (int p = 0; p < f.P(); ++p, ++n)
       for (int k = 0; k < 4; ++k) f.uB_own[4 * p + k] = uB[4 * n + k];
   }
+}
+
+extern "C" int or_mesh_lists(void* h, int* points, int* elements, int* marker, int* curve_edge, int* curve_inv) {
+  const Oracle& o = *static_cast<Oracle*>(h);
+  const int F = int(o.mf_marker.size());
+  if (points) std::copy(o.mf_points.begin(), o.mf_points.end(), points);
+  if (elements) std::copy(o.mf_elements.begin(), o.mf_elements.end(), elements);
+  if (marker) std::copy(o.mf_marker.begin(), o.mf_marker.end(), marker);
+  if (curve_edge) std::copy(o.mf_curve_edge.begin(), o.mf_curve_edge.end(), curve_edge);
+  if (curve_inv) std::copy(o.mf_curve_inv.begin(), o.mf_curve_inv.end(), curve_inv);
+  return F;
 }

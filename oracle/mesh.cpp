@@ -557,11 +557,19 @@ void build_mesh(Oracle& o, const or_mesh& m) {
     cy[k].assign(m.curve_y + size_t(k) * m.curve_np1, m.curve_y + size_t(k + 1) * m.curve_np1);
     for (auto& v : cx[k]) v /= Lref;
     for (auto& v : cy[k]) v /= Lref;
-    if (L.e[pos].v[1] == a && L.e[pos].v[0] == b) {
+    const bool inv = L.e[pos].v[1] == a && L.e[pos].v[0] == b;
+    if (inv) {
       std::reverse(cx[k].begin(), cx[k].end());
       std::reverse(cy[k].begin(), cy[k].end());
     }
     if (curveOfEdge[pos] < 0) curveOfEdge[pos] = k;
+    o.mf_curve_edge.push_back(pos + 1);
+    o.mf_curve_inv.push_back(inv ? 1 : 0);
+  }
+  for (size_t i = 0; i < L.e.size(); ++i) {
+    for (int k = 0; k < 3; ++k) o.mf_points.push_back(k < L.e[i].N ? L.e[i].v[k] : 0);
+    for (int k = 0; k < 3; ++k) o.mf_elements.push_back(k < int(eoe[i].size()) ? eoe[i][k] : 0);
+    o.mf_marker.push_back(marker[i]);
   }
   // elements
   o.el.resize(m.n_elements);

@@ -91,6 +91,8 @@ def lib():
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
         L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
+        L.or_mesh_lists.restype = i
+        L.or_mesh_lists.argtypes = [vp, ip, ip, ip, ip, ip]
         L.or_probe.restype = i
         L.or_probe.argtypes = [vp, i, C.c_double, C.c_double, dp]
         L.or_surface_integrals.restype = i
@@ -259,6 +261,16 @@ class Oracle:
             raise ValueError(f"unknown zone {zone}")
         return dict(surface=out[0], pressure=out[1], pressure_force=out[2:4].copy(), viscous_force=out[4:6].copy(),
                     mass_flow=out[6], flow=out[7])
+
+    def mesh_lists(self, n_curved):
+        """(points [F,3], elements [F,3], marker [F], curve_edge [n_curved], curve_inv [n_curved]) of the
+        mesh file as the reference's MeshFile builds them (1-based, list order)."""
+        F = lib().or_mesh_lists(self.h, None, None, None, None, None)
+        pts, els = np.zeros((F, 3), np.int32), np.zeros((F, 3), np.int32)
+        mk, ce, ci = np.zeros(F, np.int32), np.zeros(max(n_curved, 1), np.int32), np.zeros(max(n_curved, 1), np.int32)
+        lib().or_mesh_lists(self.h, _p(pts, C.c_int), _p(els, C.c_int), _p(mk, C.c_int), _p(ce, C.c_int),
+                            _p(ci, C.c_int))
+        return pts, els, mk, ce[:n_curved], ci[:n_curved]
 
     def probe(self, e, xi, eta):
         out = np.zeros(4)

@@ -124,6 +124,11 @@ int     or_surface_integrals(void* h, int zone, double out[8]);
 /* Probe (Monitors.f90:740-830): the state at reference coordinates (xi, eta) of element e (0-based). */
 int     or_probe(void* h, int e, double xi, double eta, double out[4]);
 int     or_zone_edge_nodes(void* h, int zone, double* X);
+/* The mesh file's edge lists as computeFaces / mergeDividedFaces / computeElementOfEdges /
+ * computeFaceMarkers / computeCurvedEdges leave them (1-based, list order): points[F][3] (0 when a
+ * simple edge), elements[F][3] (0 unused), marker[F], curve_edge[n_curved], curve_inv[n_curved];
+ * any pointer may be NULL.  Returns F. */
+int     or_mesh_lists(void* h, int* points, int* elements, int* marker, int* curve_edge, int* curve_inv);
 void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                        int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,

@@ -134,6 +134,8 @@ struct Oracle {
   std::vector<double> av_mu;                          // element artificial viscosity of the current state
   std::vector<double> av_g_ext;                       // externally supplied indicator G (OR_IND_EXTERNAL)
   bool av_hold = false;                               // later RK stages: keep the modal / external viscosity
+  // the mesh file's lists as MeshFile builds them (1-based; exported for the library's builder tests)
+  std::vector<int> mf_points, mf_elements, mf_marker, mf_curve_edge, mf_curve_inv;
   int64_t ndof = 0;
   // EstimateTimeStep SAVE variables (DGTimeIntegrator.f90:471-473)
   double save_umax = 0.0, save_amax = 0.0;

@@ -105,3 +105,46 @@ def test_locate_points_for_probes(kind):
         assert abs(a - xi[i]) < 1e-10 and abs(b - xi[j]) < 1e-10
     with pytest.raises(ValueError):
         hmesh.locate(d, [[100.0, 100.0]], hg.NODES_LG)
+
+
+@pytest.mark.parametrize("name", ["VortexTransportBench", "VortexTransportCase", "CylinderBench", "RampBench",
+                                  "CouetteBench", "ShockWave"])
+def test_library_connectivity_matches_mesh_file_construction(name):
+    """hg_mesh_connectivity (O(E), C++ in the library) gives the lists of the reference's MeshFile
+    construction -- edge order and orientation, subdivided (hanging-node) edges, elements of each
+    edge, markers, curved-edge assignment and orientation -- as the oracle restates it, on every
+    reference mesh the tests carry (the VortexTransport meshes have hanging nodes, the cylinder
+    curved edges)."""
+    from cases_util import load_mesh
+    from oracle import oracle as O
+    m = load_mesh(name)
+    n_markers = int(np.max(m["bdry_marker"]))
+    orc = O.Oracle(m, 2, nodes=O.LG, riemann=O.ROE, mach=0.3, bcs=[dict(type=O.BC_EULERWALL)] * n_markers)
+    n_curved = int(np.asarray(m.get("curved_edges", np.zeros((0, 2)))).reshape(-1, 2).shape[0])
+    pts, els, mk, ce, ci = orc.mesh_lists(n_curved)
+    c = hmesh.connectivity(m)
+    np.testing.assert_array_equal(c["points_of_edges"], pts)
+    np.testing.assert_array_equal(c["elements_of_edges"], els)
+    np.testing.assert_array_equal(c["edge_marker"], mk)
+    np.testing.assert_array_equal(c["curved_edges"], ce)
+    np.testing.assert_array_equal(c["curve_inverted"], ci)
+    if name == "VortexTransportBench":
+        assert np.any(pts[:, 2] > 0)            # hanging nodes merged into subdivided edges
+
+
+def test_library_connectivity_scales_linearly():
+    """A 1024 x 1024 quad mesh (the Kelvin-Helmholtz workload's size) is connected in seconds."""
+    import time
+    n = 1024
+    ij = np.arange((n + 1) * (n + 1)).reshape(n + 1, n + 1) + 1
+    quads = np.stack([ij[:-1, :-1], ij[:-1, 1:], ij[1:, 1:], ij[1:, :-1]], -1).reshape(-1, 4)
+    sides = [np.stack([ij[0, :-1], ij[0, 1:]], 1), np.stack([ij[-1, :-1], ij[-1, 1:]], 1),
+             np.stack([ij[:-1, 0], ij[1:, 0]], 1), np.stack([ij[:-1, -1], ij[1:, -1]], 1)]
+    m = dict(points=np.zeros(((n + 1) ** 2, 2)), quads=quads, bdry_edges=np.concatenate(sides),
+             bdry_marker=np.repeat(np.arange(1, 5, dtype=np.int32), n))
+    t0 = time.perf_counter()
+    c = hmesh.connectivity(m)
+    el = time.perf_counter() - t0
+    assert len(c["edge_marker"]) == 2 * n * (n + 1) and int((c["edge_marker"] == 3).sum()) == n
+    assert np.all(c["elements_of_edges"][c["edge_marker"] == 0][:, 1] > 0)
+    assert el < 20.0
