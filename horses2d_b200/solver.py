@@ -146,6 +146,52 @@ class GpuDGSEM:
         self._check(self._lib.hg_estimate_dt(self._h, cfl, dt_cap, C.byref(d)))
         return d.value
 
+    def integrate(self, scheme, *, transient, t0, t_end, max_iter, cfl, dt_cap, residual_target=0.0,
+                  estimate_interval=100):
+        """The reference's integration loop (Approximation/DGTimeIntegrator.f90:173-242) around the
+        library's steps: dt from EstimateTimeStep, re-estimated every `estimate_interval` iterations;
+        transient mode clips the last step to end exactly at t_end; steady mode stops when the largest
+        residual falls below residual_target.  The host replays the loop's time arithmetic exactly and
+        issues runs of ordinary transient steps through the multi-step call.  Returns (iterations, t)."""
+        def same(a, b):   # the reference's almost-equal test of the final time
+            eps = np.finfo(float).eps
+            if a == 0.0 or b == 0.0:
+                return abs(a - b) <= 2.0 * eps
+            return abs(b - a) <= 2.0 * eps * max(abs(a), abs(b))
+
+        t = t0
+        dt = self.estimate_time_step(cfl, dt_cap)
+        pending, t_first = 0, t0      # ordinary steps of the current dt not yet issued
+
+        def flush():
+            nonlocal pending
+            if pending:
+                self.time_steps(scheme, pending, t_first, dt)
+                pending = 0
+
+        it = 0
+        for it in range(1, max_iter + 1):
+            if transient and t + dt >= t_end:
+                flush()
+                dt = t_end - t
+                self.time_step(scheme, t, dt)
+            elif transient:
+                if pending == 0:
+                    t_first = t
+                pending += 1
+            else:
+                self.time_step(scheme, t, dt)
+            t = t + dt
+            if transient and same(t, t_end):
+                break
+            if it % estimate_interval == 0:
+                flush()
+                dt = self.estimate_time_step(cfl, dt_cap)
+            if not transient and np.max(np.abs(self.residuals())) < residual_target:
+                break
+        flush()
+        return it, t
+
     # --- plumbing ----------------------------------------------------------
     def set_stream(self, cuda_stream_handle):
         self._check(self._lib.hg_set_stream(self._h, C.c_void_p(cuda_stream_handle)))
