@@ -702,7 +702,17 @@ extern "C" int hg_set_sensor(hg_ctx* c, int32_t kind, double s0, double kappa, c
       HG_CUDA(cudaMemcpy(d, h, n * sizeof(float), cudaMemcpyHostToDevice));
     };
     drop_graph(c);
-    put(c->d_mlp, mlp, HG_MLP_PARAMS);
+    // the device keeps the weights with the hidden unit fastest (W1^T, W2^T), the order in which the
+    // kernels' lanes read them; the caller's layout is the row-major one of hg_mlp_*
+    std::vector<float> wt;
+    if (mlp) {
+      wt.assign(mlp, mlp + HG_MLP_PARAMS);
+      for (int o = 0; o < MLP_H; ++o) {
+        for (int q = 0; q < MLP_IN; ++q) wt[MLP_W1 + q * MLP_H + o] = mlp[MLP_W1 + o * MLP_IN + q];
+        for (int q = 0; q < MLP_H; ++q) wt[MLP_W2 + q * MLP_H + o] = mlp[MLP_W2 + o * MLP_H + q];
+      }
+    }
+    put(c->d_mlp, mlp ? wt.data() : nullptr, HG_MLP_PARAMS);
     put(c->d_feat_lo, lo, HG_SENSOR_FEATURES);
     put(c->d_feat_hi, hi, HG_SENSOR_FEATURES);
     c->sensor_kind = kind;

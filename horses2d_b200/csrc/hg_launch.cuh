@@ -89,7 +89,6 @@ __global__ void __launch_bounds__(block_ns(P)) sensor_eval_kernel(int n_el, cons
   constexpr int NP = P * P;
   __shared__ real sQ[4][EPB][NP];
   __shared__ real sV[NP];
-  __shared__ real scr[EPB][sensor_scratch(P)];
   const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
   const int e = blockIdx.x * EPB + le;
   const bool active = le < EPB && e < n_el;
@@ -104,7 +103,8 @@ __global__ void __launch_bounds__(block_ns(P)) sensor_eval_kernel(int n_el, cons
   ph.load(pc);
   SensorArgs s2 = sa;
   if (sa.mlp) s2.kind = SENSOR_LEARNED;
-  SensorOut so = element_sensor<P, EPB, real>(s2, ph, sQ, scr[le < EPB ? le : 0], sV, le, tid, active,
+  const int n_active = n_el - int(blockIdx.x) * EPB < EPB ? n_el - int(blockIdx.x) * EPB : EPB;
+  SensorOut so = element_sensor<P, EPB, real>(s2, ph, sQ, n_active, sV, le, tid, active,
                                              (active && feat) ? feat + size_t(e) * MLP_IN : nullptr);
   if (active && tid == 0 && out) {
     const double g = sa.kind == SENSOR_LEARNED ? so.g : (sa.kind == SENSOR_MODAL ? so.g_modal : -1.0);

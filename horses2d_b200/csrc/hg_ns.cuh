@@ -70,21 +70,23 @@ __host__ __device__ constexpr int epb_ns_of(int P, int variant) { return variant
 __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) + 31) / 32) * 32; }
 
 // Shared tiles of one CTA.
-template <int P, int EPB, typename real, bool AFFINE>
+// ST: the stage kernel's tiles; the gradient kernel has no contravariant fluxes (Fc, Gc) and leaves
+// that shared memory to the shock sensor.
+template <int P, int EPB, typename real, bool AFFINE, bool ST = true>
 struct NSTiles {
   static constexpr int NP = P * P, FT = 4 * P;
   real mat[3 * NP + 7 * P];   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w Vinv
   real Q[4][EPB][NP];
   real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : NP];   // Ja00 Ja01 Ja10 Ja11 J
   real dQ[2][4][EPB][NP];
-  real Fc[4][EPB][NP];
-  real Gc[4][EPB][NP];
+  real Fc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
+  real Gc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
   real face[12][EPB][FT];   // BR1 u* dS n (8) / F* (4) + gradient-face contravariant fluxes (8)
   double red[32][4];
 };
 
-template <int P, int EPB, typename real, bool AFFINE>
-__device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE>& s, const real (*src)[EPB][P * P], int k,
+template <int P, int EPB, typename real, bool AFFINE, bool ST>
+__device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE, ST>& s, const real (*src)[EPB][P * P], int k,
                                          int le, int side, int kk, const real* lbv) {
   real t = real(0);
 #pragma unroll
@@ -111,8 +113,8 @@ __device__ __forceinline__ void trace4(const real (*src)[EPB][P * P], int le, in
 }
 
 // Element gradient into s.dQ (both kernels).  Requires s.Q (and s.Ja) filled and synchronized.
-template <int P, int EPB, typename real, bool AFFINE, bool IP>
-__device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+template <int P, int EPB, typename real, bool AFFINE, bool IP, bool ST>
+__device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE, ST>& s,
                                                  const Phys<real>& ph, int le, int tid, int e, bool active,
                                                  const real* geoE) {
   constexpr int NP = P * P, FT = 4 * P;
@@ -222,8 +224,8 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
   }
 }
 
-template <int P, int EPB, typename real, bool AFFINE>
-__device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s, int flat, int le,
+template <int P, int EPB, typename real, bool AFFINE, bool ST>
+__device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE, ST>& s, int flat, int le,
                                            int tid, int e, bool active, real* geoE) {
   constexpr int NP = P * P;
   for (int k = flat; k < 3 * NP + 7 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
@@ -250,17 +252,17 @@ __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB
 // Mesh/QuadElement_EdgeProcedures.incf:1348-1619): sum over the edge nodes, in the edge's order, of
 // w (2 (QL-QR)/(QL+QR))^2 dS for rho and rhoE; boundary and periodic edges use the viscous boundary
 // state (uSB) and dS at their first node.  Uses s.face[0..1] as scratch; ends with a barrier.
-template <int P, int EPB, typename real, bool AFFINE>
-__device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+template <int P, int EPB, typename real, bool AFFINE, bool ST>
+__device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE, ST>& s,
                                                   const Phys<real>& ph, int le, int tid, int e, bool active) {
   constexpr int NP = P * P, FT = 4 * P;
   if (a.sensor.kind != SENSOR_JUMPS) {   // modal-decay or learned indicator (hg_sensor.cuh)
     // evaluated on the first stage of a time step (and for a bare time derivative); the later stages
     // of the step keep that viscosity.  The reference's jumps indicator is re-evaluated every stage.
     if (!a.first) return;
-    __shared__ real s_scr[EPB][sensor_scratch(P)];
-    const SensorOut so = element_sensor<P, EPB, real>(a.sensor, ph, s.Q, s_scr[le < EPB ? le : 0],
-                                                      s.mat + 2 * NP + 7 * P, le, tid, active, nullptr);
+    const int n_active = a.n_el - int(blockIdx.x) * EPB < EPB ? a.n_el - int(blockIdx.x) * EPB : EPB;
+    const SensorOut so = element_sensor<P, EPB, real>(a.sensor, ph, s.Q, n_active, s.mat + 2 * NP + 7 * P, le,
+                                                      tid, active, nullptr);
     if (active && tid == 0) a.mu_av[e] = a.av_el[2 * size_t(e)] * so.g;
     __syncthreads();
     return;
@@ -331,7 +333,7 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
 template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
 __global__ void __launch_bounds__(block_of(P, EPB)) ns_gradient_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
-  __shared__ NSTiles<P, EPB, real, AFFINE> s;
+  __shared__ NSTiles<P, EPB, real, AFFINE, false> s;
   const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
   const int e = blockIdx.x * EPB + le;
   const bool active = le < EPB && e < a.n_el;

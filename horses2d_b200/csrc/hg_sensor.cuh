@@ -24,7 +24,7 @@ constexpr int MLP_W1 = 0, MLP_B1 = MLP_W1 + MLP_H * MLP_IN, MLP_W2 = MLP_B1 + ML
 struct SensorArgs {
   int kind;            // SENSOR_*
   double s0, kappa;    // modal ramp centre and half width
-  const float* mlp;    // [MLP_PARAMS] W1[32][16] b1 W2[32][32] b2 W3[32] b3
+  const float* mlp;    // [MLP_PARAMS] W1^T[16][32] b1 W2^T[32][32] b2 W3[32] b3 (hidden unit fastest)
   const float* lo;     // [16] feature box of the training set (with margin)
   const float* hi;     // [16]
 };
@@ -52,19 +52,29 @@ struct SensorOut {
 };
 
 // Modal indicator and (if asked) the learned one for element `le` of the CTA.  Q: the element tiles
-// [4][EPB][NP] in shared memory; scr: this element's scratch row of sensor_scratch(P) reals.  All
-// threads of the CTA call it (it holds barriers); results are valid in thread tid == 0 of each element.
+// [4][EPB][NP] in shared memory; n_active: elements of this CTA that exist.  All threads of the CTA call it (it holds barriers);
+// results are valid in thread tid == 0 of each element.
+//
+// Network inference: the weights (stored with the hidden unit fastest) are copied once per CTA into
+// shared memory, and each warp evaluates one element at a time with one lane per hidden unit: the
+// inputs are broadcast from the element's scratch row, the 32-input sums of the second layer run as
+// four interleaved partial sums, and the output unit is a warp shuffle tree.
 template <int P, int EPB, typename real>
 __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const Phys<real>& ph,
-                                                    const real (*Q)[EPB][P * P], real* scr, const real* Vinv,
-                                                    int le, int tid, bool active, float* feat_out) {
-  constexpr int NP = P * P, N = P - 1;
+                                                    const real (*Q)[EPB][P * P], int n_active,
+                                                    const real* Vinv, int le, int tid, bool active,
+                                                    float* feat_out) {
+  constexpr int NP = P * P, N = P - 1, SS = sensor_scratch(P);
+  // scratch rows of the CTA's elements, declared here so that every access is a shared-memory one
+  __shared__ real s_scr[EPB * SS];
+  real* const scr_all = s_scr;
+  real* scr = scr_all + (le < EPB ? le : 0) * SS;
   real* uh = scr;                 // [2][NP] modal coefficients of rho, p (k_eta * P + k_xi)
   real* en = scr + 2 * NP;        // [2][12]: Ex[4], Ey[4], E, EN, -, -
   real* ft = en + 24;             // [16] features
   real* h1 = ft + MLP_IN;         // [32]
   real* h2 = h1 + MLP_H;          // [32]
-  real* pn = h2 + MLP_H;          // [2] modal-decay indicators of rho and p
+  real* pn = h2 + MLP_H;          // [2] modal-decay indicators of rho and p, [2] learned G
   SensorOut out{0.0, 0.0, 0.0, 0};
   // nodal pressure into uh[NP..) as a staging area, then the transform in place per variable
   real pnode = real(0);
@@ -139,28 +149,32 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
     out.ood = ood;
   }
   if (sa.kind == SENSOR_LEARNED) {
+    static_assert(MLP_H == 32, "one lane per hidden unit");
+    __shared__ float s_w[MLP_PARAMS];   // W1^T[16][32] b1 W2^T[32][32] b2 W3 b3
+    for (int d = threadIdx.x; d < MLP_PARAMS; d += blockDim.x) s_w[d] = __ldg(sa.mlp + d);
     __syncthreads();
-    if (active)
-      for (int o = tid; o < MLP_H; o += NP) {
-        float z = __ldg(sa.mlp + MLP_B1 + o);
+    const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (int el = threadIdx.x >> 5; el < n_active; el += nw) {
+      real* r = scr_all + el * SS;
+      const real* f = r + 2 * NP + 24;
+      real* g1 = r + 2 * NP + 24 + MLP_IN;
+      float z = s_w[MLP_B1 + lane];
 #pragma unroll
-        for (int q = 0; q < MLP_IN; ++q) z += __ldg(sa.mlp + MLP_W1 + o * MLP_IN + q) * float(ft[q]);
-        h1[o] = real(tanhf(z));
-      }
-    __syncthreads();
-    if (active)
-      for (int o = tid; o < MLP_H; o += NP) {
-        float z = __ldg(sa.mlp + MLP_B2 + o);
-#pragma unroll 8
-        for (int q = 0; q < MLP_H; ++q) z += __ldg(sa.mlp + MLP_W2 + o * MLP_H + q) * float(h1[q]);
-        h2[o] = real(tanhf(z));
-      }
-    __syncthreads();
-    if (active && tid == 0) {
-      float z = __ldg(sa.mlp + MLP_B3);
-      for (int q = 0; q < MLP_H; ++q) z += __ldg(sa.mlp + MLP_W3 + q) * float(h2[q]);
-      out.g_learned = double(mlp_sigmoid(z));
+      for (int q = 0; q < MLP_IN; ++q) z += s_w[MLP_W1 + q * MLP_H + lane] * float(f[q]);
+      g1[lane] = real(tanhf(z));
+      __syncwarp();
+      float zp[4] = {s_w[MLP_B2 + lane], 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int q = 0; q < MLP_H; ++q) zp[q & 3] += s_w[MLP_W2 + q * MLP_H + lane] * float(g1[q]);
+      const float h = tanhf((zp[0] + zp[1]) + (zp[2] + zp[3]));
+      float y = s_w[MLP_W3 + lane] * h;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
+      if (lane == 0) r[2 * NP + 24 + MLP_IN + 2 * MLP_H + 2] = real(mlp_sigmoid(y + s_w[MLP_B3]));
+      __syncwarp();
     }
+    __syncthreads();
+    if (active && tid == 0) out.g_learned = double(pn[2]);
   }
   out.g = sa.kind == SENSOR_LEARNED ? (out.ood ? out.g_modal : out.g_learned) : out.g_modal;
   return out;
