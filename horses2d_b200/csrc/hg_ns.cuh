@@ -342,8 +342,12 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_gradient_kernel(NSArgs<re
   real geoE[5];
   load_tiles(a, s, flat, le, tid, e, active, geoE);
   __syncthreads();
-  element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
-  __syncthreads();
+  // the interior-penalty gradient is element-local: without viscous fluxes nothing here uses it (the
+  // launch then only evaluates the indicator); a.viscous is uniform over the launch
+  if (!IP || a.viscous) {
+    element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+    __syncthreads();
+  }
   if (AV) element_viscosity<P, EPB, real, AFFINE>(a, s, ph, le, tid, e, active);
   if (!active) return;
   if (!IP) {   // the lifted gradient is not local: store it for the stage kernel
