@@ -386,9 +386,13 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   real geoE[5];
   load_tiles(a, s, flat, le, tid, e, active, geoE);
   const real mu_e = (AV && active) ? real(a.mu_av[e]) : real(0);
+  const bool visc = a.viscous != 0;
+  // the element gradient feeds the viscous fluxes and the Laplacian dissipation's volume term; an
+  // element without either (mu_e = 0: that term is exactly zero) skips it
+  const bool need_grad = visc || (AV && a.av == 1 && mu_e != real(0));
   if (IP) {   // the interior-penalty gradient is element-local: recompute it here
     __syncthreads();
-    element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+    element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active && need_grad, geoE);
   } else if (active) {
     const real* g = a.dQ + size_t(e) * 8 * NP + tid;
 #pragma unroll
@@ -397,7 +401,6 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       for (int k = 0; k < 4; ++k) s.dQ[d][k][le][tid] = g[(d * 4 + k) * NP];
   }
   __syncthreads();
-  const bool visc = a.viscous != 0;
   const int i = tid % P, j = tid / P;
   const real* hatD = s.mat;
   const real* lb0 = s.mat + NP;
@@ -422,7 +425,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     }
     const real mu_v = (AV && a.av == 2) ? mu + mu_e : mu;
     real ax[4] = {real(0), real(0), real(0), real(0)}, ay[4] = {real(0), real(0), real(0), real(0)};
-    if (AV && a.av == 1) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
+    if (AV && a.av == 1 && need_grad) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
       if (IP) {
 #pragma unroll
         for (int k = 0; k < 4; ++k) { ax[k] = gx[k]; ay[k] = gy[k]; }
