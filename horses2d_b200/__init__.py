@@ -7,6 +7,7 @@ CUDA sources (``csrc/``), the Python mirror of the reference interface
 (``solver.GpuDGSEM``) and host-side mesh builders (``mesh``).
 """
 from . import _lib as lib  # noqa: F401
+from . import restart  # noqa: F401
 from .solver import GpuDGSEM, GpuGroup, HorsesGpuError  # noqa: F401
 from ._lib import (NODES_LG, NODES_LGL, ROE, HLL, EXACT, LXF, INTERIOR, SCHEME_EULER, SCHEME_RK3,  # noqa: F401
                    SCHEME_RK5, PREC_FP64, PREC_FP32, BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL,

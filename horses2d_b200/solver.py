@@ -21,10 +21,12 @@ Errors raise ``HorsesGpuError`` carrying the library's message (the reference
 stops the program instead).
 """
 import ctypes as C
+import os
 
 import numpy as np
 
 from . import _lib as L
+from . import restart
 
 
 class HorsesGpuError(RuntimeError):
@@ -147,12 +149,15 @@ class GpuDGSEM:
         return d.value
 
     def integrate(self, scheme, *, transient, t0, t_end, max_iter, cfl, dt_cap, residual_target=0.0,
-                  estimate_interval=100):
-        """The reference's integration loop (Approximation/DGTimeIntegrator.f90:173-242) around the
+                  estimate_interval=100, initial_iteration=0, autosave_interval=0, solution_file=None):
+        """The reference's integration loop (Approximation/DGTimeIntegrator.f90:173-247) around the
         library's steps: dt from EstimateTimeStep, re-estimated every `estimate_interval` iterations;
         transient mode clips the last step to end exactly at t_end; steady mode stops when the largest
         residual falls below residual_target.  The host replays the loop's time arithmetic exactly and
-        issues runs of ordinary transient steps through the multi-step call.  Returns (iterations, t)."""
+        issues runs of ordinary transient steps through the multi-step call.  Iterations are numbered
+        from initial_iteration + 1 (the iteration a restart file holds); with autosave_interval > 0 a
+        restart file named after solution_file is written every that many iterations, and with a
+        solution_file the final state is saved there.  Returns (last iteration, t)."""
         def same(a, b):   # the reference's almost-equal test of the final time
             eps = np.finfo(float).eps
             if a == 0.0 or b == 0.0:
@@ -169,8 +174,8 @@ class GpuDGSEM:
                 self.time_steps(scheme, pending, t_first, dt)
                 pending = 0
 
-        it = 0
-        for it in range(1, max_iter + 1):
+        it = initial_iteration
+        for it in range(initial_iteration + 1, initial_iteration + max_iter + 1):
             if transient and t + dt >= t_end:
                 flush()
                 dt = t_end - t
@@ -184,13 +189,31 @@ class GpuDGSEM:
             t = t + dt
             if transient and same(t, t_end):
                 break
+            if autosave_interval > 0 and solution_file and it % autosave_interval == 0:
+                flush()
+                self.save_restart(restart.autosave_name(solution_file, it), t, it)
             if it % estimate_interval == 0:
                 flush()
                 dt = self.estimate_time_step(cfl, dt_cap)
             if not transient and np.max(np.abs(self.residuals())) < residual_target:
                 break
         flush()
+        if solution_file:
+            self.save_restart(solution_file, t, it)
         return it, t
+
+    # --- restart files (*.HiORst) --------------------------------------------
+    def save_restart(self, path, t, iteration):
+        """The resident state, t and iter to a restart file (TimeIntegrator_Autosave)."""
+        if self._lib.hg_save_restart(self._h, os.fsencode(path), float(t), int(iteration)) != 0:
+            raise OSError(self._lib.hg_restart_last_error().decode())
+
+    def load_restart(self, path):
+        """A restart file into the resident state (DGSEM_loadRestartFile); returns (t, iter)."""
+        t, it = C.c_double(0.0), C.c_int32(0)
+        if self._lib.hg_load_restart(self._h, os.fsencode(path), C.byref(t), C.byref(it)) != 0:
+            raise OSError(self._lib.hg_restart_last_error().decode())
+        return t.value, it.value
 
     # --- plumbing ----------------------------------------------------------
     def set_stream(self, cuda_stream_handle):

@@ -260,6 +260,22 @@ int  hg_mesh_connectivity(int32_t n_points, int32_t n_elements, const int32_t* p
                           int32_t* n_edges, int32_t* points_of_edges, int32_t* elements_of_edges,
                           int32_t* edge_marker, int32_t* curved_edges, int32_t* curve_inverted);
 const char* hg_mesh_last_error(void);
+/* Restart files (*.HiORst), host code without a NetCDF library; they replace the reference's
+ * TimeIntegrator_Autosave (Solver/src/Approximation/DGTimeIntegrator.f90:413-454, called every
+ * `Autosave interval` iterations and at the end, :216-218, :247) and DGSEM_loadRestartFile
+ * (Solver/src/Approximation/DGSEM_class.f90:263-291, IC "Restart").  The file is NetCDF classic
+ * (CDF-1) with dimensions one=1, NDOF, N, NCONS=4, no_of_elements and variables double t(one),
+ * double Q(NDOF), int iter(one), laid out as the reference writes it (files written here are
+ * byte-identical to the reference's for the same values); the reader accepts any classic file
+ * (CDF-1 or CDF-2) that holds t, Q and iter.  Q is Storage%Q: the state layout of hg_set_state.
+ * hg_read_restart with Q == NULL only reports the sizes (*ndof).  Errors: hg_restart_last_error(). */
+int  hg_write_restart(const char* path, double t, int32_t iter, const double* Q, int64_t ndof, int32_t N,
+                      int32_t n_elements);
+int  hg_read_restart(const char* path, double* t, int32_t* iter, double* Q, int64_t capacity, int64_t* ndof);
+/* The context's resident state to a restart file, and a restart file into the context (sizes must match). */
+int  hg_save_restart(hg_ctx* ctx, const char* path, double t, int32_t iter);
+int  hg_load_restart(hg_ctx* ctx, const char* path, double* t, int32_t* iter);
+const char* hg_restart_last_error(void);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N
  * (NodesAndWeightsClass.f90:251-332 computeNodesAndWeights).  xi, w: N+1 doubles. */
 int  hg_nodes(int32_t N, int32_t node_type, double* xi, double* w);
