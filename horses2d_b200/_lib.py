@@ -42,7 +42,9 @@ class MeshDesc(C.Structure):
     _fields_ = [("n_elements", C.c_int32), ("n_edges", C.c_int32), ("N", I32P), ("Ja", F64P), ("jac", F64P),
                 ("x", F64P), ("volume", F64P), ("vertices", F64P), ("edge_elem", I32P), ("edge_side", I32P),
                 ("edge_inverse", I32P), ("edge_marker", I32P), ("edge_n", F64P), ("edge_dS", F64P),
-                ("periodic_partner", I32P), ("edge_invh", F64P)]
+                ("periodic_partner", I32P), ("edge_invh", F64P), ("n_mortars", C.c_int32),
+                ("mortar_elem", I32P), ("mortar_side", I32P), ("mortar_flip", I32P), ("mortar_n", F64P),
+                ("mortar_dS", F64P)]
 
 
 _lib = None
@@ -58,7 +60,7 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
-KERNEL_KINDS = ("stage", "gradient", "trace", "reduce", "speed", "face_flux")
+KERNEL_KINDS = ("stage", "gradient", "trace", "reduce", "speed", "face_flux", "mortar")
 TILINGS = 2
 
 

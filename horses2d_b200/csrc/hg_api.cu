@@ -36,14 +36,15 @@ static void drop_graph(hg_ctx* c) {
   ++c->gen;
 }
 
-static void free_ctx(hg_ctx* c) {
+void ctx_free(hg_ctx* c) {
   if (!c) return;
+  composite_free(c);
   drop_graph(c);
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
                   c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
-                  c->d_FX, c->d_bq, c->d_si_out};
+                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF};
   for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -75,8 +76,26 @@ static int max_grid(const hg_ctx* c) {
     default: throw std::runtime_error("unsupported polynomial order"); \
   }
 
+// Euler kernels: orders 1-12
+#define HG_DISPATCH_P_EULER(P_, FN, ...)                \
+  switch (P_) {                                         \
+    case 2: FN<2, real>(__VA_ARGS__); break;            \
+    case 3: FN<3, real>(__VA_ARGS__); break;            \
+    case 4: FN<4, real>(__VA_ARGS__); break;            \
+    case 5: FN<5, real>(__VA_ARGS__); break;            \
+    case 6: FN<6, real>(__VA_ARGS__); break;            \
+    case 7: FN<7, real>(__VA_ARGS__); break;            \
+    case 8: FN<8, real>(__VA_ARGS__); break;            \
+    case 9: FN<9, real>(__VA_ARGS__); break;            \
+    case 10: FN<10, real>(__VA_ARGS__); break;          \
+    case 11: FN<11, real>(__VA_ARGS__); break;          \
+    case 12: FN<12, real>(__VA_ARGS__); break;          \
+    case 13: FN<13, real>(__VA_ARGS__); break;          \
+    default: throw std::runtime_error("unsupported polynomial order"); \
+  }
+
 template <typename real>
-static void run_trace(hg_ctx* c) { HG_DISPATCH_P(c->P, launch_trace_P, c); }
+static void run_trace(hg_ctx* c) { HG_DISPATCH_P_EULER(c->P, launch_trace_P, c); }
 
 template <int P, typename real>
 static void ns_dispatch(hg_ctx* c, const NSArgs<real>& a) {
@@ -147,6 +166,7 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.zones = c->d_zones;
   a.bq = c->d_bq;
   a.FX = static_cast<const real*>(c->d_FX);
+  a.NF = static_cast<const real*>(c->d_NF);
   a.Q = c->d_Q;
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
@@ -159,12 +179,26 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.riemann = c->riemann;
   a.pc = c->pc;
   if (c->exact) launch_exact_flux<real>(c);
-  HG_DISPATCH_P(c->P, stage_dispatch, c, a);
+  HG_DISPATCH_P_EULER(c->P, stage_dispatch, c, a);
   c->last_T = c->cur;   // trace buffer of the state this stage evaluated (surface integrals read it)
   if (update) c->cur ^= 1;
 }
 
-static void stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
+  if (is_composite(c)) {
+    // faces between orders and subdivided edges first, then every part's fused stage; the parts'
+    // launches are counted on the composite
+    launch_mortar(c);
+    for (hg_ctx* p : c->parts) {
+      const int64_t l0 = p->launches;
+      ctx_stage(p, ca, cb, cc, first, update, qdot ? p->d_QDot : nullptr, resid);
+      c->launches += p->launches - l0;
+      p->launches = l0;
+    }
+    c->last_T = c->cur;
+    if (update) c->cur ^= 1;
+    return;
+  }
   if (c->precision == HG_PREC_FP32) run_stage<float>(c, ca, cb, cc, first, update, qdot, resid);
   else run_stage<double>(c, ca, cb, cc, first, update, qdot, resid);
 }
@@ -178,18 +212,18 @@ static void traces(hg_ctx* c) {
 static void one_step(hg_ctx* c, int scheme, double t, double dt) {
   (void)t;
   if (scheme == HG_SCHEME_EULER) {
-    stage(c, 0.0, dt, 1.0, true, true, nullptr, true);
+    ctx_stage(c, 0.0, dt, 1.0, true, true, nullptr, true);
   } else if (scheme == HG_SCHEME_RK3) {
     const double am[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
     const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
     for (int m = 0; m < 3; ++m) {
-      stage(c, am[m], 1.0, gm[m] * dt, m == 0, true, nullptr, m == 2);
+      ctx_stage(c, am[m], 1.0, gm[m] * dt, m == 0, true, nullptr, m == 2);
     }
   } else if (scheme == HG_SCHEME_RK5) {
     const double am[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
     const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
     for (int m = 0; m < 5; ++m) {
-      stage(c, am[m], dt, gm[m], m == 0, true, nullptr, m == 4);
+      ctx_stage(c, am[m], dt, gm[m], m == 0, true, nullptr, m == 4);
     }
   } else {
     throw std::runtime_error("unknown time scheme");
@@ -213,7 +247,8 @@ __global__ void element_speed_kernel(int n_el, int NP, const double* Q, double g
 }
 
 // ------------------------------------------------------------------ creation
-static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
+void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs,
+               const std::vector<int2>* flux_sides) {
   if (!m || !ph) throw std::runtime_error("null descriptor");
   int dev = 0;
   HG_CUDA(cudaGetDevice(&dev));
@@ -225,7 +260,10 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
   const int N = m->N[0];
   for (int e = 0; e < E; ++e)
     if (m->N[e] != N) throw std::runtime_error("mixed polynomial orders are not supported by this kernel set");
-  if (N < 1 || N > 8) throw std::runtime_error("polynomial order must be in 1..8");
+  if (ph->navier_stokes ? (N < 1 || N > 8) : (N < 1 || N > HG_MAX_ORDER_EULER))
+    throw std::runtime_error(ph->navier_stokes ? "polynomial order must be in 1..8 for the Navier-Stokes build"
+                                               : "polynomial order must be in 1..12");
+  if (m->n_mortars > 0) throw std::runtime_error("subdivided edges need the composite context");
   const int P = N + 1, NP = P * P;
   // the Navier-Stokes build with Re = 0 has mu = 0: its viscous terms vanish identically
   if (ph->av_type < HG_AV_NONE || ph->av_type > HG_AV_PHYSICAL) throw std::runtime_error("unknown artificial dissipation type");
@@ -349,6 +387,11 @@ static void build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, c
       if (m->edge_invh) sinvh[size_t(L) * 4 + sL] = m->edge_invh[f];
     }
   }
+  if (flux_sides)
+    for (const int2& fs : *flux_sides) {
+      if (fs.x < 0 || size_t(fs.x) >= side.size() || side[fs.x].x != -2) throw std::runtime_error("bad mortar side");
+      side[fs.x] = make_int4(fs.y, SIDE_FLUX, -1, -1);
+    }
   for (size_t s = 0; s < side.size(); ++s)
     if (side[s].x == -2) throw std::runtime_error("element side not covered by any edge");
 
@@ -473,10 +516,14 @@ extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, 
   c->precision = precision;
   try {
     if (precision != HG_PREC_FP64 && precision != HG_PREC_FP32) throw std::runtime_error("unknown precision");
-    build(c, mesh, phys, bcs, n_bcs);
+    if (!mesh || !phys) throw std::runtime_error("null descriptor");
+    bool mixed = mesh->n_mortars > 0;
+    for (int e = 1; e < mesh->n_elements && !mixed; ++e) mixed = mesh->N[e] != mesh->N[0];
+    if (mixed) composite_build(c, mesh, phys, bcs, n_bcs);
+    else ctx_build(c, mesh, phys, bcs, n_bcs, nullptr);
   } catch (const std::exception& ex) {
     g_create_err = ex.what();
-    free_ctx(c);
+    ctx_free(c);
     delete c;
     return 1;
   }
@@ -488,14 +535,72 @@ extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, 
 extern "C" void hg_destroy(hg_ctx* c) {
   if (!c) return;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  free_ctx(c);
+  ctx_free(c);
   delete c;
 }
 
 extern "C" const char* hg_last_error(const hg_ctx* c) { return c ? c->err.c_str() : g_create_err.c_str(); }
 extern "C" int64_t hg_ndof(const hg_ctx* c) { return c ? c->ndof : -1; }
-extern "C" double* hg_device_state(hg_ctx* c) { return c ? c->d_Q : nullptr; }
+extern "C" double* hg_device_state(hg_ctx* c) { return c ? c->d_Q : nullptr; }   // NULL for a composite
 extern "C" int64_t hg_launch_count(const hg_ctx* c) { return c ? c->launches : -1; }
+
+// ------------------------------------------------------------------ composite contexts
+// A mesh with mixed orders or subdivided edges is served by one part per order (hg_mortar.cu); the
+// entry points below scatter Storage%Q to the parts, gather from them, and combine their results.
+#define HG_PART(call, p)                                             \
+  do {                                                               \
+    if ((call) != 0) throw std::runtime_error((p)->err);             \
+  } while (0)
+
+static double nanmax_h(double m, double v) { return (v > m || v != v) ? v : m; }
+
+// a non-null QDot target: a composite's parts write their own buffers
+static double* qdot_target(hg_ctx* c) { return is_composite(c) ? c->parts[0]->d_QDot : c->d_QDot; }
+
+static void composite_scatter(hg_ctx* c, const double* Q) {
+  for (size_t pi = 0; pi < c->parts.size(); ++pi) {
+    hg_ctx* p = c->parts[pi];
+    const size_t n = size_t(p->P) * p->P * 4;
+    std::vector<double> q(p->ndof);
+    for (int e = 0; e < c->n_el; ++e)
+      if (c->el_part[e] == int(pi))
+        std::copy(Q + c->el_offset[e], Q + c->el_offset[e] + n, q.begin() + size_t(c->el_local[e]) * n);
+    HG_PART(hg_set_state(p, q.data(), p->ndof), p);
+  }
+}
+
+static void composite_gather(hg_ctx* c, double* Q, bool qdot) {
+  for (size_t pi = 0; pi < c->parts.size(); ++pi) {
+    hg_ctx* p = c->parts[pi];
+    const size_t n = size_t(p->P) * p->P * 4;
+    std::vector<double> q(p->ndof);
+    HG_CUDA(cudaMemcpyAsync(q.data(), qdot ? p->d_QDot : p->d_Q, p->ndof * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    for (int e = 0; e < c->n_el; ++e)
+      if (c->el_part[e] == int(pi))
+        std::copy(q.begin() + size_t(c->el_local[e]) * n, q.begin() + size_t(c->el_local[e] + 1) * n, Q + c->el_offset[e]);
+  }
+}
+
+static void composite_residuals(hg_ctx* c, double out[4]) {
+  for (int k = 0; k < 4; ++k) out[k] = 0.0;
+  for (hg_ctx* p : c->parts) {
+    double r[4];
+    const int64_t l0 = p->launches;
+    HG_PART(hg_residuals(p, r), p);
+    c->launches += p->launches - l0;
+    p->launches = l0;
+    for (int k = 0; k < 4; ++k) out[k] = nanmax_h(out[k], r[k]);
+  }
+}
+
+static int largest_part(const hg_ctx* c) {
+  int b = 0;
+  for (size_t p = 1; p < c->parts.size(); ++p)
+    if (c->parts[p]->n_el > c->parts[b]->n_el) b = int(p);
+  return b;
+}
 
 static void check_ndof(hg_ctx* c, int64_t ndof) {
   if (ndof != c->ndof) throw std::runtime_error("ndof mismatch: expected " + std::to_string(c->ndof));
@@ -503,6 +608,13 @@ static void check_ndof(hg_ctx* c, int64_t ndof) {
 
 extern "C" int hg_set_state(hg_ctx* c, const double* Q, int64_t ndof) {
   try {
+    if (is_composite(c)) {
+      check_ndof(c, ndof);
+      composite_scatter(c, Q);
+      c->cur = 0;
+      c->state_set = true;
+      return 0;
+    }
     check_ndof(c, ndof);
     HG_CUDA(cudaMemcpyAsync(c->d_Q, Q, ndof * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     c->cur = 0;
@@ -515,6 +627,11 @@ extern "C" int hg_set_state(hg_ctx* c, const double* Q, int64_t ndof) {
 
 extern "C" int hg_get_state(hg_ctx* c, double* Q, int64_t ndof) {
   try {
+    if (is_composite(c)) {
+      check_ndof(c, ndof);
+      composite_gather(c, Q, false);
+      return 0;
+    }
     check_ndof(c, ndof);
     HG_CUDA(cudaMemcpyAsync(Q, c->d_Q, ndof * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
@@ -530,9 +647,11 @@ extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
   try {
     require_state(c);
     (void)t;
-    stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, true);
+    ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), true);
     HG_CUDA(cudaGetLastError());
-    if (QDot) {
+    if (QDot && is_composite(c)) {
+      composite_gather(c, QDot, true);
+    } else if (QDot) {
       HG_CUDA(cudaMemcpyAsync(QDot, c->d_QDot, c->ndof * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
       HG_CUDA(cudaStreamSynchronize(c->stream));
     }
@@ -609,6 +728,10 @@ extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double 
 
 extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
   try {
+    if (is_composite(c)) {
+      composite_residuals(c, out);
+      return 0;
+    }
     timed(c, HG_KERNEL_REDUCE,
           [&] { residual_reduce_kernel<<<1, 256, 0, c->stream>>>(grid_for(c), c->d_resid, c->d_resid_out); });
     ++c->launches;
@@ -623,6 +746,32 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
   try {
     require_state(c);
     const int threads = 256;
+    if (is_composite(c)) {
+      // per-element maxima from every part, then the running maxima over the mesh's element order
+      std::vector<std::vector<double>> em(c->parts.size());
+      for (size_t pi = 0; pi < c->parts.size(); ++pi) {
+        hg_ctx* p = c->parts[pi];
+        timed(c, HG_KERNEL_SPEED, [&] {
+          element_speed_kernel<<<(p->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
+              p->n_el, p->P * p->P, p->d_Q, c->gamma, c->gamma - 1.0, p->d_elmax);
+        });
+        ++c->launches;
+        HG_CUDA(cudaGetLastError());
+        em[pi].resize(size_t(p->n_el) * 2);
+        HG_CUDA(cudaMemcpyAsync(em[pi].data(), p->d_elmax, em[pi].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+      }
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+      double d = dt_cap;
+      for (int e = 0; e < c->n_el; ++e) {
+        const double* v = &em[c->el_part[e]][2 * size_t(c->el_local[e])];
+        c->save_umax = std::fmax(c->save_umax, v[0]);
+        c->save_amax = std::fmax(c->save_amax, v[1]);
+        d = std::fmin(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->el_N[e] + 1));
+      }
+      *dt = d;
+      return 0;
+    }
     timed(c, HG_KERNEL_SPEED, [&] {
       element_speed_kernel<<<(c->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
           c->n_el, c->P * c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
@@ -650,6 +799,7 @@ extern "C" int hg_set_stream(hg_ctx* c, void* s) {
     if (c->own_stream) HG_CUDA(cudaStreamDestroy(c->stream));
     c->own_stream = false;
     c->stream = static_cast<cudaStream_t>(s);
+    for (hg_ctx* p : c->parts) p->stream = c->stream;
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -669,6 +819,7 @@ extern "C" int hg_profile(hg_ctx* c, int32_t enable) {
       for (int k = 0; k < HG_KERNEL_KINDS; ++k) { c->prof_ms[k] = 0.0; c->prof_n[k] = 0; }
     }
     c->prof = enable != 0;
+    for (hg_ctx* p : c->parts) HG_PART(hg_profile(p, enable), p);
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -676,9 +827,13 @@ extern "C" int hg_profile(hg_ctx* c, int32_t enable) {
 extern "C" int hg_kernel_times(hg_ctx* c, double* ms, int64_t* launches, int32_t n) {
   try {
     prof_collect(c);
+    for (hg_ctx* p : c->parts) prof_collect(p);
     for (int k = 0; k < n && k < HG_KERNEL_KINDS; ++k) {
-      if (ms) ms[k] = c->prof_ms[k];
-      if (launches) launches[k] = c->prof_n[k];
+      double t = c->prof_ms[k];
+      int64_t m = c->prof_n[k];
+      for (hg_ctx* p : c->parts) { t += p->prof_ms[k]; m += p->prof_n[k]; }
+      if (ms) ms[k] = t;
+      if (launches) launches[k] = m;
     }
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
@@ -687,6 +842,7 @@ extern "C" int hg_kernel_times(hg_ctx* c, double* ms, int64_t* launches, int32_t
 extern "C" int hg_set_sensor(hg_ctx* c, int32_t kind, double s0, double kappa, const float* mlp, const float* lo,
                              const float* hi) {
   try {
+    if (is_composite(c)) throw std::runtime_error("shock sensors need a single-order mesh");
     if (kind < HG_SENSOR_JUMPS || kind > HG_SENSOR_LEARNED) throw std::runtime_error("unknown sensor kind");
     if (kind == HG_SENSOR_LEARNED && !mlp) throw std::runtime_error("the learned sensor needs its weights");
     if ((lo == nullptr) != (hi == nullptr)) throw std::runtime_error("feature box needs both bounds");
@@ -725,6 +881,7 @@ static void sensor_eval_dispatch(hg_ctx* c, float* f, double* o) { launch_sensor
 
 extern "C" int hg_sensor_eval(hg_ctx* c, float* features, double* out) {
   try {
+    if (is_composite(c)) throw std::runtime_error("shock sensors need a single-order mesh");
     require_state(c);
     float* df = features ? dalloc<float>(size_t(c->n_el) * HG_SENSOR_FEATURES) : nullptr;
     double* dout = out ? dalloc<double>(size_t(c->n_el) * 4) : nullptr;
@@ -764,6 +921,27 @@ extern "C" int hg_element_viscosity(hg_ctx* c, double* mu) {
 
 extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, int64_t n_values) {
   try {
+    if (is_composite(c)) {
+      if (zone < 1 || zone > int(c->zone_type.size()) || c->zone_type[zone - 1] < 0)
+        throw std::runtime_error("unknown zone " + std::to_string(zone));
+      const std::vector<int>& ep = c->zone_edge_part[zone - 1];
+      int64_t expect = 0;
+      for (int p : ep) expect += int64_t(c->parts[p]->P) * 4;
+      if (!uB || n_values != expect)
+        throw std::runtime_error("zone " + std::to_string(zone) + " takes " + std::to_string(expect) + " values");
+      // the zone's edges in mesh order, each with its part's nodes: split into the parts' own lists
+      std::vector<std::vector<double>> buf(c->parts.size());
+      int64_t at = 0;
+      for (int p : ep) {
+        const int64_t n = int64_t(c->parts[p]->P) * 4;
+        buf[p].insert(buf[p].end(), uB + at, uB + at + n);
+        at += n;
+      }
+      for (size_t p = 0; p < c->parts.size(); ++p)
+        if (!buf[p].empty()) HG_PART(hg_set_boundary_state(c->parts[p], zone, buf[p].data(), int64_t(buf[p].size())), c->parts[p]);
+      drop_graph(c);
+      return 0;
+    }
     if (zone < 1 || zone > int(c->zone_type.size()) || c->zone_type[zone - 1] < 0)
       throw std::runtime_error("unknown zone " + std::to_string(zone));
     const int z = zone - 1;
@@ -799,6 +977,17 @@ extern "C" int hg_set_boundary_state(hg_ctx* c, int32_t zone, const double* uB, 
 // ------------------------------------------------------------------ surface integrals
 extern "C" int hg_surface_integrals(hg_ctx* c, int32_t zone, double out[8]) {
   try {
+    if (is_composite(c)) {
+      require_state(c);
+      if (!out) throw std::runtime_error("null output");
+      for (int k = 0; k < 8; ++k) out[k] = 0.0;
+      for (hg_ctx* p : c->parts) {
+        double o[8];
+        HG_PART(hg_surface_integrals(p, zone, o), p);
+        for (int k = 0; k < 8; ++k) out[k] += o[k];
+      }
+      return 0;
+    }
     require_state(c);
     if (!out) throw std::runtime_error("null output");
     if (zone < 1 || zone > int(c->zone_type.size()) || c->zone_type[zone - 1] < 0)
@@ -829,6 +1018,29 @@ extern "C" int hg_probes(hg_ctx* c, int32_t n, const int32_t* elements, const do
   double* d_x = nullptr;
   double* d_o = nullptr;
   try {
+    if (is_composite(c)) {
+      require_state(c);
+      if (n < 0 || (n > 0 && (!elements || !xi_eta || !out))) throw std::runtime_error("bad probe arguments");
+      for (int k = 0; k < n; ++k)
+        if (elements[k] < 0 || elements[k] >= c->n_el) throw std::runtime_error("probe element out of range");
+      for (size_t pi = 0; pi < c->parts.size(); ++pi) {
+        std::vector<int32_t> idx, le;
+        std::vector<double> xe;
+        for (int k = 0; k < n; ++k)
+          if (c->el_part[elements[k]] == int(pi)) {
+            idx.push_back(k);
+            le.push_back(c->el_local[elements[k]]);
+            xe.push_back(xi_eta[2 * k]);
+            xe.push_back(xi_eta[2 * k + 1]);
+          }
+        if (idx.empty()) continue;
+        std::vector<double> o(idx.size() * 4);
+        HG_PART(hg_probes(c->parts[pi], int32_t(idx.size()), le.data(), xe.data(), o.data()), c->parts[pi]);
+        for (size_t k = 0; k < idx.size(); ++k)
+          for (int q = 0; q < 4; ++q) out[4 * size_t(idx[k]) + q] = o[4 * k + q];
+      }
+      return 0;
+    }
     require_state(c);
     if (n < 0 || (n > 0 && (!elements || !xi_eta || !out))) throw std::runtime_error("bad probe arguments");
     for (int k = 0; k < n; ++k) {
@@ -901,6 +1113,7 @@ extern "C" int hg_group_create(hg_ctx* const* ctxs, int32_t n, hg_group** out) {
     if (!ctxs || n < 1) throw std::runtime_error("a group needs at least one context");
     for (int i = 0; i < n; ++i) {
       if (!ctxs[i]) throw std::runtime_error("null context in group");
+      if (is_composite(ctxs[i])) throw std::runtime_error("a mixed-order context cannot join a group");
       if (ctxs[i]->stream != ctxs[0]->stream) throw std::runtime_error("group members must share one stream");
       for (int j = 0; j < i; ++j) if (ctxs[j] == ctxs[i]) throw std::runtime_error("context listed twice");
       g->m.push_back(ctxs[i]);
@@ -1015,6 +1228,12 @@ extern "C" int hg_group_time_steps(hg_group* g, int32_t scheme, int32_t n_steps,
 // ------------------------------------------------------------------ elements-per-CTA autotuner
 extern "C" int hg_set_tiling(hg_ctx* c, int32_t variant) {
   try {
+    if (is_composite(c)) {
+      for (hg_ctx* p : c->parts) HG_PART(hg_set_tiling(p, variant), p);
+      drop_graph(c);
+      c->tiling = variant;
+      return 0;
+    }
     if (variant < 0 || variant >= HG_TILINGS) throw std::runtime_error("unknown tiling variant");
     HG_CUDA(cudaStreamSynchronize(c->stream));
     if (variant != c->tiling) drop_graph(c);
@@ -1025,6 +1244,7 @@ extern "C" int hg_set_tiling(hg_ctx* c, int32_t variant) {
 
 extern "C" int hg_get_tiling(const hg_ctx* c, int32_t out[3]) {
   if (!c || !out) return 1;
+  if (is_composite(c)) return hg_get_tiling(c->parts[largest_part(c)], out);
   const int epb = epb_of(c, c->tiling);
   out[0] = c->tiling;
   out[1] = epb;
@@ -1039,6 +1259,31 @@ extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* m
   try {
     require_state(c);
     if (trials < 1) throw std::runtime_error("autotune needs at least one trial");
+    if (is_composite(c)) {
+      // each part by itself (its mortar sides read the last mortar fluxes); reported: the largest
+      // part's choice and the per-variant times summed over the parts
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+      drop_graph(c);
+      double sum[HG_TILINGS] = {};
+      int chosen_big = 0;
+      for (size_t pi = 0; pi < c->parts.size(); ++pi) {
+        hg_ctx* p = c->parts[pi];
+        int32_t ch = 0;
+        double ms[HG_TILINGS] = {};
+        const int64_t l0 = p->launches;
+        HG_PART(hg_autotune(p, trials, &ch, ms), p);
+        p->launches = l0;
+        for (int v = 0; v < HG_TILINGS; ++v) sum[v] += ms[v];
+        if (int(pi) == largest_part(c)) chosen_big = ch;
+      }
+      // residual partials of the resident state through the full composite stage
+      ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), true);
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+      if (chosen) *chosen = chosen_big;
+      if (ms_per_variant)
+        for (int v = 0; v < HG_TILINGS; ++v) ms_per_variant[v] = sum[v];
+      return 0;
+    }
     HG_CUDA(cudaStreamSynchronize(c->stream));
     drop_graph(c);
     c->prof = false;
@@ -1049,9 +1294,9 @@ extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* m
     for (int v = 0; v < HG_TILINGS; ++v) {
       c->tiling = v;
       // residual launches of the resident state (no update): the stage's full arithmetic and loads
-      for (int w = 0; w < 2; ++w) stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, false);
+      for (int w = 0; w < 2; ++w) ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
       HG_CUDA(cudaEventRecord(ev[0], c->stream));
-      for (int k = 0; k < trials; ++k) stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, false);
+      for (int k = 0; k < trials; ++k) ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
       HG_CUDA(cudaEventRecord(ev[1], c->stream));
       HG_CUDA(cudaEventSynchronize(ev[1]));
       float ms = 0.f;
@@ -1062,7 +1307,7 @@ extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* m
     }
     c->tiling = best_v;
     // leave the residual partials of the resident state in the chosen layout (as hg_time_derivative)
-    stage(c, 0.0, 0.0, 0.0, true, false, c->d_QDot, true);
+    ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), true);
     HG_CUDA(cudaGetLastError());
     HG_CUDA(cudaStreamSynchronize(c->stream));
     c->prof = prof;

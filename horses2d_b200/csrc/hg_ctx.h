@@ -54,6 +54,18 @@ struct hg_ctx {
   int tiling = 0;                 // elements-per-CTA variant of the stage kernels (hg_autotune / hg_set_tiling)
   bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
   void* d_FX = nullptr;           // its face fluxes of the current stage [n_el*4][P][4], context precision
+  void* d_NF = nullptr;           // mortar fluxes of the SIDE_FLUX sides [slots][P][4], context precision
+  // Mixed orders and subdivided edges: the context is a composite of one part per polynomial order
+  // (each an ordinary context over its elements, on this context's stream); the faces between parts
+  // and the subdivided edges are evaluated by the mortar kernel (hg_mortar.cu) before each stage.
+  std::vector<hg_ctx*> parts;
+  std::vector<int> el_part, el_local, el_N;   // per mesh element: part, index in the part, order
+  std::vector<int64_t> el_offset;             // per mesh element: offset of its Q in Storage%Q (doubles)
+  std::vector<std::vector<int>> zone_edge_part;   // per zone: the part of each of its edges, in mesh order
+  int n_mortar_faces = 0;
+  void* d_mfaces = nullptr;       // MortarFace records
+  void* d_mmat = nullptr;         // projection matrices, context precision
+  void* d_mgeo = nullptr;         // face-node rows {nx, ny, dS}, context precision
   // zones fed per node (hg_set_boundary_state): state rows [rows][P][4] indexed by side.w
   double* d_bq = nullptr;
   int n_bq_rows = 0;
@@ -132,6 +144,18 @@ inline void max_carveout(K kernel) {
   HG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
                                int(cudaSharedmemCarveoutMaxShared)));
 }
+
+// Shared between hg_api.cu and hg_mortar.cu.
+void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs,
+               const std::vector<int2>* flux_sides);
+void ctx_free(hg_ctx* c);
+void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid);
+void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs);
+void composite_free(hg_ctx* c);
+void launch_mortar(hg_ctx* c);
+inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
+constexpr int HG_MAX_PARTS = 12;
+constexpr int HG_MAX_ORDER_EULER = 12;
 
 // Per-order launches, explicitly instantiated in hg_inst_*.cu (V = tiling variant: 0 in the plain
 // units, 1 in the *_t1 units).

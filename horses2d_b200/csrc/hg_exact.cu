@@ -21,7 +21,7 @@ __global__ void __launch_bounds__(128) exact_flux_kernel(int n_el, int P, int af
   const int64_t es = idx / P;          // element * 4 + side
   const int4 sd = side[es];
   const int kind = sd.y & 15;
-  if (kind == SIDE_WALL) return;       // prescribed wall flux, no Riemann problem
+  if (kind == SIDE_WALL || kind == SIDE_FLUX) return;   // prescribed wall flux / mortar face: no Riemann problem here
   int solver = riemann;
   if (sd.z >= 0) {
     const int zr = zones[sd.z].riemann;

@@ -1,0 +1,528 @@
+// hg_mortar.cu -- mixed polynomial orders and subdivided edges (Euler build).
+//
+// The reference couples elements of different orders through the edge's own order N_edge =
+// max(N_L, N_R): the lower-order trace is interpolated to the edge nodes (T_forward), the Riemann
+// flux is evaluated there, scaled by dS and L2-projected back (T_backward = M^-1 T^T M_edge)
+// (projection types 3-6, Mesh/QuadElement_EdgeProcedures.incf:749-1345, selection :161-197).  A
+// subdivided edge (SubdividedEdge_t, hanging node) holds one LEFT element against two RIGHT
+// elements: LEFT's trace is interpolated to the nodes of each half, the fluxes of both halves are
+// projected back and summed on LEFT, and each RIGHT element takes its half
+// (ComputeRiemannSolver_SubdividedEdge / CurvedSubdividedEdge,
+// Approximation/DGSpatialDiscretizationMethods.f90:761-1140; matrices SubdividedEdge_LinkWithElements,
+// Mesh/QuadElement_EdgeProcedures.incf).
+//
+// B200 layout: a context over such a mesh is a composite of one ordinary context (part) per order,
+// each running the per-order fused stage kernel over its own packed elements.  Element sides on a
+// p-nonconforming or subdivided edge are marked SIDE_FLUX in their part: before every stage one
+// launch of mortar_kernel (one warp per face) reads the parts' traces, evaluates these faces and
+// writes each side's lifted flux -- projected to that element's side nodes, dS and sign applied --
+// to the part's NF buffer, which the stage kernel reads in place of a Riemann evaluation.
+#include "hg_ctx.h"
+#include "hg_spectral.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+
+namespace {
+
+// One face of the mortar kernel.  kind 0: edge between two orders (sides L, R); kind 1: subdivided
+// edge (sides L, RN, RS).  Projections tf/tb: kind 0 {L, R} (-1: identity), kind 1 {LN, LS, RN, RS};
+// offsets into the matrix pool, row-major [rows][cols].
+struct MortarFace {
+  int kind;
+  int part[3], el[3], side[3], slot[3], P[3];
+  int PE[2];      // edge nodes (kind 0), or north and south half nodes (kind 1)
+  int inv;        // kind 0: RIGHT traverses the edge backwards
+  int tf[4], tb[4];
+  int geo[2];     // rows {nx, ny, dS} of the edge (kind 0) or of the north and south halves (kind 1)
+};
+
+template <typename real>
+struct MortarArgs {
+  int n;
+  const MortarFace* f;
+  const real* mat;
+  const real* geo;
+  const real* T[HG_MAX_PARTS];
+  real* NF[HG_MAX_PARTS];
+  int riemann;
+  PhysConst pc;
+};
+
+constexpr int MW = 4;        // faces (warps) per CTA
+constexpr int MP = 16;       // node capacity of a side or half edge (orders up to 15)
+
+// row `r` of (matrix m, or the identity) applied to the node vector src[cols][4] in shared memory
+template <typename real>
+__device__ __forceinline__ void project_row(const real* mat, int m, int cols, int r, const real (*src)[4], real* out) {
+  if (m < 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = src[r][k];
+    return;
+  }
+  real acc[4] = {real(0), real(0), real(0), real(0)};
+  const real* row = mat + m + size_t(r) * cols;
+  for (int l = 0; l < cols; ++l) {
+    const real t = row[l];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[k] = acc[k] + t * src[l][k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) out[k] = acc[k];
+}
+
+template <typename real>
+__device__ __forceinline__ void face_flux(int solver, const Phys<real>& ph, const real* qL, const real* qR,
+                                          const real* g, real* F) {
+  if (solver == RIEMANN_EXACT) exact(ph, qL, qR, g[0], g[1], F);
+  else riemann(solver, ph, qL, qR, g[0], g[1], F);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) F[k] = F[k] * g[2];
+}
+
+template <typename real>
+__global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
+  __shared__ real sT[MW][3][MP][4];   // traces of the face's element sides
+  __shared__ real sF[MW][2][MP][4];   // fluxes at the edge (half) nodes, x dS
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int fi = blockIdx.x * MW + w;
+  if (fi >= a.n) return;   // whole warps leave together; the kernel synchronises warps only
+  const MortarFace& f = a.f[fi];
+  const int ns = f.kind == 0 ? 2 : 3;
+  for (int t = lane; t < ns * MP; t += 32) {
+    const int s = t / MP, k = t % MP;
+    if (k < f.P[s]) {
+      const real* tp = a.T[f.part[s]] + ((size_t(f.el[s]) * 4 + f.side[s]) * f.P[s] + k) * 4;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) sT[w][s][k][q] = tp[q];
+    }
+  }
+  __syncwarp();
+  Phys<real> ph;
+  ph.load(a.pc);
+  if (f.kind == 0) {
+    const int PE = f.PE[0];
+    if (lane < PE) {
+      real qL[4], qR[4], F[4];
+      project_row(a.mat, f.tf[0], f.P[0], lane, sT[w][0], qL);
+      project_row(a.mat, f.tf[1], f.P[1], f.inv ? PE - 1 - lane : lane, sT[w][1], qR);
+      face_flux(a.riemann, ph, qL, qR, a.geo + size_t(f.geo[0] + lane) * 3, F);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sF[w][0][lane][k] = F[k];
+    }
+    __syncwarp();
+    // LEFT: FL = Tb F (or F); RIGHT: FR = -(Tb F) in its own node order
+    if (lane < f.P[0]) {
+      real out[4];
+      project_row(a.mat, f.tb[0], PE, lane, sF[w][0], out);
+      real* np = a.NF[f.part[0]] + (size_t(f.slot[0]) * f.P[0] + lane) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) np[k] = out[k];
+    } else if (lane >= 16 && lane - 16 < f.P[1]) {
+      const int j = lane - 16;
+      real out[4];
+      project_row(a.mat, f.tb[1], PE, f.inv ? f.P[1] - 1 - j : j, sF[w][0], out);
+      real* np = a.NF[f.part[1]] + (size_t(f.slot[1]) * f.P[1] + j) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) np[k] = -out[k];
+    }
+  } else {
+    // lanes 0-15: north half (LEFT against RIGHT_NORTH), lanes 16-31: south half
+    const int h = lane >> 4, i = lane & 15;
+    if (i < f.PE[h]) {
+      real qL[4], qR[4], F[4];
+      project_row(a.mat, f.tf[h], f.P[0], i, sT[w][0], qL);
+      project_row(a.mat, f.tf[2 + h], f.P[1 + h], i, sT[w][1 + h], qR);
+      face_flux(a.riemann, ph, qL, qR, a.geo + size_t(f.geo[h] + i) * 3, F);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) sF[w][h][i][k] = F[k];
+    }
+    __syncwarp();
+    if (h == 0 && i < f.P[0]) {
+      // LEFT collects both halves: FL = Tb_LN F_N + Tb_LS F_S
+      real acc[4] = {real(0), real(0), real(0), real(0)};
+      for (int hh = 0; hh < 2; ++hh) {
+        const int cols = f.PE[hh];
+        const real* row = a.mat + f.tb[hh] + size_t(i) * cols;
+        for (int l = 0; l < cols; ++l) {
+          const real t = row[l];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) acc[k] = acc[k] + t * sF[w][hh][l][k];
+        }
+      }
+      real* np = a.NF[f.part[0]] + (size_t(f.slot[0]) * f.P[0] + i) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) np[k] = acc[k];
+    } else if (h == 1) {
+      for (int r = 0; r < 2; ++r) {
+        if (i < f.P[1 + r]) {
+          real out[4];
+          project_row(a.mat, f.tb[2 + r], f.PE[r], i, sF[w][r], out);
+          real* np = a.NF[f.part[1 + r]] + (size_t(f.slot[1 + r]) * f.P[1 + r] + i) * 4;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) np[k] = -out[k];
+        }
+      }
+    }
+  }
+}
+
+template <typename T>
+T* dalloc_n(size_t n) {
+  void* p = nullptr;
+  HG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  return static_cast<T*>(p);
+}
+
+void upload_prec(void*& dst, const std::vector<double>& src, int precision) {
+  if (precision == HG_PREC_FP32) {
+    std::vector<float> f(src.begin(), src.end());
+    dst = dalloc_n<float>(f.size());
+    HG_CUDA(cudaMemcpy(dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+  } else {
+    dst = dalloc_n<double>(src.size());
+    HG_CUDA(cudaMemcpy(dst, src.data(), src.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
+}
+
+// Matrix pool: interpolation from an element's nodes to given points (T_forward) and its L2 back
+// projection with the edge quadrature (T_backward(i, l) = T_forward(l, i) w_edge(l) / w_el(i)).
+struct MatPool {
+  std::vector<double> v;
+  int node_type = 0;
+  std::map<int, NodalOps> ops;
+  const NodalOps& op(int N) {
+    auto it = ops.find(N);
+    if (it == ops.end()) it = ops.emplace(N, make_nodal_ops(N, node_type)).first;
+    return it->second;
+  }
+  // forward matrix [Ne+1 rows = points][Nel+1]; flip: the element's nodes run the other way
+  std::vector<double> forward(int Nel, const std::vector<double>& pts, bool flip) {
+    const NodalOps& e = op(Nel);
+    std::vector<double> T(pts.size() * e.P);
+    for (size_t r = 0; r < pts.size(); ++r) {
+      const std::vector<double> l = lagrange_basis(e, pts[r]);
+      for (int c = 0; c < e.P; ++c) T[r * e.P + (flip ? e.P - 1 - c : c)] = l[c];
+    }
+    return T;
+  }
+  std::vector<double> backward(int Nel, int Nedge, const std::vector<double>& Tf, bool flip) {
+    const NodalOps& e = op(Nel);
+    const NodalOps& g = op(Nedge);
+    // unflipped forward matrix first (the flip reverses the rows of the back projection)
+    std::vector<double> Tb(size_t(e.P) * g.P);
+    for (int i = 0; i < e.P; ++i)
+      for (int l = 0; l < g.P; ++l) {
+        const int ci = flip ? e.P - 1 - i : i;   // column of Tf holding element node i
+        Tb[size_t(flip ? e.P - 1 - i : i) * g.P + l] = ((1.0 / e.w[i]) * Tf[size_t(l) * e.P + ci]) * g.w[l];
+      }
+    return Tb;
+  }
+  int add(const std::vector<double>& m) {
+    const int off = int(v.size());
+    v.insert(v.end(), m.begin(), m.end());
+    return off;
+  }
+};
+
+}  // namespace
+
+void launch_mortar(hg_ctx* c) {
+  if (c->n_mortar_faces == 0) return;
+  const int grid = (c->n_mortar_faces + MW - 1) / MW;
+  auto go = [&](auto tag) {
+    using real = decltype(tag);
+    MortarArgs<real> a{};
+    a.n = c->n_mortar_faces;
+    a.f = static_cast<const MortarFace*>(c->d_mfaces);
+    a.mat = static_cast<const real*>(c->d_mmat);
+    a.geo = static_cast<const real*>(c->d_mgeo);
+    for (size_t p = 0; p < c->parts.size(); ++p) {
+      a.T[p] = static_cast<const real*>(c->parts[p]->d_T[c->parts[p]->cur]);
+      a.NF[p] = static_cast<real*>(c->parts[p]->d_NF);
+    }
+    a.riemann = c->riemann;
+    a.pc = c->pc;
+    timed(c, HG_KERNEL_MORTAR, [&] { mortar_kernel<real><<<grid, MW * 32, 0, c->stream>>>(a); });
+  };
+  if (c->precision == HG_PREC_FP32) go(float{});
+  else go(double{});
+  ++c->launches;
+}
+
+void composite_free(hg_ctx* c) {
+  for (hg_ctx* p : c->parts) {
+    ctx_free(p);
+    delete p;
+  }
+  c->parts.clear();
+  for (void* p : {c->d_mfaces, c->d_mmat, c->d_mgeo})
+    if (p) cudaFree(p);
+  c->d_mfaces = c->d_mmat = c->d_mgeo = nullptr;
+}
+
+void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
+  if (ph->navier_stokes) throw std::runtime_error("mixed orders and subdivided edges are supported for the Euler build only");
+  const int E = m->n_elements;
+  if (E <= 0) throw std::runtime_error("mesh has no elements");
+  c->el_N.assign(m->N, m->N + E);
+  for (int e = 0; e < E; ++e)
+    if (c->el_N[e] < 1 || c->el_N[e] > HG_MAX_ORDER_EULER)
+      throw std::runtime_error("polynomial order must be in 1.." + std::to_string(HG_MAX_ORDER_EULER));
+  // parts: one per order, ascending; elements in mesh order within a part
+  std::vector<int> orders(c->el_N);
+  std::sort(orders.begin(), orders.end());
+  orders.erase(std::unique(orders.begin(), orders.end()), orders.end());
+  if (int(orders.size()) > HG_MAX_PARTS) throw std::runtime_error("too many polynomial orders");
+  const int NPART = int(orders.size());
+  std::vector<int> part_of_order(HG_MAX_ORDER_EULER + 1, -1);
+  for (int p = 0; p < NPART; ++p) part_of_order[orders[p]] = p;
+  c->el_part.resize(E);
+  c->el_local.resize(E);
+  c->el_offset.resize(E);
+  std::vector<int> part_n(NPART, 0);
+  std::vector<std::vector<int>> part_el(NPART);
+  std::vector<int64_t> node0(E);
+  int64_t nodes = 0;
+  for (int e = 0; e < E; ++e) {
+    const int p = part_of_order[c->el_N[e]];
+    c->el_part[e] = p;
+    c->el_local[e] = part_n[p]++;
+    part_el[p].push_back(e);
+    node0[e] = nodes;
+    c->el_offset[e] = nodes * 4;
+    nodes += int64_t(c->el_N[e] + 1) * (c->el_N[e] + 1);
+  }
+  c->n_el = E;
+  c->ndof = nodes * 4;
+  c->N = orders.back();
+  c->P = c->N + 1;
+  c->node_type = ph->node_type;
+  c->riemann = ph->riemann;
+  c->precision = c->precision;
+  const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
+  c->gamma = gamma; c->mach = ph->mach;
+  c->pc.gamma = gamma;
+  c->pc.gm1 = gamma - 1.0;
+  c->pc.cp = gamma / (gamma - 1.0);
+  c->pc.cv = 1.0 / (gamma - 1.0);
+  c->pc.invSqrtGammaMach = 1.0 / (std::sqrt(gamma) * ph->mach);
+
+  // edges: node offsets, owning part (conforming) or mortar face (two orders)
+  const int F = m->n_edges;
+  std::vector<int64_t> enode(F + 1, 0);
+  std::vector<int> edge_part(F, -1);
+  for (int f = 0; f < F; ++f) {
+    const int L = m->edge_elem[2 * f], R = m->edge_elem[2 * f + 1];
+    if (L < 0 || L >= E) throw std::runtime_error("bad edge connectivity");
+    const bool interior = m->edge_marker[f] == 0;
+    if (interior && (R < 0 || R >= E)) throw std::runtime_error("interior edge without RIGHT element");
+    const int NE = interior ? std::max(c->el_N[L], c->el_N[R]) : c->el_N[L];
+    enode[f + 1] = enode[f] + NE + 1;
+    if (!interior || c->el_N[L] == c->el_N[R]) edge_part[f] = c->el_part[L];
+  }
+  // zones: the part of each zone edge, in mesh order (per-node boundary states are split by it)
+  c->zone_type.assign(std::max(1, n_bcs), -1);
+  for (int z = 0; z < n_bcs; ++z) c->zone_type[z] = bcs[z].type;
+  c->zone_edge_part.assign(std::max(1, n_bcs), std::vector<int>());
+  for (int f = 0; f < F; ++f) {
+    const int mk = m->edge_marker[f];
+    if (mk == 0) continue;
+    if (mk < 1 || mk > n_bcs) throw std::runtime_error("boundary edge with unknown marker");
+    c->zone_edge_part[mk - 1].push_back(edge_part[f]);
+    if (bcs[mk - 1].type == HG_BC_PERIODIC) {
+      const int q = m->periodic_partner ? m->periodic_partner[f] : -1;
+      if (q < 0 || q >= F) throw std::runtime_error("periodic edge without partner");
+      if (c->el_N[m->edge_elem[2 * q]] != c->el_N[m->edge_elem[2 * f]])
+        throw std::runtime_error("periodic edges between different polynomial orders are not supported");
+    }
+  }
+  // local edge numbering per part
+  std::vector<int> edge_local(F, -1);
+  std::vector<std::vector<int>> part_edges(NPART);
+  for (int f = 0; f < F; ++f)
+    if (edge_part[f] >= 0) {
+      edge_local[f] = int(part_edges[edge_part[f]].size());
+      part_edges[edge_part[f]].push_back(f);
+    }
+
+  // mortar faces, their projection matrices and geometry; SIDE_FLUX slots per part
+  MatPool pool;
+  pool.node_type = ph->node_type;
+  std::vector<double> geo;
+  std::vector<MortarFace> faces;
+  std::vector<std::vector<int2>> flux_sides(NPART);
+  auto side_slot = [&](int e, int s) {
+    const int p = c->el_part[e];
+    const int slot = int(flux_sides[p].size());
+    flux_sides[p].push_back(make_int2(c->el_local[e] * 4 + s, slot));
+    return slot;
+  };
+  auto fill_side = [&](MortarFace& mf, int k, int e, int s) {
+    mf.part[k] = c->el_part[e];
+    mf.el[k] = c->el_local[e];
+    mf.side[k] = s;
+    mf.P[k] = c->el_N[e] + 1;
+    mf.slot[k] = side_slot(e, s);
+  };
+  for (int f = 0; f < F; ++f) {
+    if (edge_part[f] >= 0) continue;
+    const int L = m->edge_elem[2 * f], R = m->edge_elem[2 * f + 1];
+    const int sL = m->edge_side[2 * f] - 1, sR = m->edge_side[2 * f + 1] - 1;
+    if (sL < 0 || sL > 3 || sR < 0 || sR > 3) throw std::runtime_error("bad edge connectivity");
+    MortarFace mf{};
+    mf.kind = 0;
+    fill_side(mf, 0, L, sL);
+    fill_side(mf, 1, R, sR);
+    mf.part[2] = mf.el[2] = mf.side[2] = mf.slot[2] = mf.P[2] = 0;
+    const int NE = std::max(c->el_N[L], c->el_N[R]);
+    mf.PE[0] = NE + 1;
+    mf.PE[1] = 0;
+    mf.inv = m->edge_inverse[f] != 0;
+    for (int k = 0; k < 4; ++k) mf.tf[k] = mf.tb[k] = -1;
+    const std::vector<double> xe = pool.op(NE).xi;
+    for (int k = 0; k < 2; ++k) {
+      const int Nk = c->el_N[k == 0 ? L : R];
+      if (Nk == NE) continue;
+      const std::vector<double> Tf = pool.forward(Nk, xe, false);
+      mf.tf[k] = pool.add(Tf);
+      mf.tb[k] = pool.add(pool.backward(Nk, NE, Tf, false));
+    }
+    mf.geo[0] = int(geo.size() / 3);
+    mf.geo[1] = 0;
+    for (int64_t n = enode[f]; n < enode[f + 1]; ++n) {
+      geo.push_back(m->edge_n[2 * n]);
+      geo.push_back(m->edge_n[2 * n + 1]);
+      geo.push_back(m->edge_dS[n]);
+    }
+    faces.push_back(mf);
+  }
+  int64_t mnode = 0;
+  for (int q = 0; q < m->n_mortars; ++q) {
+    const int* el = m->mortar_elem + 3 * q;
+    const int* sd = m->mortar_side + 3 * q;
+    for (int k = 0; k < 3; ++k)
+      if (el[k] < 0 || el[k] >= E || sd[k] < 1 || sd[k] > 4) throw std::runtime_error("bad subdivided-edge connectivity");
+    const int NL = c->el_N[el[0]], NRN = c->el_N[el[1]], NRS = c->el_N[el[2]];
+    const int NN = std::max(NL, NRN), NS = std::max(NL, NRS);
+    MortarFace mf{};
+    mf.kind = 1;
+    for (int k = 0; k < 3; ++k) fill_side(mf, k, el[k], sd[k] - 1);
+    mf.PE[0] = NN + 1;
+    mf.PE[1] = NS + 1;
+    mf.inv = 0;
+    std::vector<double> xN = pool.op(NN).xi, xS = pool.op(NS).xi;
+    std::vector<double> hN(xN.size()), hS(xS.size());
+    for (size_t p = 0; p < xN.size(); ++p) hN[p] = 0.5 + 0.5 * xN[p];
+    for (size_t p = 0; p < xS.size(); ++p) hS[p] = 0.5 * xS[p];
+    const bool flipN = m->mortar_flip[2 * q] != 0, flipS = m->mortar_flip[2 * q + 1] != 0;
+    const std::vector<double> TLN = pool.forward(NL, hN, false), TLS = pool.forward(NL, hS, false);
+    const std::vector<double> TRN = pool.forward(NRN, xN, flipN), TRS = pool.forward(NRS, xS, flipS);
+    mf.tf[0] = pool.add(TLN);
+    mf.tf[1] = pool.add(TLS);
+    mf.tf[2] = pool.add(TRN);
+    mf.tf[3] = pool.add(TRS);
+    mf.tb[0] = pool.add(pool.backward(NL, NN, TLN, false));
+    mf.tb[1] = pool.add(pool.backward(NL, NS, TLS, false));
+    mf.tb[2] = pool.add(pool.backward(NRN, NN, TRN, flipN));
+    mf.tb[3] = pool.add(pool.backward(NRS, NS, TRS, flipS));
+    mf.geo[0] = int(geo.size() / 3);
+    for (int p = 0; p < NN + 1; ++p, ++mnode) {
+      geo.push_back(m->mortar_n[2 * mnode]);
+      geo.push_back(m->mortar_n[2 * mnode + 1]);
+      geo.push_back(m->mortar_dS[mnode]);
+    }
+    mf.geo[1] = int(geo.size() / 3);
+    for (int p = 0; p < NS + 1; ++p, ++mnode) {
+      geo.push_back(m->mortar_n[2 * mnode]);
+      geo.push_back(m->mortar_n[2 * mnode + 1]);
+      geo.push_back(m->mortar_dS[mnode]);
+    }
+    faces.push_back(mf);
+  }
+  for (const MortarFace& mf : faces)
+    for (int k = 0; k < (mf.kind == 0 ? 2 : 3); ++k)
+      if (mf.P[k] > MP || mf.PE[0] > MP || mf.PE[1] > MP) throw std::runtime_error("order too high for a mortar face");
+
+  // the parts: ordinary contexts over sub-descriptors of one order
+  for (int p = 0; p < NPART; ++p) {
+    const int Np = orders[p], Pp = Np + 1, NPp = Pp * Pp;
+    const std::vector<int>& els = part_el[p];
+    const std::vector<int>& eds = part_edges[p];
+    const int Ep = int(els.size()), Fp = int(eds.size());
+    std::vector<int> sN(Ep, Np), eelem(2 * Fp), eside(2 * Fp), einv(Fp), emark(Fp), epart(Fp, -1);
+    std::vector<double> Ja(size_t(Ep) * NPp * 4), jac(size_t(Ep) * NPp), x(size_t(Ep) * NPp * 2), vol(Ep),
+        vert(size_t(Ep) * 8), en(size_t(Fp) * Pp * 2), eds_(size_t(Fp) * Pp), invh(Fp, 0.0);
+    for (int k = 0; k < Ep; ++k) {
+      const int e = els[k];
+      const int64_t n0 = node0[e];
+      std::copy(m->Ja + n0 * 4, m->Ja + (n0 + NPp) * 4, Ja.begin() + size_t(k) * NPp * 4);
+      std::copy(m->jac + n0, m->jac + n0 + NPp, jac.begin() + size_t(k) * NPp);
+      if (m->x) std::copy(m->x + n0 * 2, m->x + (n0 + NPp) * 2, x.begin() + size_t(k) * NPp * 2);
+      vol[k] = m->volume ? m->volume[e] : 0.0;
+      if (m->vertices) std::copy(m->vertices + size_t(e) * 8, m->vertices + size_t(e) * 8 + 8, vert.begin() + size_t(k) * 8);
+    }
+    for (int k = 0; k < Fp; ++k) {
+      const int f = eds[k];
+      const int L = m->edge_elem[2 * f], R = m->edge_elem[2 * f + 1];
+      eelem[2 * k] = c->el_local[L];
+      eelem[2 * k + 1] = (m->edge_marker[f] == 0) ? c->el_local[R] : -1;
+      eside[2 * k] = m->edge_side[2 * f];
+      eside[2 * k + 1] = m->edge_side[2 * f + 1];
+      einv[k] = m->edge_inverse[f];
+      emark[k] = m->edge_marker[f];
+      if (m->periodic_partner && m->periodic_partner[f] >= 0) epart[k] = edge_local[m->periodic_partner[f]];
+      if (m->edge_invh) invh[k] = m->edge_invh[f];
+      for (int n = 0; n < Pp; ++n) {
+        en[(size_t(k) * Pp + n) * 2] = m->edge_n[(enode[f] + n) * 2];
+        en[(size_t(k) * Pp + n) * 2 + 1] = m->edge_n[(enode[f] + n) * 2 + 1];
+        eds_[size_t(k) * Pp + n] = m->edge_dS[enode[f] + n];
+      }
+    }
+    hg_mesh_desc sub{};
+    sub.n_elements = Ep;
+    sub.n_edges = Fp;
+    sub.N = sN.data();
+    sub.Ja = Ja.data();
+    sub.jac = jac.data();
+    sub.x = m->x ? x.data() : nullptr;
+    sub.volume = m->volume ? vol.data() : nullptr;
+    sub.vertices = m->vertices ? vert.data() : nullptr;
+    sub.edge_elem = eelem.data();
+    sub.edge_side = eside.data();
+    sub.edge_inverse = einv.data();
+    sub.edge_marker = emark.data();
+    sub.edge_n = en.data();
+    sub.edge_dS = eds_.data();
+    sub.periodic_partner = epart.data();
+    sub.edge_invh = m->edge_invh ? invh.data() : nullptr;
+    hg_ctx* pc = new hg_ctx();
+    pc->precision = c->precision;
+    c->parts.push_back(pc);
+    ctx_build(pc, &sub, ph, bcs, n_bcs, &flux_sides[p]);
+    // the part runs on the composite's stream
+    HG_CUDA(cudaStreamDestroy(pc->stream));
+    pc->own_stream = false;
+    pc->stream = nullptr;
+    const size_t rs = c->precision == HG_PREC_FP32 ? sizeof(float) : sizeof(double);
+    pc->d_NF = dalloc_n<char>(flux_sides[p].size() * Pp * 4 * rs);
+    HG_CUDA(cudaMemset(pc->d_NF, 0, std::max<size_t>(flux_sides[p].size() * Pp * 4 * rs, 1)));
+  }
+  // per-element corner distances of the whole mesh (EstimateTimeStep runs over mesh order)
+  c->dx.assign(E, 0.0);
+  if (m->vertices)
+    for (int e = 0; e < E; ++e) {
+      const double* v = m->vertices + size_t(e) * 8;
+      auto d = [&](int a, int b) { return std::sqrt((v[2 * a] - v[2 * b]) * (v[2 * a] - v[2 * b]) + (v[2 * a + 1] - v[2 * b + 1]) * (v[2 * a + 1] - v[2 * b + 1])); };
+      c->dx[e] = std::fmin(std::fmin(d(0, 1), d(1, 2)), std::fmin(d(2, 3), d(0, 3)));
+    }
+  HG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->own_stream = true;
+  for (hg_ctx* pc : c->parts) pc->stream = c->stream;
+  c->n_mortar_faces = int(faces.size());
+  c->d_mfaces = dalloc_n<MortarFace>(faces.size());
+  HG_CUDA(cudaMemcpy(c->d_mfaces, faces.data(), faces.size() * sizeof(MortarFace), cudaMemcpyHostToDevice));
+  upload_prec(c->d_mmat, pool.v, c->precision);
+  upload_prec(c->d_mgeo, geo, c->precision);
+}

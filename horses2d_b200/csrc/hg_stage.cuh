@@ -30,8 +30,9 @@
 
 namespace hg {
 
-// side kinds
-enum { SIDE_LEFT = 0, SIDE_RIGHT = 1, SIDE_STATE = 2, SIDE_WALL = 3 };
+// side kinds; SIDE_FLUX: a p-nonconforming or subdivided edge, whose lifted flux (projected to this
+// element's side nodes, dS and sign applied) the mortar kernel has written to the NF buffer
+enum { SIDE_LEFT = 0, SIDE_RIGHT = 1, SIDE_STATE = 2, SIDE_WALL = 3, SIDE_FLUX = 4 };
 constexpr int SIDE_REVERSED = 16;
 
 template <typename real>
@@ -44,6 +45,7 @@ struct StageArgs {
   const Zone* zones;
   const double* bq;        // per-node Dirichlet states [rows][P][4] (sides whose side.w >= 0)
   const real* FX;          // exact-solver face fluxes [n_el*4][P][4] of this stage (RIEMANN_EXACT faces)
+  const real* NF;          // mortar fluxes [slots][P][4] of SIDE_FLUX sides (slot = side.x)
   double* Q;               // [n_el][P*P][4]
   real* G;                 // [n_el][P*P][4]
   const real* T_in;        // [n_el*4][P][4]
@@ -60,7 +62,7 @@ struct StageArgs {
 // Elements per CTA: tiling variant 0 (default, large CTAs) and variant 1 (small CTAs: more CTAs in
 // flight on small meshes); hg_autotune times both on the resident state and keeps the faster.
 __host__ __device__ constexpr int epb_for(int P) {
-  return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : 3;
+  return P == 2 ? 32 : P == 3 ? 16 : P == 4 ? 16 : P == 5 ? 8 : P == 6 ? 8 : P == 7 ? 4 : P == 8 ? 4 : P <= 11 ? 3 : 2;
 }
 __host__ __device__ constexpr int epb_small_for(int P) {
   return P == 2 ? 8 : P == 3 ? 4 : P == 4 ? 4 : P == 5 ? 2 : P == 6 ? 2 : P == 7 ? 2 : 1;
@@ -134,6 +136,12 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
       const int s = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + s];
       const int kind = sd.y & 15;
+      if (kind == SIDE_FLUX) {
+        const real* fp = a.NF + (size_t(sd.x) * P + kk) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s_F[k][le][t] = fp[k];
+        continue;
+      }
       const real* lbv = (s == 0 || s == 3) ? lb0 : lb1;
       real qo[4] = {real(0), real(0), real(0), real(0)};
       if (LGL) {

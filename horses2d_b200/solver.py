@@ -74,6 +74,11 @@ class GpuDGSEM:
         put("edge_dS", "edge_dS", np.float64, C.c_double)
         put("periodic_partner", "periodic_partner", np.int32, C.c_int32, True)
         put("edge_invh", "edge_invh", np.float64, C.c_double, True)
+        md.n_mortars = int(len(np.asarray(mesh.get("mortar_elem", ()))) // 3)
+        for f, dt, ct in (("mortar_elem", np.int32, C.c_int32), ("mortar_side", np.int32, C.c_int32),
+                          ("mortar_flip", np.int32, C.c_int32), ("mortar_n", np.float64, C.c_double),
+                          ("mortar_dS", np.float64, C.c_double)):
+            put(f, f, dt, ct, True)
         ph = L.PhysicsDesc(node_type=node_type, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous,
                            ip_method=ip_method, sigma0_ip=sigma0_ip, mach=mach, reynolds=reynolds,
                            prandtl=prandtl, pressure_ref=pressure_ref, temperature_ref=temperature_ref, reynolds_length=reynolds_length, gamma=gamma,

@@ -78,7 +78,14 @@ typedef struct {
 
 /* The mesh after the reference's construction (QuadMesh_t after
  * constructFromFile + ConstructZones), flattened.  Per-node arrays follow the
- * Storage%Q node order (offset/4).  Edge arrays follow mesh%edges order. */
+ * Storage%Q node order (offset/4).  Edge arrays follow mesh%edges order with the
+ * subdivided edges taken out (they are the mortar list below); an edge carries
+ * N_edge+1 nodes, N_edge = max of its elements' orders (the edge's own order in the
+ * reference), stored one edge after the other.
+ * Mixed orders and subdivided edges (p-nonconforming projections types 3-6 and
+ * SubdividedEdge_t, Mesh/QuadElement_EdgeProcedures.incf:749-1345) are supported for
+ * the Euler build (navier_stokes = 0), orders 1-12; the Navier-Stokes build takes one
+ * order (1-8) and no mortars. */
 typedef struct {
   int32_t n_elements;
   int32_t n_edges;
@@ -96,6 +103,16 @@ typedef struct {
   const double*  edge_dS;       /* [n_edges][N_edge+1]    surface jacobian */
   const int32_t* periodic_partner; /* [n_edges] partner boundary edge of a periodic edge, else -1 */
   const double*  edge_invh;     /* [n_edges] Area / min(volume) (interior penalty); may be NULL */
+  /* Subdivided edges (SubdividedEdge_LinkWithElements, Mesh/QuadElement_EdgeProcedures.incf):
+   * a LEFT element against two RIGHT elements, each covering half of the edge; LEFT runs the
+   * edge forwards.  PN = max(N_LEFT, N_RIGHT_NORTH)+1 and PS = max(N_LEFT, N_RIGHT_SOUTH)+1
+   * nodes on the north half (edge parameter 1/2..1) and the south half (0..1/2). */
+  int32_t n_mortars;
+  const int32_t* mortar_elem;   /* [n_mortars][3] LEFT, RIGHT_NORTH, RIGHT_SOUTH (0-based) */
+  const int32_t* mortar_side;   /* [n_mortars][3] edgeLocation 1..4 of each */
+  const int32_t* mortar_flip;   /* [n_mortars][2] RIGHT_NORTH, RIGHT_SOUTH traverse their half backwards */
+  const double*  mortar_n;      /* [n_mortars][PN+PS][2] unit normals outward from LEFT (north then south) */
+  const double*  mortar_dS;     /* [n_mortars][PN+PS]    surface jacobians of the halves */
 } hg_mesh_desc;
 
 /* Create a context: uploads geometry, connectivity and boundary zones once.
@@ -162,7 +179,8 @@ int64_t hg_launch_count(const hg_ctx* ctx);
  * hg_kernel_times synchronises and returns, per HG_KERNEL_* class (first n),
  * the summed milliseconds and the launch count since timing started. */
 enum { HG_KERNEL_STAGE = 0, HG_KERNEL_GRADIENT = 1, HG_KERNEL_TRACE = 2, HG_KERNEL_REDUCE = 3,
-       HG_KERNEL_SPEED = 4, HG_KERNEL_FACEFLUX = 5, HG_KERNEL_KINDS = 6 };
+       HG_KERNEL_SPEED = 4, HG_KERNEL_FACEFLUX = 5, HG_KERNEL_MORTAR = 6,
+       HG_KERNEL_KINDS = 7 };
 int  hg_profile(hg_ctx* ctx, int32_t enable);
 int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
 /* hg_residuals_noalloc -- no reference counterpart.  Per-variable max |x| (the reduction of

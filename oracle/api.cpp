@@ -230,13 +230,21 @@ extern "C" int or_edge_count_by_type(void* h, int type) {
   return c;
 }
 
+extern "C" void or_export_sizes(void* h, int out[4]) {
+  Oracle& o = *static_cast<Oracle*>(h);
+  int F = 0, FN = 0, M = 0, MN = 0;
+  for (auto& f : o.ed) {
+    if (f.is_subdiv()) { ++M; MN += f.spN->P + f.spS->P; }
+    else { ++F; FN += f.P(); }
+  }
+  out[0] = F; out[1] = FN; out[2] = M; out[3] = MN;
+}
+
 extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                               int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
-                              double* edge_dS, int* periodic_partner, double* edge_invh) {
+                              double* edge_dS, int* periodic_partner, double* edge_invh, int* mortar_elem,
+                              int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS) {
   Oracle& o = *static_cast<Oracle*>(h);
-  const int N0 = o.el[0].N;
-  for (auto& e : o.el) if (e.N != N0) return -1;
-  for (auto& f : o.ed) if (f.is_subdiv()) return -1;
   for (size_t ei = 0; ei < o.el.size(); ++ei) {
     const Element& e = o.el[ei];
     N[ei] = e.N;
@@ -253,25 +261,56 @@ extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* 
       vertices[ei * 8 + 2 * k + 1] = o.nodeX[2 * e.nodes[k] + 1];
     }
   }
-  const int P = N0 + 1;
+  // the subdivided edges leave the edge list: renumber the others (periodic partners included)
+  std::vector<int> renum(o.ed.size(), -1);
+  int F = 0;
+  for (size_t fi = 0; fi < o.ed.size(); ++fi) if (!o.ed[fi].is_subdiv()) renum[fi] = F++;
+  int fo = 0, node = 0, m = 0, mnode = 0;
   for (size_t fi = 0; fi < o.ed.size(); ++fi) {
     const Edge& f = o.ed[fi];
+    if (f.is_subdiv()) {
+      const int PN = f.spN->P, PS = f.spS->P;
+      const bool curved = f.kind == E_CURVED_SUBDIV;
+      const int slots[3] = {SLOT_LEFT, SLOT_RN, SLOT_RS};
+      for (int s = 0; s < 3; ++s) {
+        mortar_elem[3 * m + s] = f.quads[slots[s]];
+        mortar_side[3 * m + s] = f.edgeLocation[slots[s]];
+      }
+      for (int s = 0; s < 2; ++s) {
+        const int slot = s == 0 ? SLOT_RN : SLOT_RS;
+        const Element& R = o.el[f.quads[slot]];
+        mortar_flip[2 * m + s] = R.edgesDirection[f.edgeLocation[slot] - 1] == BACKWARD ? 1 : 0;
+      }
+      for (int p = 0; p < PN; ++p, ++mnode) {
+        mortar_n[2 * mnode] = curved ? f.normal_N[p] : f.normal_N[0];
+        mortar_n[2 * mnode + 1] = curved ? f.normal_N[PN + p] : f.normal_N[1];
+        mortar_dS[mnode] = curved ? f.dS_N[p] : f.dS_N[0];
+      }
+      for (int p = 0; p < PS; ++p, ++mnode) {
+        mortar_n[2 * mnode] = curved ? f.normal_S[p] : f.normal_S[0];
+        mortar_n[2 * mnode + 1] = curved ? f.normal_S[PS + p] : f.normal_S[1];
+        mortar_dS[mnode] = curved ? f.dS_S[p] : f.dS_S[0];
+      }
+      ++m;
+      continue;
+    }
     if (f.is_bdry()) {
-      edge_elem[2 * fi] = f.quads[0]; edge_elem[2 * fi + 1] = -1;
-      edge_side[2 * fi] = f.edgeLocation[0]; edge_side[2 * fi + 1] = 0;
+      edge_elem[2 * fo] = f.quads[0]; edge_elem[2 * fo + 1] = -1;
+      edge_side[2 * fo] = f.edgeLocation[0]; edge_side[2 * fo + 1] = 0;
     } else {
-      edge_elem[2 * fi] = f.quads[SLOT_LEFT]; edge_elem[2 * fi + 1] = f.quads[SLOT_RIGHT];
-      edge_side[2 * fi] = f.edgeLocation[SLOT_LEFT]; edge_side[2 * fi + 1] = f.edgeLocation[SLOT_RIGHT];
+      edge_elem[2 * fo] = f.quads[SLOT_LEFT]; edge_elem[2 * fo + 1] = f.quads[SLOT_RIGHT];
+      edge_side[2 * fo] = f.edgeLocation[SLOT_LEFT]; edge_side[2 * fo + 1] = f.edgeLocation[SLOT_RIGHT];
     }
-    edge_inverse[fi] = f.inverse ? 1 : 0;
-    edge_marker[fi] = f.edgeType;
-    for (int p = 0; p < P; ++p) {
-      edge_n[(fi * P + p) * 2] = f.nx(p);
-      edge_n[(fi * P + p) * 2 + 1] = f.ny(p);
-      edge_dS[fi * P + p] = f.straight_like() ? f.dS[0] : f.dS[p];
+    edge_inverse[fo] = f.inverse ? 1 : 0;
+    edge_marker[fo] = f.edgeType;
+    for (int p = 0; p < f.P(); ++p, ++node) {
+      edge_n[2 * node] = f.nx(p);
+      edge_n[2 * node + 1] = f.ny(p);
+      edge_dS[node] = f.straight_like() ? f.dS[0] : f.dS[p];
     }
-    periodic_partner[fi] = f.periodic_partner;
-    edge_invh[fi] = f.invh;
+    periodic_partner[fo] = f.periodic_partner >= 0 ? renum[f.periodic_partner] : -1;
+    edge_invh[fo] = f.invh;
+    ++fo;
   }
   return 0;
 }

@@ -90,7 +90,9 @@ def lib():
         L.or_edge_count_by_type.restype = i
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
-        L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp]
+        L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp, ip, ip, ip, dp, dp]
+        L.or_export_sizes.restype = None
+        L.or_export_sizes.argtypes = [vp, ip]
         L.or_mesh_lists.restype = i
         L.or_mesh_lists.argtypes = [vp, ip, ip, ip, ip, ip]
         L.or_probe.restype = i
@@ -283,18 +285,22 @@ class Oracle:
         lib().or_set_zone_state(self.h, zone, _p(uB, C.c_double))
 
     def export_mesh(self):
-        """The constructed mesh flattened like include/horses_gpu.h hg_mesh_desc."""
-        E, F, n = self.n_elements, lib().or_n_edges(self.h), self.ndof // 4
-        P = int(self.orders[0]) + 1
+        """The constructed mesh flattened like include/horses_gpu.h hg_mesh_desc (subdivided edges as
+        the mortar list)."""
+        E, n = self.n_elements, self.ndof // 4
+        sz = np.zeros(4, np.int32)
+        lib().or_export_sizes(self.h, _p(sz, C.c_int))
+        F, FN, M, MN = (int(v) for v in sz)
         d = dict(N=np.zeros(E, np.int32), Ja=np.zeros(4 * n), jac=np.zeros(n), x=np.zeros(2 * n), volume=np.zeros(E),
                  vertices=np.zeros(8 * E), edge_elem=np.zeros(2 * F, np.int32), edge_side=np.zeros(2 * F, np.int32),
-                 edge_inverse=np.zeros(F, np.int32), edge_marker=np.zeros(F, np.int32), edge_n=np.zeros(2 * P * F),
-                 edge_dS=np.zeros(P * F), periodic_partner=np.zeros(F, np.int32), edge_invh=np.zeros(F))
+                 edge_inverse=np.zeros(F, np.int32), edge_marker=np.zeros(F, np.int32), edge_n=np.zeros(2 * FN),
+                 edge_dS=np.zeros(FN), periodic_partner=np.zeros(F, np.int32), edge_invh=np.zeros(F),
+                 mortar_elem=np.zeros(3 * M, np.int32), mortar_side=np.zeros(3 * M, np.int32),
+                 mortar_flip=np.zeros(2 * M, np.int32), mortar_n=np.zeros(2 * MN), mortar_dS=np.zeros(MN))
         ip_, dp_ = C.c_int, C.c_double
-        rc = lib().or_export_mesh(self.h, *[_p(d[k], ip_ if d[k].dtype == np.int32 else dp_) for k in
-                                            ("N", "Ja", "jac", "x", "volume", "vertices", "edge_elem", "edge_side",
-                                             "edge_inverse", "edge_marker", "edge_n", "edge_dS", "periodic_partner",
-                                             "edge_invh")])
-        if rc != 0:
-            raise RuntimeError("mesh has mortars or mixed polynomial orders")
+        lib().or_export_mesh(self.h, *[_p(d[k], ip_ if d[k].dtype == np.int32 else dp_) for k in
+                                       ("N", "Ja", "jac", "x", "volume", "vertices", "edge_elem", "edge_side",
+                                        "edge_inverse", "edge_marker", "edge_n", "edge_dS", "periodic_partner",
+                                        "edge_invh", "mortar_elem", "mortar_side", "mortar_flip", "mortar_n",
+                                        "mortar_dS")])
         return d

@@ -108,11 +108,13 @@ void    or_ref_values(void* h, double out[8]); /* rho, a, p, V, T, L, mu_dimless
 /* Geometry export for cross-checking host-side mesh builders. */
 void    or_element_geometry(void* h, double* Ja, double* jac, double* volume); /* Ja [ndof/4][2][2], jac [ndof/4], volume [E] */
 int     or_edge_count_by_type(void* h, int type);
-/* Flattened mesh in the layout of include/horses_gpu.h hg_mesh_desc (conforming,
- * uniform-order meshes).  Array sizes: N[E], Ja[nodes*4], jac[nodes], x[nodes*2],
- * volume[E], vertices[E*8], edge_elem[2F], edge_side[2F], edge_inverse[F],
- * edge_marker[F], edge_n[F*P*2], edge_dS[F*P], periodic_partner[F], edge_invh[F].
- * Returns 0, or -1 when the mesh has mortars or mixed orders. */
+/* Flattened mesh in the layout of include/horses_gpu.h hg_mesh_desc: subdivided edges form the
+ * mortar list, the other edges keep their order (renumbered).  or_export_sizes: {F edges, their
+ * nodes FN, M subdivided edges, their half-edge nodes MN}.  Array sizes: N[E], Ja[nodes*4],
+ * jac[nodes], x[nodes*2], volume[E], vertices[E*8], edge_elem[2F], edge_side[2F], edge_inverse[F],
+ * edge_marker[F], edge_n[FN*2], edge_dS[FN], periodic_partner[F], edge_invh[F], mortar_elem[3M],
+ * mortar_side[3M], mortar_flip[2M], mortar_n[MN*2], mortar_dS[MN].  Returns 0. */
+void    or_export_sizes(void* h, int out[4]);
 /* Boundary states given by functions (the problem-file plugin's BoundaryConditionFunction,
  * BoundaryConditions/BoundaryConditionFunctionDrivers.incf): or_zone_edge_nodes returns the
  * number of edge nodes of a zone and (if X != NULL) their coordinates [n][2], edges in
@@ -132,7 +134,8 @@ int     or_mesh_lists(void* h, int* points, int* elements, int* marker, int* cur
 void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                        int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
-                       double* edge_dS, int* periodic_partner, double* edge_invh);
+                       double* edge_dS, int* periodic_partner, double* edge_invh, int* mortar_elem,
+                       int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS);
 
 #ifdef __cplusplus
 }
