@@ -44,7 +44,7 @@ void ctx_free(hg_ctx* c) {
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
                   c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
-                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF};
+                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG};
   for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -121,6 +121,8 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.zones = c->d_zones;
   a.bq = c->d_bq;
   a.FX = static_cast<const real*>(c->d_FX);
+  a.NF = static_cast<const real*>(c->d_NF);
+  a.NFG = static_cast<const real*>(c->d_NFG);
   a.Q = c->d_Q;
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
@@ -148,8 +150,11 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.side_area = c->d_side_area;
   a.mu_av = c->d_mu_av;
   a.sensor = sensor_args(c);
-  if (c->exact) launch_exact_flux<real>(c);
+  a.run_stage = c->ns_phase != 1;
+  if (c->ns_phase == 2) a.run_gradient = 0;
+  if (c->exact && a.run_stage) launch_exact_flux<real>(c);
   HG_DISPATCH_P(c->P, ns_dispatch, c, a);
+  if (!a.run_stage) return;
   c->last_T = c->cur;   // trace buffer of the state this stage evaluated (surface integrals read it)
   if (update) c->cur ^= 1;
 }
@@ -187,13 +192,27 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
 void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid) {
   if (is_composite(c)) {
     // faces between orders and subdivided edges first, then every part's fused stage; the parts'
-    // launches are counted on the composite
-    launch_mortar(c);
-    for (hg_ctx* p : c->parts) {
-      const int64_t l0 = p->launches;
-      ctx_stage(p, ca, cb, cc, first, update, qdot ? p->d_QDot : nullptr, resid);
-      c->launches += p->launches - l0;
-      p->launches = l0;
+    // launches are counted on the composite.  Navier-Stokes (BR1): the mortar kernel's gradient face
+    // terms, the parts' gradient kernels, the mortar kernel's inviscid + viscous fluxes (they need
+    // the gradient traces), the parts' stage kernels.
+    auto parts_stage = [&](int phase) {
+      for (hg_ctx* p : c->parts) {
+        const int64_t l0 = p->launches;
+        p->ns_phase = phase;
+        ctx_stage(p, ca, cb, cc, first, update, qdot ? p->d_QDot : nullptr, resid);
+        p->ns_phase = 0;
+        c->launches += p->launches - l0;
+        p->launches = l0;
+      }
+    };
+    if (c->ns) {
+      launch_mortar(c, MORTAR_GRADIENT);
+      parts_stage(1);
+      launch_mortar(c, MORTAR_FLUX);
+      parts_stage(2);
+    } else {
+      launch_mortar(c, MORTAR_FLUX);
+      parts_stage(0);
     }
     c->last_T = c->cur;
     if (update) c->cur ^= 1;

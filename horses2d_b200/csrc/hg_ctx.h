@@ -55,6 +55,8 @@ struct hg_ctx {
   bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
   void* d_FX = nullptr;           // its face fluxes of the current stage [n_el*4][P][4], context precision
   void* d_NF = nullptr;           // mortar fluxes of the SIDE_FLUX sides [slots][P][4], context precision
+  void* d_NFG = nullptr;          // mortar BR1 gradient face terms of the SIDE_FLUX sides [slots][P][2][4]
+  int ns_phase = 0;               // a composite's Navier-Stokes part: 0 whole stage, 1 gradient kernel, 2 stage kernel
   // Mixed orders and subdivided edges: the context is a composite of one part per polynomial order
   // (each an ordinary context over its elements, on this context's stream); the faces between parts
   // and the subdivided edges are evaluated by the mortar kernel (hg_mortar.cu) before each stage.
@@ -152,7 +154,8 @@ void ctx_free(hg_ctx* c);
 void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid);
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs);
 void composite_free(hg_ctx* c);
-void launch_mortar(hg_ctx* c);
+enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1 };
+void launch_mortar(hg_ctx* c, int mode);
 inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
 constexpr int HG_MAX_PARTS = 12;
 constexpr int HG_MAX_ORDER_EULER = 12;

@@ -56,9 +56,11 @@ static void launch_ns_PAI(hg_ctx* c, const NSArgs<real>& a) {
           [&] { ns_gradient_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, BLK, 0, c->stream>>>(a); });
     ++c->launches;
   }
-  timed(c, HG_KERNEL_STAGE,
-        [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, BLK, 0, c->stream>>>(a); });
-  ++c->launches;
+  if (a.run_stage) {
+    timed(c, HG_KERNEL_STAGE,
+          [&] { ns_stage_kernel<P, EPB, real, AFFINE, IP, AV><<<grid, BLK, 0, c->stream>>>(a); });
+    ++c->launches;
+  }
 }
 
 template <int P, typename real, int V>

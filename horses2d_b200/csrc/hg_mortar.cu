@@ -1,4 +1,4 @@
-// hg_mortar.cu -- mixed polynomial orders and subdivided edges (Euler build).
+// hg_mortar.cu -- mixed polynomial orders and subdivided edges (Euler build; Navier-Stokes with BR1).
 //
 // The reference couples elements of different orders through the edge's own order N_edge =
 // max(N_L, N_R): the lower-order trace is interpolated to the edge nodes (T_forward), the Riemann
@@ -44,8 +44,12 @@ struct MortarArgs {
   const MortarFace* f;
   const real* mat;
   const real* geo;
-  const real* T[HG_MAX_PARTS];
-  real* NF[HG_MAX_PARTS];
+  const real* T[HG_MAX_PARTS];     // Q traces of the parts' current state
+  const real* GT[HG_MAX_PARTS];    // gradient traces (Navier-Stokes)
+  real* NF[HG_MAX_PARTS];          // MORTAR_FLUX output
+  real* NFG[HG_MAX_PARTS];         // MORTAR_GRADIENT output
+  int mode;                        // MORTAR_FLUX or MORTAR_GRADIENT
+  int visc;                        // MORTAR_FLUX: add the BR1 viscous flux
   int riemann;
   PhysConst pc;
 };
@@ -53,115 +57,152 @@ struct MortarArgs {
 constexpr int MW = 4;        // faces (warps) per CTA
 constexpr int MP = 16;       // node capacity of a side or half edge (orders up to 15)
 
-// row `r` of (matrix m, or the identity) applied to the node vector src[cols][4] in shared memory
-template <typename real>
-__device__ __forceinline__ void project_row(const real* mat, int m, int cols, int r, const real (*src)[4], real* out) {
+// row `r` of (matrix m, or the identity) applied to the node vector src[cols][S] (first NC values)
+template <int NC, int S, typename real>
+__device__ __forceinline__ void project_row(const real* mat, int m, int cols, int r, const real* src, real* out) {
   if (m < 0) {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) out[k] = src[r][k];
+    for (int k = 0; k < NC; ++k) out[k] = src[r * S + k];
     return;
   }
-  real acc[4] = {real(0), real(0), real(0), real(0)};
+  real acc[NC];
+#pragma unroll
+  for (int k = 0; k < NC; ++k) acc[k] = real(0);
   const real* row = mat + m + size_t(r) * cols;
   for (int l = 0; l < cols; ++l) {
     const real t = row[l];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) acc[k] = acc[k] + t * src[l][k];
+    for (int k = 0; k < NC; ++k) acc[k] = acc[k] + t * src[l * S + k];
   }
 #pragma unroll
-  for (int k = 0; k < 4; ++k) out[k] = acc[k];
+  for (int k = 0; k < NC; ++k) out[k] = acc[k];
 }
 
-template <typename real>
-__device__ __forceinline__ void face_flux(int solver, const Phys<real>& ph, const real* qL, const real* qR,
-                                          const real* g, real* F) {
-  if (solver == RIEMANN_EXACT) exact(ph, qL, qR, g[0], g[1], F);
-  else riemann(solver, ph, qL, qR, g[0], g[1], F);
+// Value at one edge node from the two sides' projected traces: MORTAR_FLUX the lifted flux
+// (Fi - Fv) dS (4 values), MORTAR_GRADIENT the BR1 terms u* dS n, u* = (qL + qR)/2 (8 values).
+template <int MODE, typename real>
+__device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys<real>& ph, const real* qL,
+                                           const real* qR, const real* dL, const real* dR, const real* g, real* out) {
+  if constexpr (MODE == MORTAR_GRADIENT) {
 #pragma unroll
-  for (int k = 0; k < 4; ++k) F[k] = F[k] * g[2];
+    for (int k = 0; k < 4; ++k) {
+      const real us = real(0.5) * (qL[k] + qR[k]);
+      out[k] = us * g[2] * g[0];
+      out[4 + k] = us * g[2] * g[1];
+    }
+  } else {
+    real F[4];
+    if (a.riemann == RIEMANN_EXACT) exact(ph, qL, qR, g[0], g[1], F);
+    else riemann(a.riemann, ph, qL, qR, g[0], g[1], F);
+    if (a.visc) {
+      real FLx[4], FLy[4], FRx[4], FRy[4];
+      viscous_flux(ph, qL, dL, dL + 4, FLx, FLy);
+      viscous_flux(ph, qR, dR, dR + 4, FRx, FRy);
+      const real mu = real(a.pc.mu);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const real fv = real(0.5) * (mu * FLx[k] + mu * FRx[k]) * g[0] + real(0.5) * (mu * FLy[k] + mu * FRy[k]) * g[1];
+        F[k] = F[k] - fv;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) out[k] = F[k] * g[2];
+  }
 }
 
-template <typename real>
+template <typename real, int MODE>
 __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
-  __shared__ real sT[MW][3][MP][4];   // traces of the face's element sides
-  __shared__ real sF[MW][2][MP][4];   // fluxes at the edge (half) nodes, x dS
+  constexpr int NC = MODE == MORTAR_GRADIENT ? 8 : 4;   // values per edge node
+  __shared__ real sT[MW][3][MP][4];   // Q traces of the face's element sides
+  __shared__ real sG[MW][3][MP][8];   // their gradient traces (x then y), viscous fluxes only
+  __shared__ real sF[MW][2][MP][NC];  // values at the edge (half) nodes
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int fi = blockIdx.x * MW + w;
   if (fi >= a.n) return;   // whole warps leave together; the kernel synchronises warps only
   const MortarFace& f = a.f[fi];
   const int ns = f.kind == 0 ? 2 : 3;
+  const bool grads = MODE == MORTAR_FLUX && a.visc;
   for (int t = lane; t < ns * MP; t += 32) {
     const int s = t / MP, k = t % MP;
     if (k < f.P[s]) {
-      const real* tp = a.T[f.part[s]] + ((size_t(f.el[s]) * 4 + f.side[s]) * f.P[s] + k) * 4;
+      const size_t row = (size_t(f.el[s]) * 4 + f.side[s]) * f.P[s] + k;
+      const real* tp = a.T[f.part[s]] + row * 4;
 #pragma unroll
       for (int q = 0; q < 4; ++q) sT[w][s][k][q] = tp[q];
+      if (grads) {
+        const real* gp = a.GT[f.part[s]] + row * 8;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) sG[w][s][k][q] = gp[q];
+      }
     }
   }
   __syncwarp();
   Phys<real> ph;
   ph.load(a.pc);
+  // edge-node values: kind 0 one edge on lanes 0..PE-1; kind 1 the north half on lanes 0-15, the
+  // south half on lanes 16-31
+  {
+    const int h = f.kind == 0 ? 0 : lane >> 4;
+    const int i = f.kind == 0 ? lane : lane & 15;
+    const int PE = f.PE[h];
+    if (i < PE) {
+      real qL[4], qR[4], dL[8], dR[8], v[NC];
+      const int sR = f.kind == 0 ? 1 : 1 + h;
+      const int mL = f.kind == 0 ? f.tf[0] : f.tf[h];
+      const int mR = f.kind == 0 ? f.tf[1] : f.tf[2 + h];
+      const int rR = (f.kind == 0 && f.inv) ? PE - 1 - i : i;
+      project_row<4, 4>(a.mat, mL, f.P[0], i, &sT[w][0][0][0], qL);
+      project_row<4, 4>(a.mat, mR, f.P[sR], rR, &sT[w][sR][0][0], qR);
+      if (grads) {
+        project_row<8, 8>(a.mat, mL, f.P[0], i, &sG[w][0][0][0], dL);
+        project_row<8, 8>(a.mat, mR, f.P[sR], rR, &sG[w][sR][0][0], dR);
+      }
+      node_value<MODE>(a, ph, qL, qR, dL, dR, a.geo + size_t(f.geo[h] + i) * 3, v);
+#pragma unroll
+      for (int k = 0; k < NC; ++k) sF[w][h][i][k] = v[k];
+    }
+  }
+  __syncwarp();
+  // back to the elements: LEFT + Tb F (both halves of a subdivided edge), RIGHT - Tb F in its own order
+  real* const* outp = MODE == MORTAR_GRADIENT ? a.NFG : a.NF;
+  auto store = [&](int s, int i, const real* v, real sign) {
+    real* np = outp[f.part[s]] + (size_t(f.slot[s]) * f.P[s] + i) * NC;
+#pragma unroll
+    for (int k = 0; k < NC; ++k) np[k] = sign * v[k];
+  };
   if (f.kind == 0) {
     const int PE = f.PE[0];
-    if (lane < PE) {
-      real qL[4], qR[4], F[4];
-      project_row(a.mat, f.tf[0], f.P[0], lane, sT[w][0], qL);
-      project_row(a.mat, f.tf[1], f.P[1], f.inv ? PE - 1 - lane : lane, sT[w][1], qR);
-      face_flux(a.riemann, ph, qL, qR, a.geo + size_t(f.geo[0] + lane) * 3, F);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) sF[w][0][lane][k] = F[k];
-    }
-    __syncwarp();
-    // LEFT: FL = Tb F (or F); RIGHT: FR = -(Tb F) in its own node order
+    real out[NC];
     if (lane < f.P[0]) {
-      real out[4];
-      project_row(a.mat, f.tb[0], PE, lane, sF[w][0], out);
-      real* np = a.NF[f.part[0]] + (size_t(f.slot[0]) * f.P[0] + lane) * 4;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) np[k] = out[k];
+      project_row<NC, NC>(a.mat, f.tb[0], PE, lane, &sF[w][0][0][0], out);
+      store(0, lane, out, real(1));
     } else if (lane >= 16 && lane - 16 < f.P[1]) {
       const int j = lane - 16;
-      real out[4];
-      project_row(a.mat, f.tb[1], PE, f.inv ? f.P[1] - 1 - j : j, sF[w][0], out);
-      real* np = a.NF[f.part[1]] + (size_t(f.slot[1]) * f.P[1] + j) * 4;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) np[k] = -out[k];
+      project_row<NC, NC>(a.mat, f.tb[1], PE, f.inv ? f.P[1] - 1 - j : j, &sF[w][0][0][0], out);
+      store(1, j, out, real(-1));
     }
   } else {
-    // lanes 0-15: north half (LEFT against RIGHT_NORTH), lanes 16-31: south half
     const int h = lane >> 4, i = lane & 15;
-    if (i < f.PE[h]) {
-      real qL[4], qR[4], F[4];
-      project_row(a.mat, f.tf[h], f.P[0], i, sT[w][0], qL);
-      project_row(a.mat, f.tf[2 + h], f.P[1 + h], i, sT[w][1 + h], qR);
-      face_flux(a.riemann, ph, qL, qR, a.geo + size_t(f.geo[h] + i) * 3, F);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) sF[w][h][i][k] = F[k];
-    }
-    __syncwarp();
     if (h == 0 && i < f.P[0]) {
-      // LEFT collects both halves: FL = Tb_LN F_N + Tb_LS F_S
-      real acc[4] = {real(0), real(0), real(0), real(0)};
+      real acc[NC];
+#pragma unroll
+      for (int k = 0; k < NC; ++k) acc[k] = real(0);
       for (int hh = 0; hh < 2; ++hh) {
         const int cols = f.PE[hh];
         const real* row = a.mat + f.tb[hh] + size_t(i) * cols;
         for (int l = 0; l < cols; ++l) {
           const real t = row[l];
 #pragma unroll
-          for (int k = 0; k < 4; ++k) acc[k] = acc[k] + t * sF[w][hh][l][k];
+          for (int k = 0; k < NC; ++k) acc[k] = acc[k] + t * sF[w][hh][l][k];
         }
       }
-      real* np = a.NF[f.part[0]] + (size_t(f.slot[0]) * f.P[0] + i) * 4;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) np[k] = acc[k];
+      store(0, i, acc, real(1));
     } else if (h == 1) {
       for (int r = 0; r < 2; ++r) {
         if (i < f.P[1 + r]) {
-          real out[4];
-          project_row(a.mat, f.tb[2 + r], f.PE[r], i, sF[w][r], out);
-          real* np = a.NF[f.part[1 + r]] + (size_t(f.slot[1 + r]) * f.P[1 + r] + i) * 4;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) np[k] = -out[k];
+          real out[NC];
+          project_row<NC, NC>(a.mat, f.tb[2 + r], f.PE[r], i, &sF[w][r][0][0], out);
+          store(1 + r, i, out, real(-1));
         }
       }
     }
@@ -228,7 +269,7 @@ struct MatPool {
 
 }  // namespace
 
-void launch_mortar(hg_ctx* c) {
+void launch_mortar(hg_ctx* c, int mode) {
   if (c->n_mortar_faces == 0) return;
   const int grid = (c->n_mortar_faces + MW - 1) / MW;
   auto go = [&](auto tag) {
@@ -239,12 +280,20 @@ void launch_mortar(hg_ctx* c) {
     a.mat = static_cast<const real*>(c->d_mmat);
     a.geo = static_cast<const real*>(c->d_mgeo);
     for (size_t p = 0; p < c->parts.size(); ++p) {
-      a.T[p] = static_cast<const real*>(c->parts[p]->d_T[c->parts[p]->cur]);
-      a.NF[p] = static_cast<real*>(c->parts[p]->d_NF);
+      hg_ctx* q = c->parts[p];
+      a.T[p] = static_cast<const real*>(q->d_T[q->cur]);
+      a.GT[p] = static_cast<const real*>(q->d_GT);
+      a.NF[p] = static_cast<real*>(q->d_NF);
+      a.NFG[p] = static_cast<real*>(q->d_NFG);
     }
+    a.mode = mode;
+    a.visc = c->ns && c->pc.mu != 0.0;
     a.riemann = c->riemann;
     a.pc = c->pc;
-    timed(c, HG_KERNEL_MORTAR, [&] { mortar_kernel<real><<<grid, MW * 32, 0, c->stream>>>(a); });
+    timed(c, HG_KERNEL_MORTAR, [&] {
+      if (mode == MORTAR_GRADIENT) mortar_kernel<real, MORTAR_GRADIENT><<<grid, MW * 32, 0, c->stream>>>(a);
+      else mortar_kernel<real, MORTAR_FLUX><<<grid, MW * 32, 0, c->stream>>>(a);
+    });
   };
   if (c->precision == HG_PREC_FP32) go(float{});
   else go(double{});
@@ -263,13 +312,17 @@ void composite_free(hg_ctx* c) {
 }
 
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
-  if (ph->navier_stokes) throw std::runtime_error("mixed orders and subdivided edges are supported for the Euler build only");
+  if (ph->navier_stokes && (ph->viscous != 0 || ph->av_type != HG_AV_NONE))
+    throw std::runtime_error("mixed orders and subdivided edges in the Navier-Stokes build take BR1 without "
+                             "artificial dissipation");
   const int E = m->n_elements;
   if (E <= 0) throw std::runtime_error("mesh has no elements");
   c->el_N.assign(m->N, m->N + E);
+  const int max_order = ph->navier_stokes ? 8 : HG_MAX_ORDER_EULER;
   for (int e = 0; e < E; ++e)
-    if (c->el_N[e] < 1 || c->el_N[e] > HG_MAX_ORDER_EULER)
-      throw std::runtime_error("polynomial order must be in 1.." + std::to_string(HG_MAX_ORDER_EULER));
+    if (c->el_N[e] < 1 || c->el_N[e] > max_order)
+      throw std::runtime_error("polynomial order must be in 1.." + std::to_string(max_order) +
+                               (ph->navier_stokes ? " for the Navier-Stokes build" : ""));
   // parts: one per order, ascending; elements in mesh order within a part
   std::vector<int> orders(c->el_N);
   std::sort(orders.begin(), orders.end());
@@ -300,7 +353,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
   c->P = c->N + 1;
   c->node_type = ph->node_type;
   c->riemann = ph->riemann;
-  c->precision = c->precision;
+  c->ns = ph->navier_stokes != 0 && ph->reynolds != 0.0;
   const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
   c->gamma = gamma; c->mach = ph->mach;
   c->pc.gamma = gamma;
@@ -508,6 +561,10 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
     const size_t rs = c->precision == HG_PREC_FP32 ? sizeof(float) : sizeof(double);
     pc->d_NF = dalloc_n<char>(flux_sides[p].size() * Pp * 4 * rs);
     HG_CUDA(cudaMemset(pc->d_NF, 0, std::max<size_t>(flux_sides[p].size() * Pp * 4 * rs, 1)));
+    if (c->ns) {
+      pc->d_NFG = dalloc_n<char>(flux_sides[p].size() * Pp * 8 * rs);
+      HG_CUDA(cudaMemset(pc->d_NFG, 0, std::max<size_t>(flux_sides[p].size() * Pp * 8 * rs, 1)));
+    }
   }
   // per-element corner distances of the whole mesh (EstimateTimeStep runs over mesh order)
   c->dx.assign(E, 0.0);
@@ -517,6 +574,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
       auto d = [&](int a, int b) { return std::sqrt((v[2 * a] - v[2 * b]) * (v[2 * a] - v[2 * b]) + (v[2 * a + 1] - v[2 * b + 1]) * (v[2 * a + 1] - v[2 * b + 1])); };
       c->dx[e] = std::fmin(std::fmin(d(0, 1), d(1, 2)), std::fmin(d(2, 3), d(0, 3)));
     }
+  c->pc = c->parts[0]->pc;   // physics constants (the parts share them)
   HG_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   c->own_stream = true;
   for (hg_ctx* pc : c->parts) pc->stream = c->stream;

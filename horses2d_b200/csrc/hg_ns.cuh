@@ -37,6 +37,8 @@ struct NSArgs {
   const Zone* zones;
   const double* bq;         // per-node Dirichlet states [rows][P][4] (sides whose side.w >= 0)
   const real* FX;           // exact-solver face fluxes [n_el*4][P][4] of this stage (RIEMANN_EXACT faces)
+  const real* NF;           // mortar face fluxes [slots][P][4] of the SIDE_FLUX sides (stage kernel)
+  const real* NFG;          // mortar BR1 gradient face terms [slots][P][2][4] of the SIDE_FLUX sides
   double* Q;
   real* G;
   const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
@@ -45,6 +47,8 @@ struct NSArgs {
   real* dQ;                 // element gradients              [n_el][2][4][NP]
   int viscous;              // viscous fluxes present: mu != 0 or the Physical artificial viscosity
   int run_gradient;         // host side: whether this stage needs the gradient kernel
+  int run_stage;            // host side: whether to launch the stage kernel (a composite runs the
+                            // mortar fluxes between the parts' gradient and stage kernels)
   double* QDot;
   double* resid;
   double a, b, c;
@@ -132,6 +136,12 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
         const int sd_ = t / P, kk = t % P;
         const int4 sd = a.side[size_t(e) * 4 + sd_];
         const int kind = sd.y & 15;
+        if (kind == SIDE_FLUX) {   // p-nonconforming or subdivided edge: terms from the mortar kernel
+          const real* gp = a.NFG + (size_t(sd.x) * P + kk) * 8;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) s.face[k][le][t] = gp[k];
+          continue;
+        }
         const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
         real qo[4];
         trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
@@ -460,6 +470,15 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       const int sd_ = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + sd_];
       const int kind = sd.y & 15;
+      if (kind == SIDE_FLUX) {   // inviscid and viscous flux of the mortar kernel (BR1, no gradient-face terms)
+        const real* fp = a.NF + (size_t(sd.x) * P + kk) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s.face[k][le][t] = fp[k];
+        if (IP && a.grad_faces && visc)
+#pragma unroll
+          for (int k = 0; k < 4; ++k) { s.face[4 + k][le][t] = real(0); s.face[8 + k][le][t] = real(0); }
+        continue;
+      }
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
       real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
       trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);

@@ -84,8 +84,8 @@ typedef struct {
  * reference), stored one edge after the other.
  * Mixed orders and subdivided edges (p-nonconforming projections types 3-6 and
  * SubdividedEdge_t, Mesh/QuadElement_EdgeProcedures.incf:749-1345) are supported for
- * the Euler build (navier_stokes = 0), orders 1-12; the Navier-Stokes build takes one
- * order (1-8) and no mortars. */
+ * the Euler build, orders 1-12, and for the Navier-Stokes build with BR1 and without
+ * artificial dissipation, orders 1-8. */
 typedef struct {
   int32_t n_elements;
   int32_t n_edges;

@@ -171,3 +171,95 @@ def test_composite_monitors_and_restart(tmp_path):
     g.time_steps(hg.SCHEME_RK3, 2, 4e-3, 1e-3)
     h.time_steps(hg.SCHEME_RK3, 2, 4e-3, 1e-3)
     assert np.array_equal(g.state(), h.state())
+
+
+# ----------------------------------------------------------------------------- Navier-Stokes (BR1)
+def cylinder_re100_case(orders=(8, 2, 8, 6, 4)):
+    m = load_mesh("CylinderBench")
+    porder = np.array(orders)[m["p_zones"]]
+    ex = O.EXACT
+    bcs = [dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_DIRICHLET, riemann=ex),
+           dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2, riemann=ex),
+           dict(type=O.BC_VISCOUSWALL, wall_type=2, riemann=ex)]
+    orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.HLL, mach=0.1, reynolds=100.0, prandtl=0.72, navier_stokes=1,
+                   viscous=O.BR1, bcs=bcs)
+    r = orc.ref
+    cv = 287.15 * 2.5
+    q = np.array([r["rho"], r["rho"] * r["V"], 0.0, cv * r["rho"] * r["T"] + 0.5 * r["rho"] * r["V"] * r["V"]])
+    q = q / np.array([r["rho"], r["rho"] * r["a"], r["rho"] * r["a"], r["p"]])
+    ge = hg.EXACT
+    zq = [orc.zone_state(z) for z in range(1, 5)]
+    gbcs = [dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[0]), dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[1]),
+            dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[2]),
+            dict(type=hg.BC_PRESSUREOUTLET, outflow_type=2, riemann=ge, state=zq[3]),
+            dict(type=hg.BC_VISCOUSWALL, wall_type=2, riemann=ge)]
+    kw = dict(mach=0.1, reynolds=100.0, prandtl=0.72, navier_stokes=1, viscous=hg.BR1, node_type=hg.NODES_LG,
+              riemann=hg.HLL, bcs=gbcs)
+    return orc, q, kw
+
+
+def test_ns_p_nonconforming_residual():
+    """CylinderRe100 mesh, orders 2-8 by zone (112 edges between orders), BR1, HLL, exact solver on
+    the zones: residual of a perturbed state and RK5 steps."""
+    orc, q, kw = cylinder_re100_case()
+    Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=31)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g = hg.GpuDGSEM(orc.export_mesh(), **kw)
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= TOL_STAGE
+    dt = orc.estimate_dt(0.1, 1e-2)    # the benchmark's CFL (order 8 elements near the wall)
+    for k in range(4):
+        orc.time_step(O.RK5, k * dt, dt)
+    g.time_steps(hg.SCHEME_RK5, 4, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_STEPS
+
+
+def test_ns_subdivided_edges_residual():
+    """Couette mesh (curved, 34 subdivided edges) in the Navier-Stokes build with BR1 and isothermal
+    walls, orders 5/7/8 by zone (the benchmark's order 10 zone capped at the Navier-Stokes kernels' 8)."""
+    from test_oracle import couette_state
+    m = load_mesh("CouetteBench")
+    porder = np.array([5, 7, 8, 7])[m["p_zones"]]
+    bcs = [dict(type=O.BC_VISCOUSWALL, wall_type=1),
+           dict(type=O.BC_VISCOUSWALL, wall_type=1, wall_v=(np.sqrt(1.4) * 0.8, 0.0)),
+           dict(type=O.BC_DIRICHLET), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2)]
+    orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.ROE, mach=0.8, reynolds=2000.0, prandtl=0.72,
+                   navier_stokes=1, viscous=O.BR1, bcs=bcs)
+    ref = orc.ref
+    scale = np.array([ref["rho"], ref["rho"] * ref["a"], ref["rho"] * ref["a"], ref["p"]])
+    X = orc.coords()
+    Q = perturbed((couette_state(X[:, 0], X[:, 1], ref) / scale).ravel(), 0.01, seed=32)
+    Xb = orc.zone_edge_nodes(3)
+    uB = (couette_state(Xb[:, 0], Xb[:, 1], ref) / scale).ravel()
+    orc.set_zone_state(3, uB)
+    orc.set_state(Q)
+    qd = orc.time_derivative(0.0)
+    gbcs = [dict(type=hg.BC_VISCOUSWALL, wall_type=1, wall_T=1.0),
+            dict(type=hg.BC_VISCOUSWALL, wall_type=1, wall_T=1.0, wall_v=(np.sqrt(1.4) * 0.8, 0.0)),
+            dict(type=hg.BC_DIRICHLET, state=orc.zone_state(3)),
+            dict(type=hg.BC_PRESSUREOUTLET, outflow_type=2, state=orc.zone_state(4))]
+    g = hg.GpuDGSEM(orc.export_mesh(), mach=0.8, reynolds=2000.0, prandtl=0.72, navier_stokes=1, viscous=hg.BR1,
+                    node_type=hg.NODES_LG, riemann=hg.ROE, bcs=gbcs)
+    g.set_boundary_state(3, uB)
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), qd) <= TOL_STAGE
+
+
+def test_cylinder_re100_benchmark_golden():
+    """The reference's CylinderRe100 regression on the device: 250 steady RK5 iterations (CFL 0.1, dt
+    cap 1e-2) on the p-refined cylinder mesh; final residuals and the wall's lift and drag."""
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["CylinderRe100"]
+    orc, q, kw = cylinder_re100_case()
+    g = hg.GpuDGSEM(orc.export_mesh(), **kw)
+    g.set_state(np.tile(q, orc.ndof // 4))
+    it, _ = g.integrate(hg.SCHEME_RK5, transient=False, t0=0.0, t_end=1e9, max_iter=250, cfl=0.1, dt_cap=1e-2,
+                        residual_target=1e-14)
+    assert it == 250
+    np.testing.assert_allclose(g.residuals(), golden["residuals"], rtol=1e-9)
+    r = orc.ref
+    si = g.surface_integrals(5)
+    dyn = 0.5 * r["rho"] * r["V"] * r["V"] * 1.0
+    force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
+    assert abs(force[1] / dyn - golden["cl"]) <= 1e-12
+    assert abs(force[0] / dyn - golden["cd"]) <= 5e-8
