@@ -33,6 +33,9 @@ Workloads (synthetic inputs with the configurations' shapes; seeds fixed):
              perturbation of amplitude 1e-2, SIPG (sigma0 10), Roe, Laplacian artificial viscosity
              driven by the learned sensor (trained as for `shock`; out-of-distribution elements use
              the modal indicator); FP32 bulk + learned beside FP64 + modal.  --kh-n sets the size.
+  prefine  : p-refined periodic vortex box (as the reference's VortexTransport p-zones): 384 x 384
+             elements on [-5,5]^2, N = 7 in the central 192 x 192 square and N = 5 around it
+             (edges between the two orders through the mortar kernel), Legendre-Gauss, Roe, FP64.
 Multi-GPU: independent replicas (the workload does not exchange data), weak scaling.
 """
 import argparse
@@ -52,7 +55,7 @@ sys.path.insert(0, ROOT)
 SEED = 20261203
 L2_BYTES = 126 * 2 ** 20
 KH_DT_COEF = 0.05   # kh workload: dt = 0.05 / n^2 (half the measured interior-penalty stability limit)
-CONFIGS = ("cylinder", "vortex16", "ensemble", "box512", "shock", "kh")
+CONFIGS = ("cylinder", "vortex16", "ensemble", "box512", "shock", "kh", "prefine")
 
 
 def peaks():
@@ -92,10 +95,25 @@ def cylinder_state(n_nodes, seed=SEED):
     return (np.tile(freestream(0.2), n_nodes) + 1e-3 * rng.standard_normal(4 * n_nodes))
 
 
+def prefine_orders(n):
+    """Orders of the p-refined box: 7 in the central n/2 x n/2 square, 5 elsewhere (row-major)."""
+    i = np.tile(np.arange(n), n)
+    j = np.repeat(np.arange(n), n)
+    inner = (i >= n // 4) & (i < n - n // 4) & (j >= n // 4) & (j < n - n // 4)
+    return np.where(inner, 7, 5).astype(np.int32)
+
+
 def build_parts(config):
     """[(descriptor, Q0, N, n_instances, solver kwargs, cfl)] -- one GPU context each."""
     from horses2d_b200 import mesh as hmesh, cases
     import horses2d_b200 as hg
+    if config == "prefine":
+        n = 384
+        desc = hmesh.box_descriptor(n, n, -5.0, 5.0, -5.0, 5.0, prefine_orders(n), hg.NODES_LG)
+        x = desc["x"].reshape(-1, 2)
+        Q0 = cases.isentropic_vortex(x[:, 0], x[:, 1], mach=0.5, beta=5.0).ravel()
+        kw = dict(mach=0.5, node_type=hg.NODES_LG, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+        return [(desc, Q0, "5/7", 1, kw, 0.4)]
     if config == "cylinder":
         N = 5
         desc = hmesh.build_descriptor(cylinder_mesh(), N, hg.NODES_LG)
@@ -253,6 +271,17 @@ class CpuArm:
                          bcs=[dict(type=O.BC_VISCOUSWALL, wall_type=2), dict(type=O.BC_FARFIELD)])
             o.set_state(cylinder_state(o.ndof // 4))
             self.orcs = [(o, o.estimate_dt(0.05, 1.0))]
+            return
+        if config == "prefine":
+            # bounded sample: one 48 x 48 box with the same order layout per host thread
+            self.inst = [dict(n=48, N="5/7")] * self.threads
+            self.orcs = []
+            for _ in self.inst:
+                o = O.Oracle(hmesh.cartesian(48, 48, -5.0, 5.0, -5.0, 5.0), prefine_orders(48), nodes=O.LG,
+                             riemann=O.ROE, mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
+                X = o.coords()
+                o.set_state(cases.isentropic_vortex(X[:, 0], X[:, 1], mach=0.5, beta=5.0).ravel())
+                self.orcs.append((o, o.estimate_dt(0.4, 1.0)))
             return
         inst = ensemble_spec() if config == "ensemble" else [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
         if config == "box512":
@@ -729,7 +758,9 @@ def main():
     # ---- roofline of the dominant kernel (fused stage kernel), from its own event times
     bpd = stage_bytes_per_dof(args.config, prec == hg.PREC_FP32, affine, ns)
     st_ms, st_n = split["stage"]
-    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
+    # one stage of a mixed-order context is one launch per order part (the parts share the bytes)
+    parts_per_stage = 2 if args.config == "prefine" else 1
+    avg_stage_s = st_ms * 1e-3 / max(st_n, 1) * parts_per_stage
     stage_launch_bytes = bpd * ndof / len(ctxs)
     achieved = stage_launch_bytes / avg_stage_s / 1e9
     peak, peak_kind = peaks()

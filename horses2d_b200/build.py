@@ -16,7 +16,7 @@ OUT = os.path.join(HERE, "libhorsesgpu.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu", "csrc/hg_mlp.cu", "csrc/hg_exact.cu", "csrc/hg_monitors.cu",
            "csrc/hg_mesh.cpp", "csrc/hg_restart.cpp", "csrc/hg_mortar.cu",
-           "csrc/hg_inst_euler_hi.cu", "csrc/hg_inst_euler_hi_t1.cu",
+           "csrc/hg_inst_euler_hi.cu", "csrc/hg_inst_euler_hi_t1.cu", "csrc/hg_inst_ns_hi.cu",
            "csrc/hg_inst_euler.cu", "csrc/hg_inst_euler_t1.cu",
            "csrc/hg_inst_sensor.cu"] + \
     [f"csrc/hg_inst_ns{prec}{part}{t}.cu" for t in ("", "_t1") for prec in ("64", "32") for part in "abcd"]

@@ -99,9 +99,26 @@ static void run_trace(hg_ctx* c) { HG_DISPATCH_P_EULER(c->P, launch_trace_P, c);
 
 template <int P, typename real>
 static void ns_dispatch(hg_ctx* c, const NSArgs<real>& a) {
-  if (c->tiling) launch_ns_PV<P, real, 1>(c, a);
+  // orders 9-10 run one element per CTA in both tilings: one instantiation serves
+  if (c->tiling && P < 10) launch_ns_PV<P, real, 1>(c, a);
   else launch_ns_PV<P, real, 0>(c, a);
 }
+
+// Navier-Stokes kernels: orders 1-8, 9 and 10
+#define HG_DISPATCH_P_NS(P_, FN, ...)                   \
+  switch (P_) {                                         \
+    case 2: FN<2, real>(__VA_ARGS__); break;            \
+    case 3: FN<3, real>(__VA_ARGS__); break;            \
+    case 4: FN<4, real>(__VA_ARGS__); break;            \
+    case 5: FN<5, real>(__VA_ARGS__); break;            \
+    case 6: FN<6, real>(__VA_ARGS__); break;            \
+    case 7: FN<7, real>(__VA_ARGS__); break;            \
+    case 8: FN<8, real>(__VA_ARGS__); break;            \
+    case 9: FN<9, real>(__VA_ARGS__); break;            \
+    case 10: FN<10, real>(__VA_ARGS__); break;          \
+    case 11: FN<11, real>(__VA_ARGS__); break;          \
+    default: throw std::runtime_error("unsupported polynomial order"); \
+  }
 template <int P, typename real>
 static void stage_dispatch(hg_ctx* c, const StageArgs<real>& a) {
   if (c->tiling) launch_stage_PV<P, real, 1>(c, a);
@@ -153,7 +170,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.run_stage = c->ns_phase != 1;
   if (c->ns_phase == 2) a.run_gradient = 0;
   if (c->exact && a.run_stage) launch_exact_flux<real>(c);
-  HG_DISPATCH_P(c->P, ns_dispatch, c, a);
+  HG_DISPATCH_P_NS(c->P, ns_dispatch, c, a);
   if (!a.run_stage) return;
   c->last_T = c->cur;   // trace buffer of the state this stage evaluated (surface integrals read it)
   if (update) c->cur ^= 1;
@@ -279,8 +296,8 @@ void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, cons
   const int N = m->N[0];
   for (int e = 0; e < E; ++e)
     if (m->N[e] != N) throw std::runtime_error("mixed polynomial orders are not supported by this kernel set");
-  if (ph->navier_stokes ? (N < 1 || N > 8) : (N < 1 || N > HG_MAX_ORDER_EULER))
-    throw std::runtime_error(ph->navier_stokes ? "polynomial order must be in 1..8 for the Navier-Stokes build"
+  if (ph->navier_stokes ? (N < 1 || N > HG_MAX_ORDER_NS) : (N < 1 || N > HG_MAX_ORDER_EULER))
+    throw std::runtime_error(ph->navier_stokes ? "polynomial order must be in 1..10 for the Navier-Stokes build"
                                                : "polynomial order must be in 1..12");
   if (m->n_mortars > 0) throw std::runtime_error("subdivided edges need the composite context");
   const int P = N + 1, NP = P * P;

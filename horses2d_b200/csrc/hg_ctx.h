@@ -159,6 +159,7 @@ void launch_mortar(hg_ctx* c, int mode);
 inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
 constexpr int HG_MAX_PARTS = 12;
 constexpr int HG_MAX_ORDER_EULER = 12;
+constexpr int HG_MAX_ORDER_NS = 10;
 
 // Per-order launches, explicitly instantiated in hg_inst_*.cu (V = tiling variant: 0 in the plain
 // units, 1 in the *_t1 units).

@@ -318,7 +318,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
   const int E = m->n_elements;
   if (E <= 0) throw std::runtime_error("mesh has no elements");
   c->el_N.assign(m->N, m->N + E);
-  const int max_order = ph->navier_stokes ? 8 : HG_MAX_ORDER_EULER;
+  const int max_order = ph->navier_stokes ? HG_MAX_ORDER_NS : HG_MAX_ORDER_EULER;
   for (int e = 0; e < E; ++e)
     if (c->el_N[e] < 1 || c->el_N[e] > max_order)
       throw std::runtime_error("polynomial order must be in 1.." + std::to_string(max_order) +

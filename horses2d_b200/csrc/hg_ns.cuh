@@ -65,7 +65,7 @@ struct NSArgs {
 };
 
 __host__ __device__ constexpr int epb_ns(int P) {
-  return P == 2 ? 16 : P == 3 ? 7 : P == 4 ? 8 : P == 5 ? 5 : P == 6 ? 4 : P == 7 ? 3 : 2;
+  return P == 2 ? 16 : P == 3 ? 7 : P == 4 ? 8 : P == 5 ? 5 : P == 6 ? 4 : P == 7 ? 3 : P <= 9 ? 2 : 1;
 }
 __host__ __device__ constexpr int epb_ns_small(int P) {
   return P == 2 ? 4 : P <= 6 ? 2 : 1;

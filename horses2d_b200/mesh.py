@@ -42,36 +42,46 @@ def box_descriptor(nx, ny, x0, x1, y0, y1, N, node_type, *, elem_offset=0, edge_
     owns it, sides are numbered EBOTTOM=1, ERIGHT=2, ETOP=3, ELEFT=4, and the
     bottom/top and left/right boundary edges are periodic partners (markers
     1/2 and 3/4).  Element e = j*nx + i (row-major, as ``cartesian``).
+    ``N``: one order, or one per element (p-refinement): an edge then carries
+    max(N_L, N_R) + 1 nodes, the reference's edge order; periodic partners must
+    share an order.
     """
     from ._lib import nodes as lib_nodes
-    P = N + 1
-    xi, _ = lib_nodes(N, node_type)
     hx, hy = (x1 - x0) / nx, (y1 - y0) / ny
     E = nx * ny
+    Ne = np.broadcast_to(np.asarray(N, np.int32), (E,)).astype(np.int32)
+    Pe = Ne + 1
     i = np.tile(np.arange(nx), ny)
     j = np.repeat(np.arange(ny), nx)
     ex0 = x0 + i * hx
     ey0 = y0 + j * hy
-    # nodes in (eta, xi) order
-    XI, ETA = np.meshgrid(xi, xi)                       # [eta][xi]
-    xn = ex0[:, None] + hx * XI.ravel()[None, :]
-    yn = ey0[:, None] + hy * ETA.ravel()[None, :]
+    # nodes in (eta, xi) order, elements one after the other (Storage%Q offsets)
+    n0 = np.concatenate([[0], np.cumsum(Pe * Pe)])
+    nodes = int(n0[-1])
+    xn, yn = np.empty(nodes), np.empty(nodes)
+    for Nk in np.unique(Ne):
+        xi, _ = lib_nodes(int(Nk), node_type)
+        XI, ETA = np.meshgrid(xi, xi)                   # [eta][xi]
+        el = np.nonzero(Ne == Nk)[0]
+        idx = (n0[el][:, None] + np.arange((Nk + 1) ** 2)[None, :]).ravel()
+        xn[idx] = (ex0[el][:, None] + hx * XI.ravel()[None, :]).ravel()
+        yn[idx] = (ey0[el][:, None] + hy * ETA.ravel()[None, :]).ravel()
     x = np.stack([xn, yn], -1).reshape(-1)
-    Ja = np.zeros((E, P * P, 4))
-    Ja[:, :, 0] = hy
-    Ja[:, :, 3] = hx
-    jac = np.full(E * P * P, hx * hy)
+    Ja = np.zeros((nodes, 4))
+    Ja[:, 0] = hy
+    Ja[:, 3] = hx
+    jac = np.full(nodes, hx * hy)
     verts = np.stack([np.stack([ex0, ey0], 1), np.stack([ex0 + hx, ey0], 1), np.stack([ex0 + hx, ey0 + hy], 1),
                       np.stack([ex0, ey0 + hy], 1)], 1).reshape(-1)
     eid = (j * nx + i).reshape(ny, nx) + elem_offset
-    edges_elem, edges_side, marker, nrm, dS, partner = [], [], [], [], [], []
+    edges_elem, edges_side, marker, nrm, dS = [], [], [], [], []
 
     def add(L, sL, R, sR, n_, d_, mk):
         edges_elem.append(np.stack([L, R], 1))
         edges_side.append(np.stack([np.full_like(L, sL), np.full_like(L, sR)], 1))
         marker.append(np.full(L.shape, mk))
-        nrm.append(np.tile(np.asarray(n_, float), (L.size, P, 1)))
-        dS.append(np.full((L.size, P), d_))
+        nrm.append(np.tile(np.asarray(n_, float), (L.size, 1)))
+        dS.append(np.full(L.size, d_))
 
     none = lambda a: np.full_like(a, -1)   # noqa: E731
     # interior vertical edges: LEFT (i, j) side ERIGHT, RIGHT (i+1, j) side ELEFT, normal +x
@@ -93,14 +103,18 @@ def box_descriptor(nx, ny, x0, x1, y0, y1, N, node_type, *, elem_offset=0, edge_
     partner[o:o + ny] = np.arange(o + ny, o + 2 * ny) + edge_offset
     partner[o + ny:o + 2 * ny] = np.arange(o, o + ny) + edge_offset
     ee = np.concatenate(edges_elem)
+    # nodes per edge: the higher order of its elements
+    loc = ee - elem_offset
+    PEd = np.where(loc[:, 1] >= 0, np.maximum(Pe[loc[:, 0]], Pe[np.maximum(loc[:, 1], 0)]), Pe[loc[:, 0]])
     # invh = Area / min(adjacent volumes) (QuadMesh_Construct.incf:270-303): 1/hx across x, 1/hy across y
     invh = np.concatenate([np.full(ny * (nx - 1), 1.0 / hx), np.full(nx * (ny - 1), 1.0 / hy),
                            np.full(2 * nx, 1.0 / hy), np.full(2 * ny, 1.0 / hx)])
-    return dict(N=np.full(E, N, np.int32), Ja=Ja.reshape(-1), jac=jac, x=x, volume=np.full(E, hx * hy),
+    return dict(N=Ne.copy(), Ja=Ja.reshape(-1), jac=jac, x=x, volume=np.full(E, hx * hy),
                 vertices=verts, edge_elem=ee.reshape(-1).astype(np.int32),
                 edge_side=np.concatenate(edges_side).reshape(-1).astype(np.int32),
                 edge_inverse=np.zeros(F, np.int32), edge_marker=np.concatenate(marker).astype(np.int32),
-                edge_n=np.concatenate(nrm).reshape(-1), edge_dS=np.concatenate(dS).reshape(-1),
+                edge_n=np.repeat(np.concatenate(nrm), PEd, axis=0).reshape(-1),
+                edge_dS=np.repeat(np.concatenate(dS), PEd),
                 periodic_partner=partner.astype(np.int32),
                 edge_invh=invh)
 

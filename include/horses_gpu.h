@@ -84,8 +84,8 @@ typedef struct {
  * reference), stored one edge after the other.
  * Mixed orders and subdivided edges (p-nonconforming projections types 3-6 and
  * SubdividedEdge_t, Mesh/QuadElement_EdgeProcedures.incf:749-1345) are supported for
- * the Euler build, orders 1-12, and for the Navier-Stokes build with BR1 and without
- * artificial dissipation, orders 1-8. */
+ * the Euler build, and for the Navier-Stokes build with BR1 and without artificial
+ * dissipation.  Orders: 1-12 (Euler build), 1-10 (Navier-Stokes build). */
 typedef struct {
   int32_t n_elements;
   int32_t n_edges;

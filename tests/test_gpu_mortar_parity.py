@@ -215,12 +215,13 @@ def test_ns_p_nonconforming_residual():
     assert rel_l2(g.state(), orc.state()) <= TOL_STEPS
 
 
-def test_ns_subdivided_edges_residual():
-    """Couette mesh (curved, 34 subdivided edges) in the Navier-Stokes build with BR1 and isothermal
-    walls, orders 5/7/8 by zone (the benchmark's order 10 zone capped at the Navier-Stokes kernels' 8)."""
+def couette_case():
+    """The Couette benchmark's set-up (TestCases/Benchmark/Simulations/Couette): curved mesh with 34
+    subdivided edges, orders 5/7/10/7 by zone, BR1, Roe, isothermal walls (one moving), a Dirichlet
+    zone fed by the plugin's boundary-condition function, a partially non-reflective outlet."""
     from test_oracle import couette_state
     m = load_mesh("CouetteBench")
-    porder = np.array([5, 7, 8, 7])[m["p_zones"]]
+    porder = np.array([5, 7, 10, 7])[m["p_zones"]]
     bcs = [dict(type=O.BC_VISCOUSWALL, wall_type=1),
            dict(type=O.BC_VISCOUSWALL, wall_type=1, wall_v=(np.sqrt(1.4) * 0.8, 0.0)),
            dict(type=O.BC_DIRICHLET), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2)]
@@ -233,8 +234,8 @@ def test_ns_subdivided_edges_residual():
     Xb = orc.zone_edge_nodes(3)
     uB = (couette_state(Xb[:, 0], Xb[:, 1], ref) / scale).ravel()
     orc.set_zone_state(3, uB)
-    orc.set_state(Q)
-    qd = orc.time_derivative(0.0)
+    q0 = couette_state(X[:, 0], X[:, 1], ref)
+    q0[X[:, 0] ** 2 + X[:, 1] ** 2 < 0.005, 1] *= 1.005
     gbcs = [dict(type=hg.BC_VISCOUSWALL, wall_type=1, wall_T=1.0),
             dict(type=hg.BC_VISCOUSWALL, wall_type=1, wall_T=1.0, wall_v=(np.sqrt(1.4) * 0.8, 0.0)),
             dict(type=hg.BC_DIRICHLET, state=orc.zone_state(3)),
@@ -242,8 +243,33 @@ def test_ns_subdivided_edges_residual():
     g = hg.GpuDGSEM(orc.export_mesh(), mach=0.8, reynolds=2000.0, prandtl=0.72, navier_stokes=1, viscous=hg.BR1,
                     node_type=hg.NODES_LG, riemann=hg.ROE, bcs=gbcs)
     g.set_boundary_state(3, uB)
+    return orc, g, Q, (q0 / scale).ravel()
+
+
+def test_ns_subdivided_edges_residual():
+    orc, g, Q, _ = couette_case()
+    orc.set_state(Q)
+    qd = orc.time_derivative(0.0)
     g.set_state(Q)
     assert rel_l2(g.compute_time_derivative(0.0), qd) <= TOL_STAGE
+    dt = orc.estimate_dt(0.4, 1.0)
+    for k in range(4):
+        orc.time_step(O.RK5, k * dt, dt)
+    g.time_steps(hg.SCHEME_RK5, 4, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_STEPS
+
+
+def test_couette_benchmark_golden():
+    """The reference's Couette regression on the device: steady RK5 at CFL 0.4 until the largest
+    residual drops below 1e-4; the reference asserts iteration 19585 and the four final residuals
+    (to 1e-12)."""
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["Couette"]
+    _, g, _, Q0 = couette_case()
+    g.set_state(Q0)
+    it, _ = g.integrate(hg.SCHEME_RK5, transient=False, t0=0.0, t_end=1.0, max_iter=100000, cfl=0.4, dt_cap=1.0,
+                        residual_target=1e-4)
+    assert it == golden["expected_iter"]
+    assert np.max(np.abs(g.residuals() - np.array(golden["expectedResiduals"]))) <= 1e-12
 
 
 def test_cylinder_re100_benchmark_golden():

@@ -9,11 +9,15 @@ from horses2d_b200 import mesh as hmesh, lib
 def side_table(d):
     """Per element-side view of an edge-centric descriptor: neighbour, orientation, normals, dS."""
     E = len(d["N"])
-    P = int(d["N"][0]) + 1
     F = len(d["edge_marker"])
     tab = {}
-    n = d["edge_n"].reshape(F, P, 2)
-    dS = d["edge_dS"].reshape(F, P)
+    # nodes per edge: the higher order of its elements
+    ee = np.asarray(d["edge_elem"]).reshape(-1, 2)
+    PE = np.where(ee[:, 1] >= 0, np.maximum(d["N"][ee[:, 0]], d["N"][np.maximum(ee[:, 1], 0)]), d["N"][ee[:, 0]]) + 1
+    off = np.concatenate([[0], np.cumsum(PE)])
+    assert off[-1] * 2 == len(d["edge_n"]) and off[-1] == len(d["edge_dS"])
+    n = [d["edge_n"][2 * off[f]:2 * off[f + 1]].reshape(-1, 2) for f in range(F)]
+    dS = [d["edge_dS"][off[f]:off[f + 1]] for f in range(F)]
     for f in range(F):
         L, R = d["edge_elem"][2 * f], d["edge_elem"][2 * f + 1]
         sL, sR = d["edge_side"][2 * f], d["edge_side"][2 * f + 1]
@@ -29,9 +33,11 @@ def side_table(d):
     return tab
 
 
-@pytest.mark.parametrize("nodes,N", [(O.LGL, 4), (O.LG, 3)])
+@pytest.mark.parametrize("nodes,N", [(O.LGL, 4), (O.LG, 3), (O.LG, "mixed"), (O.LGL, "mixed")])
 def test_box_descriptor_matches_reference_construction(nodes, N):
     nx, ny = 5, 4
+    if isinstance(N, str):   # a p-refined band (orders 3 / 5), periodic partners sharing an order
+        N = np.where(np.tile(np.arange(nx), ny) % 2 == 1, 5, 3).astype(np.int32)
     m = hmesh.cartesian(nx, ny, -5.0, 5.0, -2.0, 3.0)
     orc = O.Oracle(m, N, nodes=nodes, bcs=hmesh.periodic_bcs_cartesian())
     ref = orc.export_mesh()
