@@ -35,7 +35,8 @@ Workloads (synthetic inputs with the configurations' shapes; seeds fixed):
              the modal indicator); FP32 bulk + learned beside FP64 + modal.  --kh-n sets the size.
   prefine  : p-refined periodic vortex box (as the reference's VortexTransport p-zones): 384 x 384
              elements on [-5,5]^2, N = 7 in the central 192 x 192 square and N = 5 around it
-             (edges between the two orders through the mortar kernel), Legendre-Gauss, Roe, FP64.
+             (edges between the two orders through the mortar kernel), Legendre-Gauss, Roe, FP64,
+             CFL 0.3 (with Legendre-Gauss nodes RK3 at CFL 0.4 is unstable, for the oracle as for the kernels).
 Multi-GPU: independent replicas (the workload does not exchange data), weak scaling.
 """
 import argparse
@@ -113,7 +114,7 @@ def build_parts(config):
         x = desc["x"].reshape(-1, 2)
         Q0 = cases.isentropic_vortex(x[:, 0], x[:, 1], mach=0.5, beta=5.0).ravel()
         kw = dict(mach=0.5, node_type=hg.NODES_LG, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
-        return [(desc, Q0, "5/7", 1, kw, 0.4)]
+        return [(desc, Q0, "5/7", 1, kw, 0.3)]
     if config == "cylinder":
         N = 5
         desc = hmesh.build_descriptor(cylinder_mesh(), N, hg.NODES_LG)
@@ -281,7 +282,7 @@ class CpuArm:
                              riemann=O.ROE, mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
                 X = o.coords()
                 o.set_state(cases.isentropic_vortex(X[:, 0], X[:, 1], mach=0.5, beta=5.0).ravel())
-                self.orcs.append((o, o.estimate_dt(0.4, 1.0)))
+                self.orcs.append((o, o.estimate_dt(0.3, 1.0)))
             return
         inst = ensemble_spec() if config == "ensemble" else [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
         if config == "box512":
