@@ -56,7 +56,8 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
             "hg_autotune", "hg_set_tiling", "hg_get_tiling", "hg_group_create", "hg_group_destroy",
             "hg_group_time_steps", "hg_group_last_error", "hg_surface_integrals", "hg_probes",
             "hg_mesh_connectivity", "hg_mesh_last_error", "hg_write_restart", "hg_read_restart",
-            "hg_save_restart", "hg_load_restart", "hg_restart_last_error")
+            "hg_save_restart", "hg_load_restart", "hg_restart_last_error", "hg_save_restart_async",
+            "hg_restart_wait")
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
@@ -117,6 +118,8 @@ def load():
     L.hg_load_restart.argtypes = [vp, C.c_char_p, F64P, I32P]
     L.hg_restart_last_error.argtypes = []
     L.hg_restart_last_error.restype = C.c_char_p
+    L.hg_save_restart_async.argtypes = [vp, C.c_char_p, C.c_double, C.c_int32]
+    L.hg_restart_wait.argtypes = [vp]
     L.hg_set_tiling.argtypes = [vp, C.c_int32]
     L.hg_get_tiling.argtypes = [vp, I32P]
     L.hg_group_create.argtypes = [C.POINTER(vp), C.c_int32, C.POINTER(vp)]

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "libhorsesgpu.so")
 OBJ_DIR = os.path.join(HERE, "_build")
 SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu", "csrc/hg_mlp.cu", "csrc/hg_exact.cu", "csrc/hg_monitors.cu",
-           "csrc/hg_mesh.cpp", "csrc/hg_restart.cpp", "csrc/hg_mortar.cu",
+           "csrc/hg_mesh.cpp", "csrc/hg_restart.cpp", "csrc/hg_mortar.cu", "csrc/hg_autosave.cu",
            "csrc/hg_inst_euler_hi.cu", "csrc/hg_inst_euler_hi_t1.cu", "csrc/hg_inst_ns_hi.cu",
            "csrc/hg_inst_euler.cu", "csrc/hg_inst_euler_t1.cu",
            "csrc/hg_inst_sensor.cu"] + \

@@ -570,6 +570,7 @@ extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, 
 
 extern "C" void hg_destroy(hg_ctx* c) {
   if (!c) return;
+  autosave_finish(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   ctx_free(c);
   delete c;

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
+#include <memory>
 #include <stdexcept>
 
 using namespace hg;
@@ -89,6 +90,8 @@ struct hg_ctx {
   int64_t gen = 0;                // bumped whenever captured launches go stale (context groups check it)
   double g_dt = 0.0;
   int64_t g_launches[2] = {0, 0};
+  // asynchronous restart files (hg_save_restart_async): pinned copy of the state, written by a host thread
+  std::shared_ptr<struct AutosaveJob> autosave;
   // per-kernel timing (hg_profile): event pairs recorded around each launch
   bool prof = false;
   std::vector<cudaEvent_t> prof_pool;
@@ -147,7 +150,8 @@ inline void max_carveout(K kernel) {
                                int(cudaSharedmemCarveoutMaxShared)));
 }
 
-// Shared between hg_api.cu and hg_mortar.cu.
+// Shared between hg_api.cu, hg_mortar.cu and hg_autosave.cu.
+void autosave_finish(hg_ctx* c);   // waits for an asynchronous restart write (hg_destroy calls it)
 void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs,
                const std::vector<int2>* flux_sides);
 void ctx_free(hg_ctx* c);

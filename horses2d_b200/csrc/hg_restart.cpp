@@ -17,7 +17,7 @@
 
 namespace {
 
-std::string g_restart_err;
+thread_local std::string g_restart_err;   // per thread: asynchronous writes report on their own thread
 
 enum : uint32_t { NC_DIMENSION = 10, NC_VARIABLE = 11, NC_ATTRIBUTE = 12, NC_INT = 4, NC_DOUBLE = 6 };
 

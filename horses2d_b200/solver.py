@@ -196,22 +196,33 @@ class GpuDGSEM:
                 break
             if autosave_interval > 0 and solution_file and it % autosave_interval == 0:
                 flush()
-                self.save_restart(restart.autosave_name(solution_file, it), t, it)
+                self.save_restart(restart.autosave_name(solution_file, it), t, it, wait=False)
             if it % estimate_interval == 0:
                 flush()
                 dt = self.estimate_time_step(cfl, dt_cap)
             if not transient and np.max(np.abs(self.residuals())) < residual_target:
                 break
         flush()
+        self.restart_wait()
         if solution_file:
             self.save_restart(solution_file, t, it)
         return it, t
 
     # --- restart files (*.HiORst) --------------------------------------------
-    def save_restart(self, path, t, iteration):
-        """The resident state, t and iter to a restart file (TimeIntegrator_Autosave)."""
+    def save_restart(self, path, t, iteration, wait=True):
+        """The resident state, t and iter to a restart file (TimeIntegrator_Autosave).  wait=False
+        returns at once: the state is copied on the stream and a host thread writes the file while
+        stepping goes on (restart_wait() or the next save waits for it)."""
+        if not wait:
+            self._check(self._lib.hg_save_restart_async(self._h, os.fsencode(path), float(t), int(iteration)))
+            return
+        self._check(self._lib.hg_restart_wait(self._h))
         if self._lib.hg_save_restart(self._h, os.fsencode(path), float(t), int(iteration)) != 0:
             raise OSError(self._lib.hg_restart_last_error().decode())
+
+    def restart_wait(self):
+        """Wait for an asynchronous restart write; raises its error, if any."""
+        self._check(self._lib.hg_restart_wait(self._h))
 
     def load_restart(self, path):
         """A restart file into the resident state (DGSEM_loadRestartFile); returns (t, iter)."""

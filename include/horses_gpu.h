@@ -294,6 +294,12 @@ int  hg_read_restart(const char* path, double* t, int32_t* iter, double* Q, int6
 int  hg_save_restart(hg_ctx* ctx, const char* path, double t, int32_t iter);
 int  hg_load_restart(hg_ctx* ctx, const char* path, double* t, int32_t* iter);
 const char* hg_restart_last_error(void);
+/* The same file written while the context keeps stepping: the state (as of the launches queued so
+ * far) is copied on the context's stream to pinned host memory and a host thread writes the file
+ * once the copy has landed.  One write is in flight at a time (the next call, hg_restart_wait and
+ * hg_destroy wait for it); hg_restart_wait reports its outcome (reason in hg_last_error). */
+int  hg_save_restart_async(hg_ctx* ctx, const char* path, double t, int32_t iter);
+int  hg_restart_wait(hg_ctx* ctx);
 /* Interpolation nodes and weights on [0,1] used by the kernels for order N
  * (NodesAndWeightsClass.f90:251-332 computeNodesAndWeights).  xi, w: N+1 doubles. */
 int  hg_nodes(int32_t N, int32_t node_type, double* xi, double* w);

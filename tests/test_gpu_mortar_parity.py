@@ -289,3 +289,20 @@ def test_cylinder_re100_benchmark_golden():
     force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
     assert abs(force[1] / dyn - golden["cl"]) <= 1e-12
     assert abs(force[0] / dyn - golden["cd"]) <= 5e-8
+
+
+def test_ns_p_nonconforming_fp32():
+    """FP32 bulk path of the Navier-Stokes composite (CylinderRe100 mesh): residual to the FP32 bound,
+    and the stepped density within the 1e-5 relative L2 target."""
+    orc, q, kw = cylinder_re100_case()
+    Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=33)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g = hg.GpuDGSEM(orc.export_mesh(), precision=hg.PREC_FP32, **kw)
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= 1e-4
+    dt = orc.estimate_dt(0.1, 1e-2)
+    for k in range(10):
+        orc.time_step(O.RK5, k * dt, dt)
+    g.time_steps(hg.SCHEME_RK5, 10, 0.0, dt)
+    assert rel_l2(g.state().reshape(-1, 4)[:, 0], orc.state().reshape(-1, 4)[:, 0]) <= 1e-5

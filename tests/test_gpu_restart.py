@@ -66,3 +66,34 @@ def test_load_restart_size_mismatch(tmp_path):
     b = vortex(n=6)
     with pytest.raises(OSError, match="holds"):
         b.load_restart(p)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_async_save_while_stepping(tmp_path, mixed):
+    """hg_save_restart_async: the file holds the state of the requested iteration although steps are
+    queued right after the call (single-order and mixed-order contexts)."""
+    if mixed:
+        d = hmesh.box_descriptor(5, 5, -5.0, 5.0, -5.0, 5.0, np.where(np.arange(25) % 5 % 2 == 1, 5, 3),
+                                 hg.NODES_LG)
+        x = d["x"].reshape(-1, 2)
+        Q0 = cases.isentropic_vortex(x[:, 0], x[:, 1], beta=5.0).ravel()
+        mk = lambda: hg.GpuDGSEM(d, mach=0.5, node_type=hg.NODES_LG, riemann=hg.ROE,  # noqa: E731
+                                 bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    else:
+        mk = vortex
+    a = mk()
+    if mixed:
+        a.set_state(Q0)
+    dt = 0.01
+    a.time_steps(hg.SCHEME_RK3, 3, 0.0, dt)
+    expect = a.state()
+    a.save_restart(tmp_path / "async.HiORst", 3 * dt, 3, wait=False)
+    a.time_steps(hg.SCHEME_RK3, 10, 3 * dt, dt)     # queued behind the copy
+    a.restart_wait()
+    t, it, Q = restart.read(tmp_path / "async.HiORst")
+    assert (t, it) == (3 * dt, 3) and np.array_equal(Q, expect)
+    a.save_restart(tmp_path / "sync.HiORst", 3 * dt, 3)
+    assert not np.array_equal(restart.read(tmp_path / "sync.HiORst")[2], expect)   # the state moved on
+    with pytest.raises(hg.HorsesGpuError, match="restart write"):
+        a.save_restart(tmp_path / "no_such_dir" / "x.HiORst", 0.0, 0, wait=False)
+        a.restart_wait()
