@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(block_ns(P)) sensor_eval_kernel(int n_el, cons
                                                                   SensorArgs sa, PhysConst pc, float* feat,
                                                                   double* out) {
   constexpr int NP = P * P;
-  __shared__ real sQ[4][EPB][Tile<P, real>::S];
+  __shared__ real sQ[4][EPB][NP];
   __shared__ real sV[NP];
   const int flat = threadIdx.x, le = flat / NP, tid = flat - le * NP;
   const int e = blockIdx.x * EPB + le;

@@ -78,19 +78,19 @@ __host__ __device__ constexpr int block_ns(int P) { return ((P * P * epb_ns(P) +
 // that shared memory to the shock sensor.
 template <int P, int EPB, typename real, bool AFFINE, bool ST = true>
 struct NSTiles {
-  static constexpr int NP = P * P, FT = 4 * P, TS = Tile<P, real>::S;
+  static constexpr int NP = P * P, FT = 4 * P;
   real mat[3 * NP + 7 * P];   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w Vinv
-  real Q[4][EPB][TS];
-  real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : TS];   // Ja00 Ja01 Ja10 Ja11 J
-  real dQ[2][4][EPB][TS];
-  real Fc[ST ? 4 : 1][ST ? EPB : 1][ST ? TS : 1];
-  real Gc[ST ? 4 : 1][ST ? EPB : 1][ST ? TS : 1];
+  real Q[4][EPB][NP];
+  real Ja[AFFINE ? 1 : 5][AFFINE ? 1 : EPB][AFFINE ? 1 : NP];   // Ja00 Ja01 Ja10 Ja11 J
+  real dQ[2][4][EPB][NP];
+  real Fc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
+  real Gc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
   real face[12][EPB][FT];   // BR1 u* dS n (8) / F* (4) + gradient-face contravariant fluxes (8)
   double red[32][4];
 };
 
 template <int P, int EPB, typename real, bool AFFINE, bool ST>
-__device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE, ST>& s, const real (*src)[EPB][Tile<P, real>::S], int k,
+__device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE, ST>& s, const real (*src)[EPB][P * P], int k,
                                          int le, int side, int kk, const real* lbv) {
   real t = real(0);
 #pragma unroll
@@ -103,7 +103,7 @@ __device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE, ST>
 
 // The four variables' traces at face node kk of side `side` (the interpolant weights loaded once).
 template <int P, int EPB, typename real>
-__device__ __forceinline__ void trace4(const real (*src)[EPB][Tile<P, real>::S], int le, int side, int kk, const real* lbv,
+__device__ __forceinline__ void trace4(const real (*src)[EPB][P * P], int le, int side, int kk, const real* lbv,
                                        real* out) {
 #pragma unroll
   for (int k = 0; k < 4; ++k) out[k] = real(0);

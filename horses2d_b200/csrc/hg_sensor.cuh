@@ -13,7 +13,6 @@
 // No reference counterpart exists for modal and learned.
 #pragma once
 #include "hg_physics.cuh"
-#include "hg_stage.cuh"   // Tile (shared-tile element stride)
 
 namespace hg {
 
@@ -53,7 +52,7 @@ struct SensorOut {
 };
 
 // Modal indicator and (if asked) the learned one for element `le` of the CTA.  Q: the element tiles
-// [4][EPB][Tile<P, real>::S] in shared memory; n_active: elements of this CTA that exist.  All threads of the CTA call it (it holds barriers);
+// [4][EPB][NP] in shared memory; n_active: elements of this CTA that exist.  All threads of the CTA call it (it holds barriers);
 // results are valid in thread tid == 0 of each element.
 //
 // Network inference: the weights (stored with the hidden unit fastest) are copied once per CTA into
@@ -62,7 +61,7 @@ struct SensorOut {
 // four interleaved partial sums, and the output unit is a warp shuffle tree.
 template <int P, int EPB, typename real>
 __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const Phys<real>& ph,
-                                                    const real (*Q)[EPB][Tile<P, real>::S], int n_active,
+                                                    const real (*Q)[EPB][P * P], int n_active,
                                                     const real* Vinv, int le, int tid, bool active,
                                                     float* feat_out) {
   constexpr int NP = P * P, N = P - 1, SS = sensor_scratch(P);

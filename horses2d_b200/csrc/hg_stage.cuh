@@ -59,37 +59,6 @@ struct StageArgs {
   PhysConst pc;
 };
 
-// Element stride of the [var][element][node] shared tiles: P^2 values padded so that the rows
-// (stride P) and columns (stride 1) read by the lanes of one warp, which may span several elements,
-// fall in distinct shared-memory banks across the elements (0 where no pad up to P^2/4 achieves it:
-// larger pads would push the biggest tiles past the 48 KB of static shared memory).
-template <typename real>
-__host__ __device__ constexpr int tile_pad(int P) {
-  const int W = int(sizeof(real) / 4);
-  const int NP = P * P;
-  const int m = (32 + NP - 1) / NP + 1;   // elements one warp can touch
-  for (int pad = 0; pad <= NP / 4; ++pad) {
-    const int s = (NP + pad) * W;
-    bool ok = true;
-    for (int pat = 0; pat < 2 && ok; ++pat) {
-      const int st = pat == 0 ? P * W : W;
-      for (int e1 = 0; e1 < m && ok; ++e1)
-        for (int e2 = e1 + 1; e2 < m && ok; ++e2)
-          for (int a = 0; a < P && ok; ++a)
-            for (int b = 0; b < P && ok; ++b)
-              for (int w1 = 0; w1 < W && ok; ++w1)
-                for (int w2 = 0; w2 < W && ok; ++w2)
-                  if ((e1 * s + a * st + w1) % 32 == (e2 * s + b * st + w2) % 32) ok = false;
-    }
-    if (ok) return pad;
-  }
-  return 0;
-}
-template <int P, typename real>
-struct Tile {
-  static constexpr int S = P * P + tile_pad<real>(P);
-};
-
 // Elements per CTA: tiling variant 0 (default, large CTAs) and variant 1 (small CTAs: more CTAs in
 // flight on small meshes); hg_autotune times both on the resident state and keeps the faster.
 __host__ __device__ constexpr int epb_for(int P) {
@@ -120,10 +89,9 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
   constexpr int FT = 4 * P;
   constexpr int NW = block_of(P, EPB) / 32;
   __shared__ real s_mat[NP + 4 * P];
-  constexpr int TS = Tile<P, real>::S;
-  __shared__ real s_Fc[4][EPB][TS];
-  __shared__ real s_Gc[4][EPB][TS];
-  __shared__ real s_Q[4][EPB][TS];
+  __shared__ real s_Fc[4][EPB][NP];
+  __shared__ real s_Gc[4][EPB][NP];
+  __shared__ real s_Q[4][EPB][NP];
   __shared__ real s_F[4][EPB][FT];
   __shared__ double s_red[NW][4];
 
