@@ -454,6 +454,16 @@ def device_timed(ctxs, steps, warmup, dt, stream, world, dist, flush, min_load_s
     return sum(a.elapsed_time(b) for a, b in evs), sum(c["g"].launch_count() for c in ctxs) - launches0
 
 
+def max_over_ranks(values, world, dist, device="cuda"):
+    """Per-rank timings (ms) reduced to the job's: every rank gets the max over ranks (the slowest
+    replica sets the whole job's time)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
 def kernel_split(ctxs, steps, dt, stream, flush):
     """Per-kernel CUDA-event times over `steps` further steps (library timing mode)."""
     import torch
@@ -533,6 +543,7 @@ def run_shock(args, rank, world, local, dist):
     e2e_ms = (time.perf_counter() - t1) * 1e3
     if not (np.all(np.isfinite(Qe)) and np.all(np.isfinite(res))):
         raise SystemExit("non-finite state after the timed steps")
+    ms32, ms64, e2e_ms = max_over_ranks([ms32, ms64, e2e_ms], world, dist)
     value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
     value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
     bpd = stage_bytes_per_dof("shock", True, True, True)
@@ -550,7 +561,7 @@ def run_shock(args, rank, world, local, dist):
                        "l2": ("256 MB buffer written between timed steps (outside the step events)"
                               if flush.buf is not None else "inputs larger than L2"),
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": ndof * 3 * args.steps / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
+            "e2e": {"value": ndof * 3 * args.steps * world / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
                     "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
@@ -638,6 +649,7 @@ def run_kh(args, rank, world, local, dist):
     if not (np.all(np.isfinite(Qe)) and np.all(np.isfinite(res))):
         raise SystemExit("non-finite state after the timed steps")
     del Qe
+    ms32, ms64, e2e_ms = max_over_ranks([ms32, ms64, e2e_ms], world, dist)
     value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
     value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
     bpd = stage_bytes_per_dof("kh", True, True, True)
@@ -659,7 +671,7 @@ def run_kh(args, rank, world, local, dist):
                        "l2": ("256 MB buffer written between timed steps (outside the step events)"
                               if flush.buf is not None else "inputs larger than L2"),
                        "parallelism": f"replicas x{world}"},
-            "e2e": {"value": ndof * 3 * args.steps / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
+            "e2e": {"value": ndof * 3 * args.steps * world / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
                     "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
@@ -751,10 +763,7 @@ def main():
     e2e_ms = max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3)
     if not np.all(np.isfinite(res_host)) or not all(np.all(np.isfinite(q)) for q in Qout):
         raise SystemExit("non-finite state after the timed steps")
-    t_max = torch.tensor([ms, e2e_ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms, e2e_ms = float(t_max[0]), float(t_max[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], world, dist)
     value = ndof * 3 * args.steps * world / (ms * 1e-3)
     e2e = ndof * 3 * args.steps * world / (e2e_ms * 1e-3)
 
