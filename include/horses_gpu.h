@@ -168,7 +168,8 @@ int  hg_probes(hg_ctx* ctx, int32_t n, const int32_t* elements, const double* xi
 /* Stream control: run on the caller's stream (e.g. a framework's current stream). */
 int  hg_set_stream(hg_ctx* ctx, void* cuda_stream);
 int  hg_synchronize(hg_ctx* ctx);
-/* Device pointer of the resident state (reference layout) for in-HBM benchmarking. */
+/* Device pointer of the resident state (reference layout) for in-HBM benchmarking; NULL for a
+ * mixed-order context, whose state lives in one packed array per order. */
 double* hg_device_state(hg_ctx* ctx);
 /* Number of kernel launches issued by this context so far. */
 int64_t hg_launch_count(const hg_ctx* ctx);
