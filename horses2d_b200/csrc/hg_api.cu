@@ -32,7 +32,13 @@ static void drop_graph(hg_ctx* c) {
     if (x) cudaGraphExecDestroy(x);
     x = nullptr;
   }
+  for (auto& x : c->gexec1) {
+    if (x) cudaGraphExecDestroy(x);
+    x = nullptr;
+  }
   c->g_scheme = -1;
+  c->g1_scheme = -1;
+  c->g1_seen[0] = c->g1_seen[1] = 0;
   ++c->gen;
 }
 
@@ -696,10 +702,65 @@ extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
 
+static int scheme_stages(int scheme) { return scheme == HG_SCHEME_EULER ? 1 : (scheme == HG_SCHEME_RK3 ? 3 : 5); }
+
+// One step through a CUDA graph of that single step, one per trace-buffer parity at its start (an odd
+// number of stages flips the parity), for callers that step one at a time: the reference's loop with
+// a residual check per iteration.  The first step of a scheme and dt at a parity runs as plain
+// launches (it also sets kernel attributes outside any capture), the second is captured.
+static void graph_one_step(hg_ctx* c, int scheme, double t, double dt) {
+  if (c->g1_scheme != scheme || c->g1_dt != dt) {
+    for (auto& x : c->gexec1) {
+      if (x) cudaGraphExecDestroy(x);
+      x = nullptr;
+    }
+    c->g1_seen[0] = c->g1_seen[1] = 0;
+    c->g1_scheme = scheme;
+    c->g1_dt = dt;
+  }
+  const int p = c->cur;
+  if (!c->gexec1[p]) {
+    if (c->g1_seen[p]++ == 0) {
+      one_step(c, scheme, t, dt);
+      return;
+    }
+    const int64_t l0 = c->launches;
+    HG_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      one_step(c, scheme, t, dt);
+    } catch (...) {
+      cudaGraph_t g0 = nullptr;
+      cudaStreamEndCapture(c->stream, &g0);
+      if (g0) cudaGraphDestroy(g0);
+      c->launches = l0;
+      c->cur = p;
+      throw;
+    }
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    c->g1_launches[p] = c->launches - l0;
+    c->g1_last_T[p] = c->last_T;
+    c->launches = l0;
+    c->cur = p;   // the capture ran nothing
+    HG_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&c->gexec1[p], g, 0);
+    cudaGraphDestroy(g);
+    HG_CUDA(ie);
+  }
+  HG_CUDA(cudaGraphLaunch(c->gexec1[p], c->stream));
+  c->launches += c->g1_launches[p];
+  c->last_T = c->g1_last_T[p];
+  c->cur = p ^ (scheme_stages(scheme) & 1);
+}
+
 extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
   try {
     require_state(c);
-    one_step(c, scheme, t, dt);
+    if (!c->prof && c->stream != nullptr && !is_composite(c) &&
+        (scheme == HG_SCHEME_EULER || scheme == HG_SCHEME_RK3 || scheme == HG_SCHEME_RK5))
+      graph_one_step(c, scheme, t, dt);
+    else
+      one_step(c, scheme, t, dt);
     HG_CUDA(cudaGetLastError());
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }

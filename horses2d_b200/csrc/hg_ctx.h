@@ -90,6 +90,14 @@ struct hg_ctx {
   int64_t gen = 0;                // bumped whenever captured launches go stale (context groups check it)
   double g_dt = 0.0;
   int64_t g_launches[2] = {0, 0};
+  // CUDA graphs of one time step (hg_time_step), per parity at its start: captured the second time a
+  // step of the same scheme and dt starts at that parity (single-order contexts)
+  cudaGraphExec_t gexec1[2] = {nullptr, nullptr};
+  int g1_scheme = -1;
+  double g1_dt = 0.0;
+  int64_t g1_launches[2] = {0, 0};
+  int g1_seen[2] = {0, 0};
+  int g1_last_T[2] = {0, 0};
   // asynchronous restart files (hg_save_restart_async): pinned copy of the state, written by a host thread
   std::shared_ptr<struct AutosaveJob> autosave;
   // per-kernel timing (hg_profile): event pairs recorded around each launch
