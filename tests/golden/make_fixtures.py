@@ -33,6 +33,7 @@ MESHES = {
     "RampBench": "TestCases/Benchmark/Simulations/Ramp/MESH/Ramp.HiOMesh",
     "ShockWave": "TestCases/SupersonicTests/ShockWave/MESH/ShockWave.HiOMesh",
     "VortexTransportCase": "TestCases/Cases/VortexTransport/MESH/VortexTransport.HiOMesh",
+    "CylinderInflation": "TestCases/Benchmark/Simulations/CylinderRe1000/MESH/CylinderInflation.HiOMesh",
 }
 
 PLUGINS = {

@@ -20,6 +20,8 @@
   iteration 9884 and the four final residuals to 1e-11.
 * CylinderRe100 benchmark: exact Riemann solver on every zone, p-refinement, BR1, steady RK5; final
   residuals (1e-11) and the wall's lift and drag coefficients (surface integrals, 1e-12).
+* CylinderRe1000 benchmark: SIPG interior penalty across p-refinement zones (orders 4-10), exact
+  solver on every zone, transient RK5; iteration 512, residuals (1e-10), lift and drag (1e-12).
 * Spectral building blocks: exactness of the nodal derivative and quadrature.
 * Free-stream preservation on curved meshes, conservation on periodic meshes.
 """
@@ -193,6 +195,45 @@ def test_cylinder_re100_benchmark_golden():
     assert it == 250
     assert np.max(np.abs(orc.residuals() - np.array(golden["residuals"]))) <= 1e-11
     # lift / drag surface monitors: (pressure force - sqrt(gamma) M viscous force) p_ref L / (rho V^2 S / 2)
+    si = orc.surface_integrals(5)
+    dyn = 0.5 * r["rho"] * r["V"] * r["V"] * 1.0
+    force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
+    assert abs(force[1] / dyn - golden["cl"]) <= 1e-12
+    assert abs(force[0] / dyn - golden["cd"]) <= 1e-12
+
+
+def cylinder_re1000_oracle():
+    """CylinderRe1000 (TestCases/Benchmark/Simulations/CylinderRe1000): Navier-Stokes, Re 1000, M 0.1,
+    SIPG interior penalty (sigma0 10), HLL inside and the exact solver on every zone (three Dirichlet
+    zones, a partially non-reflective pressure outlet, an adiabatic wall), p-refinement zones of
+    orders 6/10/8/8 around the default 4, Legendre-Gauss nodes, uniform initial state."""
+    m = load_mesh("CylinderInflation")
+    porder = np.array([4, 6, 10, 8, 8])[m["p_zones"]]
+    ex = O.EXACT
+    bcs = [dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_DIRICHLET, riemann=ex),
+           dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2, riemann=ex),
+           dict(type=O.BC_VISCOUSWALL, wall_type=2, riemann=ex)]
+    orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.HLL, mach=0.1, reynolds=1000.0, prandtl=0.72, navier_stokes=1,
+                   viscous=O.IP, ip_method=0, sigma0_ip=10.0, bcs=bcs)
+    r = orc.ref
+    cv = 287.15 * 2.5   # UniformInitialCondition, dimensional
+    q = np.array([r["rho"], r["rho"] * r["V"], 0.0, cv * r["rho"] * r["T"] + 0.5 * r["rho"] * r["V"] * r["V"]])
+    q = q / np.array([r["rho"], r["rho"] * r["a"], r["rho"] * r["a"], r["p"]])
+    return orc, q
+
+
+def test_cylinder_re1000_benchmark_golden():
+    """The reference asserts, after the transient RK5 run to t = 0.013 (CFL 0.1, dt cap 1e-2),
+    iteration 512, the final residuals to 1e-10 and the wall's lift and drag to 1e-12
+    (SETUP/ProblemFile.f90:79-95).  Pins interior penalty across p-nonconforming edges (projection
+    types 3-6 of the viscous and gradient-face terms, penalty at the edge's order)."""
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["CylinderRe1000"]
+    orc, q = cylinder_re1000_oracle()
+    orc.set_state(np.tile(q, orc.ndof // 4))
+    it, t = orc.integrate(O.RK5, transient=True, t0=0.0, t_end=0.013, max_iter=10000000, cfl=0.1, dt_cap=1e-2)
+    assert it == golden["expected_iter"]
+    assert np.max(np.abs(orc.residuals() - np.array(golden["residuals"]))) <= 1e-10
+    r = orc.ref
     si = orc.surface_integrals(5)
     dyn = 0.5 * r["rho"] * r["V"] * r["V"] * 1.0
     force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
