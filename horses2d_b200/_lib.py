@@ -44,7 +44,7 @@ class MeshDesc(C.Structure):
                 ("edge_inverse", I32P), ("edge_marker", I32P), ("edge_n", F64P), ("edge_dS", F64P),
                 ("periodic_partner", I32P), ("edge_invh", F64P), ("n_mortars", C.c_int32),
                 ("mortar_elem", I32P), ("mortar_side", I32P), ("mortar_flip", I32P), ("mortar_n", F64P),
-                ("mortar_dS", F64P)]
+                ("mortar_dS", F64P), ("mortar_invh", F64P)]
 
 
 _lib = None

@@ -217,7 +217,8 @@ void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool upda
     // faces between orders and subdivided edges first, then every part's fused stage; the parts'
     // launches are counted on the composite.  Navier-Stokes (BR1): the mortar kernel's gradient face
     // terms, the parts' gradient kernels, the mortar kernel's inviscid + viscous fluxes (they need
-    // the gradient traces), the parts' stage kernels.
+    // the gradient traces), the parts' stage kernels.  Interior penalty: no gradient face terms; the
+    // flux pass adds the penalty and the gradient-face terms.
     auto parts_stage = [&](int phase) {
       for (hg_ctx* p : c->parts) {
         const int64_t l0 = p->launches;
@@ -229,7 +230,7 @@ void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool upda
       }
     };
     if (c->ns) {
-      launch_mortar(c, MORTAR_GRADIENT);
+      if (!c->ip) launch_mortar(c, MORTAR_GRADIENT);   // the interior-penalty gradient is element-local
       parts_stage(1);
       launch_mortar(c, MORTAR_FLUX);
       parts_stage(2);

@@ -166,7 +166,7 @@ void ctx_free(hg_ctx* c);
 void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid);
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs);
 void composite_free(hg_ctx* c);
-enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1 };
+enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1, MORTAR_FLUX_IP = 2 };
 void launch_mortar(hg_ctx* c, int mode);
 inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
 constexpr int HG_MAX_PARTS = 12;

@@ -30,6 +30,7 @@ namespace {
 // edge (sides L, RN, RS).  Projections tf/tb: kind 0 {L, R} (-1: identity), kind 1 {LN, LS, RN, RS};
 // offsets into the matrix pool, row-major [rows][cols].
 struct MortarFace {
+  double invh;    // interior penalty: Area / min(volume) of the face's elements
   int kind;
   int part[3], el[3], side[3], slot[3], P[3];
   int PE[2];      // edge nodes (kind 0), or north and south half nodes (kind 1)
@@ -48,8 +49,10 @@ struct MortarArgs {
   const real* GT[HG_MAX_PARTS];    // gradient traces (Navier-Stokes)
   real* NF[HG_MAX_PARTS];          // MORTAR_FLUX output
   real* NFG[HG_MAX_PARTS];         // MORTAR_GRADIENT output
-  int mode;                        // MORTAR_FLUX or MORTAR_GRADIENT
-  int visc;                        // MORTAR_FLUX: add the BR1 viscous flux
+  int mode;                        // MORTAR_FLUX, MORTAR_FLUX_IP or MORTAR_GRADIENT
+  int visc;                        // fluxes: add the viscous flux (BR1 average; IP adds the penalty)
+  int grad_faces;                  // MORTAR_FLUX_IP: SIPG / NIPG gradient-face terms
+  double sigma0, epsilon;          // interior penalty parameter and the method's epsilon (-1, 1, 0)
   int riemann;
   PhysConst pc;
 };
@@ -79,10 +82,14 @@ __device__ __forceinline__ void project_row(const real* mat, int m, int cols, in
 }
 
 // Value at one edge node from the two sides' projected traces: MORTAR_FLUX the lifted flux
-// (Fi - Fv) dS (4 values), MORTAR_GRADIENT the BR1 terms u* dS n, u* = (qL + qR)/2 (8 values).
+// (Fi - Fv) dS (4 values), MORTAR_GRADIENT the BR1 terms u* dS n, u* = (qL + qR)/2 (8 values),
+// MORTAR_FLUX_IP the flux with the interior-penalty term -sigma0 mu N^2 invh (qL - qR) in Fv and the
+// gradient-face terms of both sides, +-eps mu/2 Fv(q, (qL - qR) n) dS (4 + 8 + 8 values;
+// IP_RiemannSolver / IP_GradientRiemannSolver, Approximation/DGViscous_IP.f90:120-134, 240-247).
 template <int MODE, typename real>
 __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys<real>& ph, const real* qL,
-                                           const real* qR, const real* dL, const real* dR, const real* g, real* out) {
+                                           const real* qR, const real* dL, const real* dR, const real* g,
+                                           real penalty, real* out) {
   if constexpr (MODE == MORTAR_GRADIENT) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -94,25 +101,42 @@ __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys
     real F[4];
     if (a.riemann == RIEMANN_EXACT) exact(ph, qL, qR, g[0], g[1], F);
     else riemann(a.riemann, ph, qL, qR, g[0], g[1], F);
+    const real mu = real(a.pc.mu);
     if (a.visc) {
       real FLx[4], FLy[4], FRx[4], FRy[4];
       viscous_flux(ph, qL, dL, dL + 4, FLx, FLy);
       viscous_flux(ph, qR, dR, dR + 4, FRx, FRy);
-      const real mu = real(a.pc.mu);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        const real fv = real(0.5) * (mu * FLx[k] + mu * FRx[k]) * g[0] + real(0.5) * (mu * FLy[k] + mu * FRy[k]) * g[1];
+        real fv = real(0.5) * (mu * FLx[k] + mu * FRx[k]) * g[0] + real(0.5) * (mu * FLy[k] + mu * FRy[k]) * g[1];
+        if (MODE == MORTAR_FLUX_IP) fv = fv - penalty * (qL[k] - qR[k]);
         F[k] = F[k] - fv;
       }
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = F[k] * g[2];
+    if constexpr (MODE == MORTAR_FLUX_IP) {
+#pragma unroll
+      for (int k = 4; k < 20; ++k) out[k] = real(0);
+      if (a.visc && a.grad_faces) {
+        real fgx[4], fgy[4], Ax[4], Ay[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { fgx[k] = (qL[k] - qR[k]) * g[0]; fgy[k] = (qL[k] - qR[k]) * g[1]; }
+        const real cL = real(0.5) * real(a.epsilon) * mu, cR = -cL;
+        viscous_flux(ph, qL, fgx, fgy, Ax, Ay);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { out[4 + k] = cL * Ax[k] * g[2]; out[8 + k] = cL * Ay[k] * g[2]; }
+        viscous_flux(ph, qR, fgx, fgy, Ax, Ay);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { out[12 + k] = cR * Ax[k] * g[2]; out[16 + k] = cR * Ay[k] * g[2]; }
+      }
+    }
   }
 }
 
 template <typename real, int MODE>
 __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
-  constexpr int NC = MODE == MORTAR_GRADIENT ? 8 : 4;   // values per edge node
+  constexpr int NC = MODE == MORTAR_GRADIENT ? 8 : (MODE == MORTAR_FLUX_IP ? 20 : 4);   // values per edge node
   __shared__ real sT[MW][3][MP][4];   // Q traces of the face's element sides
   __shared__ real sG[MW][3][MP][8];   // their gradient traces (x then y), viscous fluxes only
   __shared__ real sF[MW][2][MP][NC];  // values at the edge (half) nodes
@@ -121,7 +145,7 @@ __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
   if (fi >= a.n) return;   // whole warps leave together; the kernel synchronises warps only
   const MortarFace& f = a.f[fi];
   const int ns = f.kind == 0 ? 2 : 3;
-  const bool grads = MODE == MORTAR_FLUX && a.visc;
+  const bool grads = MODE != MORTAR_GRADIENT && a.visc;
   for (int t = lane; t < ns * MP; t += 32) {
     const int s = t / MP, k = t % MP;
     if (k < f.P[s]) {
@@ -157,18 +181,31 @@ __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
         project_row<8, 8>(a.mat, mL, f.P[0], i, &sG[w][0][0][0], dL);
         project_row<8, 8>(a.mat, mR, f.P[sR], rR, &sG[w][sR][0][0], dR);
       }
-      node_value<MODE>(a, ph, qL, qR, dL, dR, a.geo + size_t(f.geo[h] + i) * 3, v);
+      // penalty sigma0 mu N^2 invh at the edge's (half edge's) order
+      const real penalty = real(a.sigma0 * a.pc.mu * double(PE - 1) * double(PE - 1) * f.invh);
+      node_value<MODE>(a, ph, qL, qR, dL, dR, a.geo + size_t(f.geo[h] + i) * 3, penalty, v);
 #pragma unroll
       for (int k = 0; k < NC; ++k) sF[w][h][i][k] = v[k];
     }
   }
   __syncwarp();
-  // back to the elements: LEFT + Tb F (both halves of a subdivided edge), RIGHT - Tb F in its own order
-  real* const* outp = MODE == MORTAR_GRADIENT ? a.NFG : a.NF;
+  // back to the elements: LEFT + Tb F (both halves of a subdivided edge), RIGHT - Tb F in its own order;
+  // MORTAR_FLUX_IP: also the gradient-face terms, LEFT's from values 4-11, RIGHT's from 12-19 (no sign)
   auto store = [&](int s, int i, const real* v, real sign) {
-    real* np = outp[f.part[s]] + (size_t(f.slot[s]) * f.P[s] + i) * NC;
+    if constexpr (MODE == MORTAR_FLUX_IP) {
+      real* np = a.NF[f.part[s]] + (size_t(f.slot[s]) * f.P[s] + i) * 4;
 #pragma unroll
-    for (int k = 0; k < NC; ++k) np[k] = sign * v[k];
+      for (int k = 0; k < 4; ++k) np[k] = sign * v[k];
+      real* gp = a.NFG[f.part[s]] + (size_t(f.slot[s]) * f.P[s] + i) * 8;
+      const int o = s == 0 ? 4 : 12;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) gp[k] = v[o + k];
+    } else {
+      real* const* outp = MODE == MORTAR_GRADIENT ? a.NFG : a.NF;
+      real* np = outp[f.part[s]] + (size_t(f.slot[s]) * f.P[s] + i) * NC;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) np[k] = sign * v[k];
+    }
   };
   if (f.kind == 0) {
     const int PE = f.PE[0];
@@ -286,12 +323,17 @@ void launch_mortar(hg_ctx* c, int mode) {
       a.NF[p] = static_cast<real*>(q->d_NF);
       a.NFG[p] = static_cast<real*>(q->d_NFG);
     }
+    if (mode == MORTAR_FLUX && c->ns && c->ip) mode = MORTAR_FLUX_IP;
     a.mode = mode;
     a.visc = c->ns && c->pc.mu != 0.0;
+    a.grad_faces = c->grad_faces ? 1 : 0;
+    a.sigma0 = c->sigma0;
+    a.epsilon = c->epsilon;
     a.riemann = c->riemann;
     a.pc = c->pc;
     timed(c, HG_KERNEL_MORTAR, [&] {
       if (mode == MORTAR_GRADIENT) mortar_kernel<real, MORTAR_GRADIENT><<<grid, MW * 32, 0, c->stream>>>(a);
+      else if (mode == MORTAR_FLUX_IP) mortar_kernel<real, MORTAR_FLUX_IP><<<grid, MW * 32, 0, c->stream>>>(a);
       else mortar_kernel<real, MORTAR_FLUX><<<grid, MW * 32, 0, c->stream>>>(a);
     });
   };
@@ -312,8 +354,8 @@ void composite_free(hg_ctx* c) {
 }
 
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
-  if (ph->navier_stokes && (ph->viscous != 0 || ph->av_type != HG_AV_NONE))
-    throw std::runtime_error("mixed orders and subdivided edges in the Navier-Stokes build take BR1 without "
+  if (ph->navier_stokes && ph->av_type != HG_AV_NONE)
+    throw std::runtime_error("mixed orders and subdivided edges in the Navier-Stokes build take no "
                              "artificial dissipation");
   const int E = m->n_elements;
   if (E <= 0) throw std::runtime_error("mesh has no elements");
@@ -354,7 +396,12 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
   c->node_type = ph->node_type;
   c->riemann = ph->riemann;
   c->ns = ph->navier_stokes != 0 && ph->reynolds != 0.0;
-  const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
+  c->ip = ph->viscous == 1;
+  c->grad_faces = c->ip && ph->ip_method != 2;
+  c->sigma0 = ph->sigma0_ip;
+  c->epsilon = ph->ip_method == 0 ? -1.0 : (ph->ip_method == 1 ? 1.0 : 0.0);
+  if (c->ns && c->ip && (!m->edge_invh || (m->n_mortars > 0 && !m->mortar_invh)))
+    throw std::runtime_error("interior penalty needs edge_invh (and mortar_invh for subdivided edges)");  const double gamma = ph->gamma > 0 ? ph->gamma : 1.4;
   c->gamma = gamma; c->mach = ph->mach;
   c->pc.gamma = gamma;
   c->pc.gm1 = gamma - 1.0;
@@ -433,6 +480,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
     mf.PE[0] = NE + 1;
     mf.PE[1] = 0;
     mf.inv = m->edge_inverse[f] != 0;
+    mf.invh = m->edge_invh ? m->edge_invh[f] : 0.0;
     for (int k = 0; k < 4; ++k) mf.tf[k] = mf.tb[k] = -1;
     const std::vector<double> xe = pool.op(NE).xi;
     for (int k = 0; k < 2; ++k) {
@@ -465,6 +513,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
     mf.PE[0] = NN + 1;
     mf.PE[1] = NS + 1;
     mf.inv = 0;
+    mf.invh = m->mortar_invh ? m->mortar_invh[q] : 0.0;
     std::vector<double> xN = pool.op(NN).xi, xS = pool.op(NS).xi;
     std::vector<double> hN(xN.size()), hS(xS.size());
     for (size_t p = 0; p < xN.size(); ++p) hN[p] = 0.5 + 0.5 * xN[p];

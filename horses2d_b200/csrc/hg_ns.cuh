@@ -470,13 +470,28 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       const int sd_ = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + sd_];
       const int kind = sd.y & 15;
-      if (kind == SIDE_FLUX) {   // inviscid and viscous flux of the mortar kernel (BR1, no gradient-face terms)
+      if (kind == SIDE_FLUX) {   // inviscid and viscous flux of the mortar kernel, and its gradient-face terms
         const real* fp = a.NF + (size_t(sd.x) * P + kk) * 4;
 #pragma unroll
         for (int k = 0; k < 4; ++k) s.face[k][le][t] = fp[k];
-        if (IP && a.grad_faces && visc)
+        if (IP && a.grad_faces && visc) {
+          const real* gp = a.NFG + (size_t(sd.x) * P + kk) * 8;
+          const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+          real fJa00, fJa01, fJa10, fJa11, fJ;
+          if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+          else {
+            fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
+            fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
+            fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
+            fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
+            fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+          }
 #pragma unroll
-          for (int k = 0; k < 4; ++k) { s.face[4 + k][le][t] = real(0); s.face[8 + k][le][t] = real(0); }
+          for (int k = 0; k < 4; ++k) {
+            s.face[4 + k][le][t] = (gp[k] * fJa00 + gp[4 + k] * fJa10) / fJ;
+            s.face[8 + k][le][t] = (gp[k] * fJa01 + gp[4 + k] * fJa11) / fJ;
+          }
+        }
         continue;
       }
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;

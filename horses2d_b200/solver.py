@@ -77,7 +77,7 @@ class GpuDGSEM:
         md.n_mortars = int(len(np.asarray(mesh.get("mortar_elem", ()))) // 3)
         for f, dt, ct in (("mortar_elem", np.int32, C.c_int32), ("mortar_side", np.int32, C.c_int32),
                           ("mortar_flip", np.int32, C.c_int32), ("mortar_n", np.float64, C.c_double),
-                          ("mortar_dS", np.float64, C.c_double)):
+                          ("mortar_dS", np.float64, C.c_double), ("mortar_invh", np.float64, C.c_double)):
             put(f, f, dt, ct, True)
         ph = L.PhysicsDesc(node_type=node_type, riemann=riemann, navier_stokes=navier_stokes, viscous=viscous,
                            ip_method=ip_method, sigma0_ip=sigma0_ip, mach=mach, reynolds=reynolds,

@@ -84,7 +84,7 @@ typedef struct {
  * reference), stored one edge after the other.
  * Mixed orders and subdivided edges (p-nonconforming projections types 3-6 and
  * SubdividedEdge_t, Mesh/QuadElement_EdgeProcedures.incf:749-1345) are supported for
- * the Euler build, and for the Navier-Stokes build with BR1 and without artificial
+ * the Euler build, and for the Navier-Stokes build (BR1 or interior penalty) without artificial
  * dissipation.  Orders: 1-12 (Euler build), 1-10 (Navier-Stokes build). */
 typedef struct {
   int32_t n_elements;
@@ -113,6 +113,7 @@ typedef struct {
   const int32_t* mortar_flip;   /* [n_mortars][2] RIGHT_NORTH, RIGHT_SOUTH traverse their half backwards */
   const double*  mortar_n;      /* [n_mortars][PN+PS][2] unit normals outward from LEFT (north then south) */
   const double*  mortar_dS;     /* [n_mortars][PN+PS]    surface jacobians of the halves */
+  const double*  mortar_invh;   /* [n_mortars] Area / min(volume) of the three elements (interior penalty); may be NULL */
 } hg_mesh_desc;
 
 /* Create a context: uploads geometry, connectivity and boundary zones once.

@@ -243,7 +243,8 @@ extern "C" void or_export_sizes(void* h, int out[4]) {
 extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                               int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
                               double* edge_dS, int* periodic_partner, double* edge_invh, int* mortar_elem,
-                              int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS) {
+                              int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS,
+                              double* mortar_invh) {
   Oracle& o = *static_cast<Oracle*>(h);
   for (size_t ei = 0; ei < o.el.size(); ++ei) {
     const Element& e = o.el[ei];
@@ -276,6 +277,7 @@ extern "C" int or_export_mesh(void* h, int* N, double* Ja, double* jac, double* 
         mortar_elem[3 * m + s] = f.quads[slots[s]];
         mortar_side[3 * m + s] = f.edgeLocation[slots[s]];
       }
+      mortar_invh[m] = f.invh;
       for (int s = 0; s < 2; ++s) {
         const int slot = s == 0 ? SLOT_RN : SLOT_RS;
         const Element& R = o.el[f.quads[slot]];

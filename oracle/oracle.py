@@ -90,7 +90,7 @@ def lib():
         L.or_edge_count_by_type.restype = i
         L.or_edge_count_by_type.argtypes = [vp, i]
         L.or_export_mesh.restype = i
-        L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp, ip, ip, ip, dp, dp]
+        L.or_export_mesh.argtypes = [vp, ip, dp, dp, dp, dp, dp, ip, ip, ip, ip, dp, dp, ip, dp, ip, ip, ip, dp, dp, dp]
         L.or_export_sizes.restype = None
         L.or_export_sizes.argtypes = [vp, ip]
         L.or_mesh_lists.restype = i
@@ -296,11 +296,12 @@ class Oracle:
                  edge_inverse=np.zeros(F, np.int32), edge_marker=np.zeros(F, np.int32), edge_n=np.zeros(2 * FN),
                  edge_dS=np.zeros(FN), periodic_partner=np.zeros(F, np.int32), edge_invh=np.zeros(F),
                  mortar_elem=np.zeros(3 * M, np.int32), mortar_side=np.zeros(3 * M, np.int32),
-                 mortar_flip=np.zeros(2 * M, np.int32), mortar_n=np.zeros(2 * MN), mortar_dS=np.zeros(MN))
+                 mortar_flip=np.zeros(2 * M, np.int32), mortar_n=np.zeros(2 * MN), mortar_dS=np.zeros(MN),
+                 mortar_invh=np.zeros(M))
         ip_, dp_ = C.c_int, C.c_double
         lib().or_export_mesh(self.h, *[_p(d[k], ip_ if d[k].dtype == np.int32 else dp_) for k in
                                        ("N", "Ja", "jac", "x", "volume", "vertices", "edge_elem", "edge_side",
                                         "edge_inverse", "edge_marker", "edge_n", "edge_dS", "periodic_partner",
                                         "edge_invh", "mortar_elem", "mortar_side", "mortar_flip", "mortar_n",
-                                        "mortar_dS")])
+                                        "mortar_dS", "mortar_invh")])
         return d

@@ -113,7 +113,7 @@ int     or_edge_count_by_type(void* h, int type);
  * nodes FN, M subdivided edges, their half-edge nodes MN}.  Array sizes: N[E], Ja[nodes*4],
  * jac[nodes], x[nodes*2], volume[E], vertices[E*8], edge_elem[2F], edge_side[2F], edge_inverse[F],
  * edge_marker[F], edge_n[FN*2], edge_dS[FN], periodic_partner[F], edge_invh[F], mortar_elem[3M],
- * mortar_side[3M], mortar_flip[2M], mortar_n[MN*2], mortar_dS[MN].  Returns 0. */
+ * mortar_side[3M], mortar_flip[2M], mortar_n[MN*2], mortar_dS[MN], mortar_invh[M].  Returns 0. */
 void    or_export_sizes(void* h, int out[4]);
 /* Boundary states given by functions (the problem-file plugin's BoundaryConditionFunction,
  * BoundaryConditions/BoundaryConditionFunctionDrivers.incf): or_zone_edge_nodes returns the
@@ -135,7 +135,8 @@ void    or_set_zone_state(void* h, int zone, const double* uB);
 int     or_export_mesh(void* h, int* N, double* Ja, double* jac, double* x, double* volume, double* vertices,
                        int* edge_elem, int* edge_side, int* edge_inverse, int* edge_marker, double* edge_n,
                        double* edge_dS, int* periodic_partner, double* edge_invh, int* mortar_elem,
-                       int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS);
+                       int* mortar_side, int* mortar_flip, double* mortar_n, double* mortar_dS,
+                       double* mortar_invh);
 
 #ifdef __cplusplus
 }

@@ -306,3 +306,52 @@ def test_ns_p_nonconforming_fp32():
         orc.time_step(O.RK5, k * dt, dt)
     g.time_steps(hg.SCHEME_RK5, 10, 0.0, dt)
     assert rel_l2(g.state().reshape(-1, 4)[:, 0], orc.state().reshape(-1, 4)[:, 0]) <= 1e-5
+
+
+# ----------------------------------------------------------------------------- Navier-Stokes (interior penalty)
+def cylinder_re1000_gpu():
+    from test_oracle import cylinder_re1000_oracle
+    orc, q = cylinder_re1000_oracle()
+    ge = hg.EXACT
+    zq = [orc.zone_state(z) for z in range(1, 5)]
+    gbcs = [dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[0]), dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[1]),
+            dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[2]),
+            dict(type=hg.BC_PRESSUREOUTLET, outflow_type=2, riemann=ge, state=zq[3]),
+            dict(type=hg.BC_VISCOUSWALL, wall_type=2, riemann=ge)]
+    g = hg.GpuDGSEM(orc.export_mesh(), mach=0.1, reynolds=1000.0, prandtl=0.72, navier_stokes=1, viscous=hg.IP,
+                    ip_method=hg.SIPG, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.HLL, bcs=gbcs)
+    return orc, q, g
+
+
+def test_ns_ip_mortar_residual():
+    """CylinderRe1000 mesh (orders 4-10, 138 edges between orders, 92 subdivided edges), SIPG: the
+    penalty at the edge's order and the gradient-face terms through the mortars; residual of a
+    perturbed state and RK5 steps."""
+    orc, q, g = cylinder_re1000_gpu()
+    Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=41)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= TOL_STAGE
+    dt = orc.estimate_dt(0.1, 1e-2)
+    for k in range(3):
+        orc.time_step(O.RK5, k * dt, dt)
+    g.time_steps(hg.SCHEME_RK5, 3, 0.0, dt)
+    assert rel_l2(g.state(), orc.state()) <= TOL_STEPS
+
+
+def test_cylinder_re1000_benchmark_golden():
+    """The reference's CylinderRe1000 regression on the device: transient RK5 to t = 0.013 (CFL 0.1,
+    dt cap 1e-2); iteration 512, the final residuals (reference: 1e-10) and the wall's lift and drag."""
+    golden = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["CylinderRe1000"]
+    orc, q, g = cylinder_re1000_gpu()
+    g.set_state(np.tile(q, orc.ndof // 4))
+    it, _ = g.integrate(hg.SCHEME_RK5, transient=True, t0=0.0, t_end=0.013, max_iter=10000000, cfl=0.1, dt_cap=1e-2)
+    assert it == golden["expected_iter"]
+    np.testing.assert_allclose(g.residuals(), golden["residuals"], rtol=1e-9)
+    r = orc.ref
+    si = g.surface_integrals(5)
+    dyn = 0.5 * r["rho"] * r["V"] * r["V"] * 1.0
+    force = (si["pressure_force"] - si["viscous_force"] * np.sqrt(1.4) * 0.1) * r["p"] * r["L"]
+    assert abs(force[1] / dyn - golden["cl"]) <= 1e-12
+    assert abs(force[0] / dyn - golden["cd"]) <= 5e-8
