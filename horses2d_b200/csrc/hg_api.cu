@@ -705,6 +705,15 @@ extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
 
 static int scheme_stages(int scheme) { return scheme == HG_SCHEME_EULER ? 1 : (scheme == HG_SCHEME_RK3 ? 3 : 5); }
 
+// A composite's parts step in lockstep with it: their trace parity and last evaluated traces follow
+// the composite's after a capture (which ran nothing) and after a replay.
+static void sync_parts(hg_ctx* c) {
+  for (hg_ctx* p : c->parts) {
+    p->cur = c->cur;
+    p->last_T = c->last_T;
+  }
+}
+
 // One step through a CUDA graph of that single step, one per trace-buffer parity at its start (an odd
 // number of stages flips the parity), for callers that step one at a time: the reference's loop with
 // a residual check per iteration.  The first step of a scheme and dt at a parity runs as plain
@@ -735,6 +744,7 @@ static void graph_one_step(hg_ctx* c, int scheme, double t, double dt) {
       if (g0) cudaGraphDestroy(g0);
       c->launches = l0;
       c->cur = p;
+      sync_parts(c);
       throw;
     }
     cudaGraph_t g = nullptr;
@@ -743,6 +753,7 @@ static void graph_one_step(hg_ctx* c, int scheme, double t, double dt) {
     c->g1_last_T[p] = c->last_T;
     c->launches = l0;
     c->cur = p;   // the capture ran nothing
+    sync_parts(c);
     HG_CUDA(ce);
     const cudaError_t ie = cudaGraphInstantiate(&c->gexec1[p], g, 0);
     cudaGraphDestroy(g);
@@ -752,12 +763,13 @@ static void graph_one_step(hg_ctx* c, int scheme, double t, double dt) {
   c->launches += c->g1_launches[p];
   c->last_T = c->g1_last_T[p];
   c->cur = p ^ (scheme_stages(scheme) & 1);
+  sync_parts(c);
 }
 
 extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
   try {
     require_state(c);
-    if (!c->prof && c->stream != nullptr && !is_composite(c) &&
+    if (!c->prof && c->stream != nullptr &&
         (scheme == HG_SCHEME_EULER || scheme == HG_SCHEME_RK3 || scheme == HG_SCHEME_RK5))
       graph_one_step(c, scheme, t, dt);
     else

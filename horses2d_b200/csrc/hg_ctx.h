@@ -91,7 +91,7 @@ struct hg_ctx {
   double g_dt = 0.0;
   int64_t g_launches[2] = {0, 0};
   // CUDA graphs of one time step (hg_time_step), per parity at its start: captured the second time a
-  // step of the same scheme and dt starts at that parity (single-order contexts)
+  // step of the same scheme and dt starts at that parity
   cudaGraphExec_t gexec1[2] = {nullptr, nullptr};
   int g1_scheme = -1;
   double g1_dt = 0.0;

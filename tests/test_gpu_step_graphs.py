@@ -11,8 +11,10 @@ from horses2d_b200 import mesh as hmesh, cases
 pytestmark = pytest.mark.gpu
 
 
-def ctx(ns=False, precision=hg.PREC_FP64):
-    d = hmesh.box_descriptor(8, 8, -5.0, 5.0, -5.0, 5.0, 4, hg.NODES_LG)
+def ctx(ns=False, precision=hg.PREC_FP64, mixed=False):
+    # mixed: a composite of two orders (a band of order 5; periodic partners share order 4)
+    N = np.where(np.isin(np.arange(64) % 8, (3, 4)), 5, 4) if mixed else 4
+    d = hmesh.box_descriptor(8, 8, -5.0, 5.0, -5.0, 5.0, N, hg.NODES_LG)
     x = d["x"].reshape(-1, 2)
     Q = cases.isentropic_vortex(x[:, 0], x[:, 1], beta=4.0).ravel()
     kw = dict(mach=0.5, node_type=hg.NODES_LG, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
@@ -23,9 +25,9 @@ def ctx(ns=False, precision=hg.PREC_FP64):
     return g
 
 
-@pytest.mark.parametrize("ns", [False, True])
-def test_single_step_graphs_equal_plain_launches(ns):
-    a, b = ctx(ns), ctx(ns)
+@pytest.mark.parametrize("ns,mixed", [(False, False), (True, False), (False, True), (True, True)])
+def test_single_step_graphs_equal_plain_launches(ns, mixed):
+    a, b = ctx(ns, mixed=mixed), ctx(ns, mixed=mixed)
     b.profile(True)            # timing mode: plain launches only
     plan = [(hg.SCHEME_RK5, 0.01)] * 7 + [(hg.SCHEME_RK5, 0.008)] * 5 + [(hg.SCHEME_RK3, 0.008)] * 6 + \
            [(hg.SCHEME_EULER, 0.001)] * 5
