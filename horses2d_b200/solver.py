@@ -123,8 +123,12 @@ class GpuDGSEM:
         Q = _arr(Q, np.float64).ravel()
         self._check(self._lib.hg_set_state(self._h, Q.ctypes.data_as(L.F64P), Q.size))
 
-    def state(self):
-        Q = np.empty(self.ndof)
+    def state(self, out=None):
+        """Storage%Q of the resident state; `out` (contiguous float64, e.g. a pinned host buffer)
+        receives it instead of a new array."""
+        Q = np.empty(self.ndof) if out is None else out
+        if Q.dtype != np.float64 or Q.size != self.ndof or not Q.flags.c_contiguous:
+            raise HorsesGpuError("state buffer must be contiguous float64 of ndof values")
         self._check(self._lib.hg_get_state(self._h, Q.ctypes.data_as(L.F64P), Q.size))
         return Q
 
