@@ -309,9 +309,9 @@ def test_ns_p_nonconforming_fp32():
 
 
 # ----------------------------------------------------------------------------- Navier-Stokes (interior penalty)
-def cylinder_re1000_gpu():
+def cylinder_re1000_gpu(ip_method=0):
     from test_oracle import cylinder_re1000_oracle
-    orc, q = cylinder_re1000_oracle()
+    orc, q = cylinder_re1000_oracle(ip_method)
     ge = hg.EXACT
     zq = [orc.zone_state(z) for z in range(1, 5)]
     gbcs = [dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[0]), dict(type=hg.BC_DIRICHLET, riemann=ge, state=zq[1]),
@@ -319,8 +319,19 @@ def cylinder_re1000_gpu():
             dict(type=hg.BC_PRESSUREOUTLET, outflow_type=2, riemann=ge, state=zq[3]),
             dict(type=hg.BC_VISCOUSWALL, wall_type=2, riemann=ge)]
     g = hg.GpuDGSEM(orc.export_mesh(), mach=0.1, reynolds=1000.0, prandtl=0.72, navier_stokes=1, viscous=hg.IP,
-                    ip_method=hg.SIPG, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.HLL, bcs=gbcs)
+                    ip_method=ip_method, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.HLL, bcs=gbcs)
     return orc, q, g
+
+
+@pytest.mark.parametrize("ip_method", [hg.NIPG, hg.IIPG])
+def test_ns_ip_variants_mortar_residual(ip_method):
+    """NIPG (epsilon = +1) and IIPG (no gradient-face terms) through the mortars: residual parity."""
+    orc, q, g = cylinder_re1000_gpu(ip_method)
+    Q = perturbed(np.tile(q, orc.ndof // 4), 0.01, seed=42 + ip_method)
+    orc.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    g.set_state(Q)
+    assert rel_l2(g.compute_time_derivative(0.0), ref) <= TOL_STAGE
 
 
 def test_ns_ip_mortar_residual():

@@ -202,7 +202,7 @@ def test_cylinder_re100_benchmark_golden():
     assert abs(force[0] / dyn - golden["cd"]) <= 1e-12
 
 
-def cylinder_re1000_oracle():
+def cylinder_re1000_oracle(ip_method=0):
     """CylinderRe1000 (TestCases/Benchmark/Simulations/CylinderRe1000): Navier-Stokes, Re 1000, M 0.1,
     SIPG interior penalty (sigma0 10), HLL inside and the exact solver on every zone (three Dirichlet
     zones, a partially non-reflective pressure outlet, an adiabatic wall), p-refinement zones of
@@ -214,7 +214,7 @@ def cylinder_re1000_oracle():
            dict(type=O.BC_DIRICHLET, riemann=ex), dict(type=O.BC_PRESSUREOUTLET, outflow_type=2, riemann=ex),
            dict(type=O.BC_VISCOUSWALL, wall_type=2, riemann=ex)]
     orc = O.Oracle(m, porder, nodes=O.LG, riemann=O.HLL, mach=0.1, reynolds=1000.0, prandtl=0.72, navier_stokes=1,
-                   viscous=O.IP, ip_method=0, sigma0_ip=10.0, bcs=bcs)
+                   viscous=O.IP, ip_method=ip_method, sigma0_ip=10.0, bcs=bcs)
     r = orc.ref
     cv = 287.15 * 2.5   # UniformInitialCondition, dimensional
     q = np.array([r["rho"], r["rho"] * r["V"], 0.0, cv * r["rho"] * r["T"] + 0.5 * r["rho"] * r["V"] * r["V"]])
