@@ -50,7 +50,7 @@ void ctx_free(hg_ctx* c) {
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
                   c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
-                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG};
+                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG, c->d_exact_sides};
   for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -543,7 +543,21 @@ void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, cons
     }
   }
   if (c->riemann == HG_RIEMANN_EXACT) c->exact = true;
-  if (c->exact) c->d_FX = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
+  if (c->exact) {
+    c->d_FX = dalloc<char>(size_t(E) * 4 * P * 4 * rs);
+    // the sides whose Riemann problem the exact solver takes (the stage kernels' own selection)
+    std::vector<int> ex;
+    for (size_t es = 0; es < side.size(); ++es) {
+      const int kind = side[es].y & 15;
+      if (kind == SIDE_WALL || kind == SIDE_FLUX) continue;
+      int solver = c->riemann;
+      if (side[es].z >= 0 && zones[side[es].z].riemann >= 0) solver = zones[side[es].z].riemann;
+      if (solver == HG_RIEMANN_EXACT) ex.push_back(int(es));
+    }
+    c->n_exact_sides = int(ex.size());
+    c->d_exact_sides = dalloc<int>(ex.size());
+    HG_CUDA(cudaMemcpy(c->d_exact_sides, ex.data(), ex.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
   c->h_side = side;
   HG_CUDA(cudaMemcpy(c->d_side, side.data(), side.size() * sizeof(int4), cudaMemcpyHostToDevice));
   HG_CUDA(cudaMemcpy(c->d_mats, mats.data(), mats.size() * sizeof(double), cudaMemcpyHostToDevice));

@@ -55,6 +55,8 @@ struct hg_ctx {
   int tiling = 0;                 // elements-per-CTA variant of the stage kernels (hg_autotune / hg_set_tiling)
   bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
   void* d_FX = nullptr;           // its face fluxes of the current stage [n_el*4][P][4], context precision
+  int* d_exact_sides = nullptr;   // the element sides (e*4+s) whose face uses the exact solver
+  int n_exact_sides = 0;
   void* d_NF = nullptr;           // mortar fluxes of the SIDE_FLUX sides [slots][P][4], context precision
   void* d_NFG = nullptr;          // mortar BR1 gradient face terms of the SIDE_FLUX sides [slots][P][2][4]
   int ns_phase = 0;               // a composite's Navier-Stokes part: 0 whole stage, 1 gradient kernel, 2 stage kernel

@@ -12,13 +12,13 @@
 namespace hg {
 
 template <typename real>
-__global__ void __launch_bounds__(128) exact_flux_kernel(int n_el, int P, int affine, int riemann, const int4* side,
-                                                         const real* side_geo, const Zone* zones, const double* bq,
-                                                         const real* T, PhysConst pc, real* FX) {
+__global__ void __launch_bounds__(128) exact_flux_kernel(int n_sides, const int* sides, int P, int affine, int riemann,
+                                                         const int4* side, const real* side_geo, const Zone* zones,
+                                                         const double* bq, const real* T, PhysConst pc, real* FX) {
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= int64_t(n_el) * 4 * P) return;
+  if (idx >= int64_t(n_sides) * P) return;
   const int kk = int(idx % P);
-  const int64_t es = idx / P;          // element * 4 + side
+  const int64_t es = sides[idx / P];   // element * 4 + side of a face that uses the exact solver
   const int4 sd = side[es];
   const int kind = sd.y & 15;
   if (kind == SIDE_WALL || kind == SIDE_FLUX) return;   // prescribed wall flux / mortar face: no Riemann problem here
@@ -55,14 +55,19 @@ __global__ void __launch_bounds__(128) exact_flux_kernel(int n_el, int P, int af
 
 }  // namespace hg
 
+// One thread per node of the element sides whose face uses the exact solver (a list built at
+// hg_create: all Riemann faces when it is the interior solver, else the sides of the zones that
+// select it).
 template <typename real>
 void launch_exact_flux(hg_ctx* c) {
-  const int64_t n = int64_t(c->n_el) * 4 * c->P;
+  if (c->n_exact_sides == 0) return;
+  const int64_t n = int64_t(c->n_exact_sides) * c->P;
   const unsigned grid = unsigned((n + 127) / 128);
   timed(c, HG_KERNEL_FACEFLUX, [&] {
     exact_flux_kernel<real><<<grid, 128, 0, c->stream>>>(
-        c->n_el, c->P, c->affine ? 1 : 0, c->riemann, c->d_side, static_cast<const real*>(c->d_side_geo), c->d_zones,
-        c->d_bq, static_cast<const real*>(c->d_T[c->cur]), c->pc, static_cast<real*>(c->d_FX));
+        c->n_exact_sides, c->d_exact_sides, c->P, c->affine ? 1 : 0, c->riemann, c->d_side,
+        static_cast<const real*>(c->d_side_geo), c->d_zones, c->d_bq, static_cast<const real*>(c->d_T[c->cur]), c->pc,
+        static_cast<real*>(c->d_FX));
   });
   ++c->launches;
 }
