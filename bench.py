@@ -149,23 +149,105 @@ def build_parts(config):
     return parts
 
 
-def stage_bytes_per_dof(config, prec_fp32, affine, ns=False):
-    """Algorithmic DRAM bytes per DOF of one launch of the fused stage kernel (RK3 average).
+def step_bytes_per_dof_stage(fp32, affine, br1):
+    """Algorithmic DRAM bytes per DOF-stage of a Williamson RK3 step with fused stages: the state Q read
+    and written in FP64 every stage (16 B), the RK register G written every stage and read in stages 2-3
+    (sG = 4 or 8 B: 5/3 sG), the volume metrics Ja, 1/J on curved meshes (5 values per node: 1.25 sG;
+    0 on affine meshes, whose metrics are per element), and with BR1 the lifted gradient written and read
+    back (8 values per node: 4 sG).  Interior-penalty gradients are element-local (0).  Face traces and
+    nodal matrices count 0 (cache-resident).  FP64: 29.33 affine, +10 curved, +32 BR1."""
+    sg = 4.0 if fp32 else 8.0
+    return 16.0 + sg * 5.0 / 3.0 + (0.0 if affine else 1.25 * sg) + (4.0 * sg if br1 else 0.0)
 
-    State Q read + written in FP64 (16 B), RK register G written every stage and read in
-    stages 2-3 (sG = 4 or 8 B), volume metrics (Ja, 1/J: 5 values per node in the arithmetic
-    precision = 10 or 5 B/DOF) on curved meshes, 0 on affine ones; Navier-Stokes: the element
-    gradient written by the gradient kernel is read back (8 values per node = 2 sG B/DOF).
-    Face traces and nodal matrices are cache-resident."""
-    sg = 4 if prec_fp32 else 8
-    return 16.0 + sg * (1.0 + 2.0 / 3.0) + (0.0 if affine else 1.25 * sg) + (2.0 * sg if ns else 0.0)
+
+def stage_kernel_bytes_per_dof(fp32, affine, br1):
+    """The share of those bytes that the stage kernel moves: all of them except, with BR1, the gradient
+    write (2 sG), which the gradient kernel makes."""
+    return step_bytes_per_dof_stage(fp32, affine, br1) - ((8.0 if fp32 else 16.0) if br1 else 0.0)
 
 
-def gradient_bytes_per_dof(prec_fp32, affine):
-    """Navier-Stokes gradient pass: Q read (8 B), volume metrics (1.25 sG B/DOF when curved), the
-    element gradient written (2 sG B/DOF)."""
-    sg = 4 if prec_fp32 else 8
-    return 8.0 + (0.0 if affine else 1.25 * sg) + 2.0 * sg
+def roofline_from_split(split, split_steps, ms_step, ndof, fp32, affine, br1, peak, peak_kind, traffic_name=None,
+                        ns=True):
+    """Roofline of the dominant kernel (the stage kernel) from the timed region: its average launch time
+    is its share of the per-kernel event times (library timing mode, `split`) times the timed
+    milliseconds per step, divided by its launches per step; achieved = its algorithmic bytes per launch
+    over that time.  Also the whole step's algorithmic bytes over the timed step."""
+    total = sum(v[0] for v in split.values()) or 1.0
+    share = {k: round(v[0] / total, 4) for k, v in split.items() if v[1]}
+    st_ms, st_n = split["stage"]
+    per_step = st_n / split_steps
+    avg_s = (st_ms / total) * ms_step * 1e-3 / per_step
+    dof_per_launch = ndof * 3.0 / per_step
+    kbpd = stage_kernel_bytes_per_dof(fp32, affine, br1)
+    achieved = kbpd * dof_per_launch / avg_s / 1e9
+    traffic = None
+    if traffic_name:
+        tpath = os.path.join(ROOT, "profiles", f"{traffic_name}.traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath))["bytes_per_dof"] * dof_per_launch
+            except Exception:
+                traffic = None
+    sbpd = step_bytes_per_dof_stage(fp32, affine, br1)
+    step_ach = sbpd * ndof * 3.0 / (ms_step * 1e-3) / 1e9
+    kernel = {"bound": "hbm", "kernel": "ns_stage_kernel" if ns else "stage_kernel",
+              "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+              "peak_source": peak_kind, "algorithmic_bytes_per_dof": kbpd, "avg_launch_us": avg_s * 1e6,
+              "launch_time_from": "kernel share of the library's per-launch events x timed ms per step"}
+    step = {"algorithmic_bytes_per_dof_stage": sbpd, "achieved": step_ach, "frac": step_ach / peak}
+    return {"kernel": kernel, "step": step, "share": share}
+
+
+def kh_dt(n):
+    """Time step of the kh workload at n x n elements: half the measured interior-penalty limit
+    (the reference's estimate is inviscid only; measured on the oracle, dt_max ~ 0.1 / n^2)."""
+    return KH_DT_COEF / n ** 2
+
+
+KH_PHYSICS = ("Navier-Stokes, Re 1e4, M 0.3, Pr 0.72, periodic, SIPG (sigma0 10), Roe, Laplacian artificial "
+              "viscosity")
+
+
+def workload_ndof(name, args):
+    """NDOF = 4 x nodes of a workload, from its definition (no device needed)."""
+    if name == "kh":
+        return 4 * args.kh_n ** 2 * 64
+    if name == "cylinder":
+        return 4 * 64 * 128 * 36
+    if name == "shock":
+        return 4 * 512 * 64 * 16
+    if name == "vortex16":
+        return 4 * 16 * 16 * 25
+    if name == "box512":
+        return 4 * 512 * 512 * 25
+    if name == "prefine":
+        return int(4 * np.sum((prefine_orders(384) + 1) ** 2))
+    return int(sum(4 * it["n"] ** 2 * (it["N"] + 1) ** 2 for it in ensemble_spec()))
+
+
+def workload_config(name, args, world):
+    """The `config` object of a workload: what is run, identical in both arms (measured quantities and
+    the autotuner's choice go elsewhere in the line)."""
+    ndof = workload_ndof(name, args)
+    par = f"replicas x{world}"
+    l2 = ("256 MB buffer written between timed steps (outside the step events)" if ndof * 8 * 3 < 2 * L2_BYTES
+          else "inputs larger than L2")
+    if name == "kh":
+        n = args.kh_n
+        return {"workload": "kh", "ndof": ndof, "mesh": f"{n}x{n}", "N": 7, "nodes": "Legendre-Gauss",
+                "precision": "fp64", "physics": KH_PHYSICS, "sensor": "modal decay (the plain method)",
+                "dt": kh_dt(n), "scheme": "Williamson RK3", "l2": l2, "parallelism": par}
+    if name == "shock":
+        return {"workload": "shock", "ndof": ndof, "mesh": "512x64", "N": 3, "nodes": "Legendre-Gauss",
+                "precision": "fp32", "physics": "Navier-Stokes build at Re 0, Mach-3 shock, HLL, SIPG, Laplacian "
+                "artificial viscosity", "sensor": "learned (MLP 16-32-32-1) with modal fallback",
+                "scheme": "Williamson RK3", "l2": l2, "parallelism": par}
+    prec = args.precision or ("fp32" if name == "ensemble" else "fp64")
+    orders = {"cylinder": [5], "vortex16": [4], "box512": [4], "prefine": ["5/7"],
+              "ensemble": [3, 4, 5, 6, 7]}[name]
+    return {"workload": name, "ndof": ndof, "precision": prec, "orders": orders,
+            "instances": 512 if name == "ensemble" else 1, "scheme": "Williamson RK3", "l2": l2,
+            "parallelism": par}
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -343,7 +425,7 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.config},
+            "config": workload_config(args.config, args, world),
             "cpu_baseline": {"value": value, "unit": "DOF-stage/s", "cores": cores, "kind": "port",
                              "sample": f"each step: {sample}"},
             "e2e": {"value": value, "unit": "DOF-stage/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -547,28 +629,18 @@ def run_shock(args, rank, world, local, dist):
     ms32, ms64, e2e_ms = max_over_ranks([ms32, ms64, e2e_ms], world, dist)
     value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
     value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
-    bpd = stage_bytes_per_dof("shock", True, True, True)
-    st_ms, st_n = split["stage"]
-    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
-    achieved = bpd * ndof / avg_stage_s / 1e9
     peak, peak_kind = peaks()
-    total_split = sum(v[0] for v in split.values()) or 1.0
+    split_steps = max(3, min(args.steps, 10))
+    roof = roofline_from_split(split, split_steps, ms32 / args.steps, ndof, True, True, False, peak, peak_kind,
+                               "ns_stage_kernel_shock_fp32")
     line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
-            "config": {"workload": "shock", "ndof": ndof, "mesh": f"{nx}x{ny}", "N": N, "precision": "fp32",
-                       "tiling": tiling_summary(c32),
-                       "sensor": "learned (MLP 16-32-32-1) with modal fallback", "scheme": "Williamson RK3",
-                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
-                              if flush.buf is not None else "inputs larger than L2"),
-                       "parallelism": f"replicas x{world}"},
+            "config": workload_config("shock", args, world), "tiling": tiling_summary(c32),
             "e2e": {"value": ndof * 3 * args.steps * world / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
                     "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
-            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
+            "roofline": roof["kernel"], "step_roofline": roof["step"], "kernel_share": roof["share"],
             "fp64_plain_modal": {"value": value64, "ms_per_step": ms64 / args.steps, "speedup_fp32_learned": ms64 / ms32},
             "accuracy": {"rel_l2_density_fp32_vs_fp64_after_200_steps": rho_err},
             "sensor": {"training_s": train_s, "samples": info["samples"], "snapshots": 200,
@@ -588,108 +660,181 @@ def run_shock(args, rank, world, local, dist):
         dist.destroy_process_group()
 
 
+def kh_state_pinned(n, N, xi, seed):
+    """The kh initial state (cases.kelvin_helmholtz at the box's nodes) in pinned host memory: the
+    separable factors are evaluated on the host and multiplied out on the device (input preparation,
+    outside every timed region), then copied once into the pinned buffer that the e2e leg uploads."""
+    import torch
+    from horses2d_b200 import cases
+    rho_y, u_y, damp_y, vx = (torch.from_numpy(a).cuda() for a in cases.kelvin_helmholtz_factors(n, N, xi, seed=seed))
+    P = N + 1
+    rho = rho_y[:, None, :, None].expand(n, n, P, P)
+    uu = u_y[:, None, :, None].expand(n, n, P, P)
+    v = vx[None, :, None, :] * damp_y[:, None, :, None]
+    Q = torch.empty((n, n, P, P, 4), dtype=torch.float64, device="cuda")
+    Q[..., 0] = rho
+    Q[..., 1] = rho * uu
+    Q[..., 2] = rho * v
+    Q[..., 3] = 1.0 / 0.4 + 0.5 * rho * (uu * uu + v * v)
+    host = torch.empty(Q.numel(), dtype=torch.float64).pin_memory()
+    host.copy_(Q.reshape(-1))
+    del Q, v
+    torch.cuda.synchronize()
+    return host
+
+
+def kh_kwargs(hg):
+    return dict(mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0,
+                node_type=hg.NODES_LG, riemann=hg.ROE, av_type=hg.AV_LAPLACIAN, av_intensity=1.0,
+                bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+
+
+def kh_accuracy(params, lo, hi, n=32, steps=100):
+    """Density error of the device paths against the FP64 oracle on a bounded sample of the kh workload
+    (n x n elements, same order, physics and dt rule; `steps` RK3 steps from the same state): FP64 plain
+    and FP32 plain against the oracle with the modal indicator, FP32 + learned against the oracle with
+    the FP64 restatement of the learned indicator (oracle/mlp.py).  The oracle is the checker here."""
+    import horses2d_b200 as hg
+    from horses2d_b200 import mesh as hmesh, cases
+    from oracle import oracle as O, mlp as omlp
+    O.lib().or_set_threads(os.cpu_count() or 1)
+    N, dt = 7, kh_dt(n)
+    okw = dict(nodes=O.LG, riemann=O.ROE, mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=O.IP, ip_method=0,
+               sigma0_ip=10.0, bcs=hmesh.periodic_bcs_cartesian(), av_type=O.AV_LAPLACIAN, av_intensity=1.0)
+    m = hmesh.cartesian(n, n, 0.0, 1.0, 0.0, 1.0)
+    om = O.Oracle(m, N, av_indicator=O.IND_MODAL, **okw)
+    ol = O.Oracle(m, N, av_indicator=O.IND_EXTERNAL, **okw)
+    X = om.coords()
+    Q0 = cases.kelvin_helmholtz(X[:, 0], X[:, 1], seed=SEED).ravel()
+    t0 = time.perf_counter()
+    om.set_state(Q0)
+    ol.set_state(Q0)
+    xi = omlp.gauss_nodes(N + 1)
+    s0 = np.log10(1.0 / (N + 1) ** 4)
+    for k in range(steps):
+        om.time_step(O.RK3, k * dt, dt)
+        omlp.step_learned(ol, params, lo, hi, xi, O.RK3, k * dt, dt, s0)
+    oracle_s = time.perf_counter() - t0
+    ref = {"modal": om.state()[0::4], "learned": ol.state()[0::4]}
+    desc = om.export_mesh()
+    out = {}
+    for name, prec, sensor, against in (("fp64_plain", hg.PREC_FP64, hg.SENSOR_MODAL, "modal"),
+                                        ("fp32_plain", hg.PREC_FP32, hg.SENSOR_MODAL, "modal"),
+                                        ("fp32_learned", hg.PREC_FP32, hg.SENSOR_LEARNED, "learned")):
+        g = hg.GpuDGSEM(desc, precision=prec, **kh_kwargs(hg))
+        if sensor == hg.SENSOR_LEARNED:
+            g.set_sensor(sensor, mlp=params, lo=lo, hi=hi)
+        else:
+            g.set_sensor(sensor)
+        g.set_state(Q0)
+        g.time_steps(hg.SCHEME_RK3, steps, 0.0, dt)
+        r = g.state()[0::4]
+        out[name] = float(np.linalg.norm(r - ref[against]) / np.linalg.norm(ref[against]))
+        g.close()
+    return {"sample": f"{n}x{n} elements of the kh workload (N=7, same physics, dt = {KH_DT_COEF}/n^2 = {dt:.3e}), "
+                      f"{steps} RK3 steps from the same state (t = {steps * dt:.3e}); oracle runs {oracle_s:.1f} s",
+            "reference": "FP64 oracle: modal indicator for the plain paths; for fp32_learned the oracle with the "
+                         "learned indicator evaluated in FP64 (oracle/mlp.py) at each step's start",
+            "rel_l2_density": out, "tolerance": 1e-5}
+
+
 def run_kh(args, rank, world, local, dist):
-    """Kelvin-Helmholtz shear layer (NS, SIPG, Roe, Laplacian artificial viscosity driven by the learned
-    sensor): FP32 + learned timed beside FP64 + modal on the same workload; density error of FP32 +
-    learned against FP64 + learned after K steps from the same state."""
+    """The Kelvin-Helmholtz shear layer (configuration C5: NS, SIPG, Roe, Laplacian artificial viscosity).
+    value = the plain FP64 path (modal-decay sensor); the FP32-bulk + learned-sensor path is timed beside
+    it on the same workload; roofline of the dominant kernel from the timed region; density error of each
+    path against the FP64 oracle on a bounded sample."""
     import torch
     import horses2d_b200 as hg
-    from horses2d_b200 import sensor as S, mesh as hmesh, cases
+    from horses2d_b200 import sensor as S, mesh as hmesh
     n, N = args.kh_n, 7
+    cfg = workload_config("kh", args, world)
     t0 = time.perf_counter()
     params, lo, hi, info = S.train_two_rounds(100, SEED, nx=512, ny=64, N=3, steps=100, epochs=30, batch=4096)
     train_s = time.perf_counter() - t0
+    xi, _ = hg._lib.nodes(N, hg.NODES_LG)
+    Qh = kh_state_pinned(n, N, xi, SEED)
     desc = hmesh.box_descriptor(n, n, 0.0, 1.0, 0.0, 1.0, N, hg.NODES_LG)
-    x = desc["x"].reshape(-1, 2)
-    Q0 = cases.kelvin_helmholtz(x[:, 0], x[:, 1], seed=SEED).ravel()
-    del x
-    kw = dict(mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0,
-              node_type=hg.NODES_LG, riemann=hg.ROE, av_type=hg.AV_LAPLACIAN, av_intensity=1.0,
-              bcs=[dict(type=hg.BC_PERIODIC)] * 4)
     stream = torch.cuda.Stream()
-    parts = [(desc, Q0, N, 1, kw, 0.2)]
-    c32 = make_contexts(parts, hg.PREC_FP32, stream)
-    c32[0]["g"].set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
-    c32[0]["tune"] = c32[0]["g"].autotune(trials=10)    # again, with the sensor that will run
-    c64 = make_contexts(parts, hg.PREC_FP64, stream)
-    c64[0]["g"].set_sensor(hg.SENSOR_MODAL)
-    c64[0]["tune"] = c64[0]["g"].autotune(trials=10)
+
+    def context(prec, learned):
+        g = hg.GpuDGSEM(desc, precision=prec, **kh_kwargs(hg))
+        g.set_stream(stream.cuda_stream)
+        g.set_state(Qh.numpy())
+        if learned:
+            g.set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
+        else:
+            g.set_sensor(hg.SENSOR_MODAL)
+        return dict(g=g, Qh=Qh, N=N, ninst=1, cfl=None, tune=g.autotune(trials=5))
+
+    c64 = [context(hg.PREC_FP64, False)]
+    c32 = [context(hg.PREC_FP32, True)]
     del desc
-    g32, g64 = c32[0]["g"], c64[0]["g"]
-    ndof = g32.ndof
-    # the interior-penalty terms at Re 1e4, N = 7 limit the step like h^2 (the reference's estimate is
-    # inviscid only): measured on the oracle, dt_max ~ 0.1 / n^2 at 32^2 and 64^2; half of it is used
-    dt = min(g64.estimate_time_step(0.2, 1.0), KH_DT_COEF / n ** 2)
-    flush = L2Flush(ndof * 8 * 3 < 2 * L2_BYTES)
+    g64, g32 = c64[0]["g"], c32[0]["g"]
+    ndof = g64.ndof
+    assert ndof == cfg["ndof"]
+    dt = cfg["dt"]
+    flush = L2Flush(False)       # Q alone is 2.1 GB: inputs larger than L2
     clocks = ClockSampler(local)
     clocks.start()
-    ms32, launches = device_timed(c32, args.steps, args.warmup, dt, stream, world, dist, flush, min_load_s=2.0)
+    ms64, launches = device_timed(c64, args.steps, args.warmup, dt, stream, world, dist, flush, min_load_s=2.0)
     clk = clocks.stop()
-    ms64, _ = device_timed(c64, args.steps, args.warmup, dt, stream, world, dist, flush)
-    split = kernel_split(c32, max(3, min(args.steps, 10)), dt, stream, flush)
-    # accuracy: FP32 + learned against FP64 + learned, K steps from the same state
-    g64.set_sensor(hg.SENSOR_LEARNED, mlp=params, lo=lo, hi=hi)
-    for g in (g32, g64):
-        g.set_state(Q0)
-        g.time_steps(hg.SCHEME_RK3, args.steps, 0.0, dt)
-    r32 = g32.state()[0::4]
-    r64 = g64.state()[0::4]
-    rho_err = float(np.linalg.norm(r32 - r64) / np.linalg.norm(r64))
-    del r32, r64
+    ms32, _ = device_timed(c32, args.steps, args.warmup, dt, stream, world, dist, flush)
+    split_steps = max(3, min(args.steps, 5))
+    split64 = kernel_split(c64, split_steps, dt, stream, flush)
+    split32 = kernel_split(c32, split_steps, dt, stream, flush)
+    # sensor statistics of the learned path on the stepped state
     _, out32 = g32.sensor_eval()
-    # end to end through the public API with host buffers (FP32 + learned)
-    Qpin = torch.empty(g32.ndof, dtype=torch.float64).pin_memory()
+    # end to end through the public API with host buffers (plain FP64 path): state from pinned host,
+    # K x (hg_time_step + hg_residuals), the final state into pinned host
+    Qpin = torch.empty(ndof, dtype=torch.float64).pin_memory()
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    g32.set_state(c32[0]["Qh"].numpy())
+    g64.set_state(Qh.numpy())
     res = np.zeros(4)
-    for s in range(args.steps):
-        g32.time_step(hg.SCHEME_RK3, s * dt, dt)
-        res = np.maximum(res, g32.residuals())
-    Qe = g32.state(out=Qpin.numpy())
+    for k in range(args.steps):
+        g64.time_step(hg.SCHEME_RK3, k * dt, dt)
+        res = np.maximum(res, g64.residuals())
+    Qe = g64.state(out=Qpin.numpy())
     e2e_ms = (time.perf_counter() - t1) * 1e3
     if not (np.all(np.isfinite(Qe)) and np.all(np.isfinite(res))):
         raise SystemExit("non-finite state after the timed steps")
     del Qe
-    ms32, ms64, e2e_ms = max_over_ranks([ms32, ms64, e2e_ms], world, dist)
-    value = ndof * 3 * args.steps * world / (ms32 * 1e-3)
-    value64 = ndof * 3 * args.steps * world / (ms64 * 1e-3)
-    bpd = stage_bytes_per_dof("kh", True, True, True)
-    st_ms, st_n = split["stage"]
-    avg_stage_s = st_ms * 1e-3 / max(st_n, 1)
-    achieved = bpd * ndof / avg_stage_s / 1e9
+    ms64, ms32, e2e_ms = max_over_ranks([ms64, ms32, e2e_ms], world, dist)
+    value = ndof * 3 * args.steps * world / (ms64 * 1e-3)
+    value32 = ndof * 3 * args.steps * world / (ms32 * 1e-3)
     peak, peak_kind = peaks()
-    total_split = sum(v[0] for v in split.values()) or 1.0
+    roof64 = roofline_from_split(split64, split_steps, ms64 / args.steps, ndof, False, True, False, peak, peak_kind,
+                                 "ns_stage_kernel_kh_fp64")
+    roof32 = roofline_from_split(split32, split_steps, ms32 / args.steps, ndof, True, True, False, peak, peak_kind,
+                                 "ns_stage_kernel_kh_fp32")
+    troubled = float((out32[:, 3] > S.TROUBLED).mean())
     line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms32 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc", "data": "synthetic",
-            "config": {"workload": "kh", "ndof": ndof, "mesh": f"{n}x{n}", "N": N, "precision": "fp32",
-                       "tiling": tiling_summary(c32),
-                       "physics": "NS Re 1e4 M 0.3, SIPG (sigma0 10), Roe, Laplacian artificial viscosity",
-                       "dt": dt,
-                       "sensor": "learned (MLP 16-32-32-1, trained on the shock workload's snapshots at N=3) "
-                                 "with modal fallback",
-                       "scheme": "Williamson RK3",
-                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
-                              if flush.buf is not None else "inputs larger than L2"),
-                       "parallelism": f"replicas x{world}"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms64 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
+            "tiling": tiling_summary(c64),
             "e2e": {"value": ndof * 3 * args.steps * world / (e2e_ms * 1e-3), "unit": "DOF-stage/s",
-                    "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps},
+                    "h2d_bytes_per_step": ndof * 8 / args.steps, "d2h_bytes_per_step": 32 + ndof * 8 / args.steps,
+                    "note": "hg_set_state from pinned host, K x (hg_time_step + hg_residuals), hg_get_state into "
+                            "pinned host; plain FP64 path"},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
-            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
-            "fp64_plain_modal": {"value": value64, "ms_per_step": ms64 / args.steps,
-                                 "speedup_fp32_learned": ms64 / ms32},
-            "accuracy": {f"rel_l2_density_fp32_vs_fp64_after_{args.steps}_steps": rho_err},
-            "sensor": {"training_s": train_s, "ood_fraction": float(out32[:, 2].mean()),
-                       "troubled_fraction": float((out32[:, 3] > 0.5).mean()),
-                       "disagreement_vs_modal": S.disagreement(out32[:, 0], out32[:, 3])},
+            "roofline": roof64["kernel"], "step_roofline": roof64["step"], "kernel_share": roof64["share"],
+            "fp32_learned": {"value": value32, "ms_per_step": ms32 / args.steps, "dtype": "f32+f64acc",
+                             "speedup_vs_fp64_plain": ms64 / ms32, "tiling": tiling_summary(c32),
+                             "roofline": roof32["kernel"], "step_roofline": roof32["step"],
+                             "kernel_share": roof32["share"],
+                             "sensor": {"training_s": train_s, "training_snapshots": 200,
+                                        "troubled_fraction": troubled,
+                                        "ood_fraction": float(out32[:, 2].mean()),
+                                        "disagreement_vs_modal": S.disagreement(out32[:, 0], out32[:, 3]),
+                                        "note": ("the learned indicator runs every step (inference fused into the "
+                                                 "gradient pass); the shear layer is smooth, and it flags "
+                                                 f"{troubled:.1%} of the elements (the modal indicator: "
+                                                 f"{float((out32[:, 0] > S.TROUBLED).mean()):.1%})")}},
             "clocks": clk}
     if rank == 0 and not args.no_cpu_baseline:
         rate, cores, sample = CpuArm("kh").sample(12.0)
         line["cpu_baseline"] = {"value": rate, "unit": "DOF-stage/s", "cores": cores, "kind": "port", "sample": sample}
+        line["accuracy"] = kh_accuracy(params, lo, hi)
     line["node_stage_per_s"] = line["value"] / 4.0   # DOF-stage/s over the 4 variables of a node
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -705,7 +850,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="cylinder", choices=CONFIGS)
+    ap.add_argument("--config", default="kh", choices=CONFIGS)
     ap.add_argument("--precision", default=None, choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--kh-n", type=int, default=1024, help="elements per side of the kh workload")
@@ -768,48 +913,22 @@ def main():
     value = ndof * 3 * args.steps * world / (ms * 1e-3)
     e2e = ndof * 3 * args.steps * world / (e2e_ms * 1e-3)
 
-    # ---- roofline of the dominant kernel (fused stage kernel), from its own event times
-    bpd = stage_bytes_per_dof(args.config, prec == hg.PREC_FP32, affine, ns)
-    st_ms, st_n = split["stage"]
-    # one stage of a mixed-order context is one launch per order part (the parts share the bytes)
-    parts_per_stage = 2 if args.config == "prefine" else 1
-    avg_stage_s = st_ms * 1e-3 / max(st_n, 1) * parts_per_stage
-    stage_launch_bytes = bpd * ndof / len(ctxs)
-    achieved = stage_launch_bytes / avg_stage_s / 1e9
+    # ---- roofline of the dominant kernel (fused stage kernel), launch time from the timed region
     peak, peak_kind = peaks()
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", f"stage_kernel_{args.config}_{precision}.traffic.json")
-    if os.path.exists(tpath):
-        try:
-            traffic = json.load(open(tpath))["bytes_per_dof"] * ndof / len(ctxs)
-        except Exception:
-            traffic = None
-    step_bytes_per_dof_stage = bpd + (gradient_bytes_per_dof(prec == hg.PREC_FP32, affine) if ns else 0.0)
-    step_achieved = step_bytes_per_dof_stage * ndof * 3 * args.steps / (ms * 1e-3) / 1e9
-    total_split = sum(v[0] for v in split.values()) or 1.0
+    br1 = any(p[4].get("navier_stokes") and p[4].get("viscous", 0) == hg.BR1 for p in parts)
+    roof = roofline_from_split(split, max(3, min(args.steps, 10)), ms / args.steps, ndof, prec == hg.PREC_FP32,
+                               affine, br1, peak, peak_kind,
+                               f"{'ns_' if ns else ''}stage_kernel_{args.config}_{precision}", ns=ns)
     line = {"metric": "DOF-stage updates/s", "value": value, "unit": "DOF-stage/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64acc" if prec == hg.PREC_FP32 else "f64",
-            "data": "synthetic",
-            "config": {"workload": args.config, "ndof": ndof, "precision": precision,
-                       "orders": [c["N"] for c in ctxs], "instances": sum(c["ninst"] for c in ctxs),
-                       "tiling": tiling_summary(ctxs),
-                       "scheme": "Williamson RK3",
-                       "l2": ("256 MB buffer written between timed steps (outside the step events)"
-                              if flush.buf is not None else "inputs larger than L2"),
-                       "parallelism": f"replicas x{world}"},
+            "data": "synthetic", "config": workload_config(args.config, args, world), "tiling": tiling_summary(ctxs),
             "e2e": {"value": e2e, "unit": "DOF-stage/s", "h2d_bytes_per_step": ndof * 8 / args.steps,
                     "d2h_bytes_per_step": 32 * len(ctxs) + ndof * 8 / args.steps,
                     "note": "hg_set_state from pinned host, K x (hg_time_step + hg_residuals), hg_get_state "
                             "into pinned host; consecutive steps, no L2 flush"},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "kernel": "ns_stage_kernel" if ns else "stage_kernel",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes_per_dof": bpd, "avg_launch_us": avg_stage_s * 1e6},
-            "step_roofline": {"algorithmic_bytes_per_dof_stage": step_bytes_per_dof_stage,
-                              "achieved": step_achieved, "frac": step_achieved / peak},
-            "kernel_share": {k: round(v[0] / total_split, 4) for k, v in split.items() if v[1]},
+            "roofline": roof["kernel"], "step_roofline": roof["step"], "kernel_share": roof["share"],
             "clocks": clk}
 
     # ---- FP32-bulk companion on the same workload (FP64 runs): speed and density error after K steps

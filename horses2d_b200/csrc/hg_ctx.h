@@ -93,7 +93,11 @@ struct hg_ctx {
   double g_dt = 0.0;
   int64_t g_launches[2] = {0, 0};
   // CUDA graphs of one time step (hg_time_step), per parity at its start: captured the second time a
-  // step of the same scheme and dt starts at that parity
+  // step of the same scheme and dt starts at that parity.
+  // Rule for every graph above and below: a captured launch holds its kernel arguments and device
+  // pointers by value, so any call that changes a kernel argument or replaces a device buffer must call
+  // drop_graph (hg_api.cu); a call that only rewrites the contents of an existing buffer need not (the
+  // replay reads the buffer then).  The step time t enters no kernel.
   cudaGraphExec_t gexec1[2] = {nullptr, nullptr};
   int g1_scheme = -1;
   double g1_dt = 0.0;

@@ -2,11 +2,11 @@
 // without allocating device memory (declared in include/horses_gpu.h).
 //
 // The per-block partial maxima and the four results live in one file-scope device array of fixed
-// size (na_scratch, 512 KB + 32 B).  Its address is looked up once per device with
-// cudaGetSymbolAddress on the first call made with that device current.  Nothing in the scratch
-// has to start at zero: every slot a call reads was written earlier in the same call, on the same
-// stream.  Two calls that overlap in time on one device (different streams or host threads) share
-// the scratch and race; callers serialise them.
+// size (na_scratch, 512 KB + 32 B).  Every call looks up its address on the current device with
+// cudaGetSymbolAddress (a host-side lookup; nothing is cached, so a reset device or another host
+// thread never sees a stale address).  Nothing in the scratch has to start at zero: every slot a call
+// reads was written earlier in the same call, on the same stream.  Two calls that overlap in time on
+// one device (different streams or host threads) share the scratch and race; callers serialise them.
 #include "../../include/horses_gpu.h"
 
 #include <cuda_runtime.h>
@@ -16,12 +16,9 @@ namespace {
 constexpr int NA_THREADS = 256;
 constexpr int64_t NA_NODES_PER_BLOCK = 8192;   // 32 nodes per thread
 constexpr int NA_MAX_BLOCKS = 16384;           // partials: 16384 x 4 doubles = 512 KB
-constexpr int NA_MAX_DEVICES = 64;
 static_assert(int64_t(NA_MAX_BLOCKS) * NA_NODES_PER_BLOCK * 4 == HG_NOALLOC_MAX_NDOF, "scratch size and limit");
 
 static __device__ __align__(256) double na_scratch[NA_MAX_BLOCKS * 4 + 4];
-
-double* g_scratch[NA_MAX_DEVICES] = {};
 
 __device__ __forceinline__ double na_max(double m, double v) { return (v > m || v != v) ? v : m; }
 
@@ -75,19 +72,18 @@ __global__ void __launch_bounds__(NA_THREADS) na_reduce_kernel(int nblocks, cons
 extern "C" int hg_residuals_noalloc(const double* qdot, int64_t ndof, void* cuda_stream, double out[4]) {
   if (!qdot || !out || ndof <= 0 || ndof % 4 != 0 || ndof > HG_NOALLOC_MAX_NDOF) return 1;
   if ((reinterpret_cast<uintptr_t>(qdot) & 31) != 0) return 1;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return 2;
-  if (!g_scratch[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return 2;
-    g_scratch[dev] = static_cast<double*>(p);
-  }
-  double* part = g_scratch[dev];
+  // an error left pending by earlier work on this thread is not this call's: report it as such and
+  // leave it pending for the code that caused it
+  if (cudaPeekAtLastError() != cudaSuccess) return 4;
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, na_scratch) != cudaSuccess || !p) return 2;
+  double* part = static_cast<double*>(p);
   double* res = part + size_t(NA_MAX_BLOCKS) * 4;
   cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
   const int64_t n_nodes = ndof / 4;
   const int nblocks = int((n_nodes + NA_NODES_PER_BLOCK - 1) / NA_NODES_PER_BLOCK);
   na_partial_kernel<<<nblocks, NA_THREADS, 0, st>>>(qdot, n_nodes, part);
+  if (cudaGetLastError() != cudaSuccess) return 3;
   na_reduce_kernel<<<1, NA_THREADS, 0, st>>>(nblocks, part, res);
   if (cudaGetLastError() != cudaSuccess) return 3;
   if (cudaMemcpyAsync(out, res, 4 * sizeof(double), cudaMemcpyDeviceToHost, st) != cudaSuccess) return 3;

@@ -193,11 +193,12 @@ int  hg_kernel_times(hg_ctx* ctx, double* ms, int64_t* launches, int32_t n);
  * larger or malformed sizes are rejected before any launch.  For callers that hold a QDot (or
  * any state-shaped) array on the device and may not allocate, e.g. a monitor running inside a
  * fixed device-memory budget.  Runs on cuda_stream (NULL: legacy default stream) and
- * synchronises it.  The first call with a device current looks up the scratch address for that
- * device (cudaGetSymbolAddress); make one call before any stream capture if you capture.  Calls
- * that overlap in time on one device share the scratch and race: serialise them.
+ * synchronises it, so it must not be called on a stream that is being captured.  Each call looks
+ * up the scratch address on the current device (cudaGetSymbolAddress).  Calls that overlap in time
+ * on one device share the scratch and race: serialise them.
  * Returns 0 ok, 1 bad argument (null, ndof <= 0, not a multiple of 4, above the limit,
- * misaligned), 2 set-up failed, 3 launch or copy failed. */
+ * misaligned), 2 set-up failed, 3 launch or copy failed, 4 an error from earlier work was already
+ * pending on this thread (left pending; nothing launched). */
 #define HG_NOALLOC_MAX_NDOF 536870912LL
 int  hg_residuals_noalloc(const double* qdot, int64_t ndof, void* cuda_stream, double out[4]);
 /* Shock sensor of the artificial dissipation (no reference counterpart beyond HG_SENSOR_JUMPS, the

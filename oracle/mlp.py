@@ -97,3 +97,31 @@ def element_features(Q, xi, gamma=1.4):
 
 def ramp(s, s0, kappa):
     return np.where(s < s0 - kappa, 0.0, np.where(s < s0 + kappa, 0.5 * np.sin(0.5 * np.pi * (s - s0) / kappa) + 0.5, 1.0))
+
+
+def gauss_nodes(P):
+    """Legendre-Gauss nodes on [0,1] (numpy's Golub-Welsch nodes; the checker needs no bitwise match)."""
+    x, _ = np.polynomial.legendre.leggauss(P)
+    return 0.5 * (x + 1.0)
+
+
+def learned_indicator(params, lo, hi, Q, xi, s0, kappa=1.0):
+    """Per-element G of the learned indicator, as the device forms it (hg_sensor.cuh element_sensor):
+    the network's sigmoid output on the element's 16 features, or the modal-decay G (sine ramp of the
+    modal indicator around s0, half width kappa) where a feature, rounded to FP32, lies outside the
+    training box [lo, hi] (the out-of-distribution fallback).  FP64 throughout."""
+    X, s = element_features(Q, xi)
+    g_modal = ramp(s, s0, kappa)
+    X32 = X.astype(np.float32)
+    ood = np.any((X32 < np.asarray(lo, np.float32)) | (X32 > np.asarray(hi, np.float32)), axis=1)
+    return np.where(ood, g_modal, predict(params, X)), ood
+
+
+def step_learned(orc, params, lo, hi, xi, scheme, t, dt, s0, kappa=1.0):
+    """One time step of an oracle built with the external indicator (IND_EXTERNAL), with G set from the
+    learned indicator of the state at the start of the step (the device holds the indicator of the
+    step's first stage for the whole step)."""
+    P = len(xi)
+    G, _ = learned_indicator(params, lo, hi, orc.state().reshape(-1, P * P, 4), xi, s0, kappa)
+    orc.set_av_g(G)
+    orc.time_step(scheme, t, dt)

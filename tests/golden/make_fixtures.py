@@ -1,8 +1,8 @@
 """Generate the committed golden fixtures from the HORSES2D reference tree.
 
-Run once in a container that has the reference checked out (default path
-``/root/reference``; override with ``HORSES2D_REF``).  Outputs, next to this
-script:
+Run once in a container that has the reference checked out, with ``HORSES2D_REF``
+set to the root of that tree (the script refuses to run without it).  Outputs, next to
+this script:
 
 * ``<name>.mesh.npz`` -- the .HiOMesh NetCDF variables (points, quads, boundary
   edges/markers, curved edges, p-refinement zones) of the meshes the reference's
@@ -23,7 +23,7 @@ import sys
 import numpy as np
 from scipy.io import netcdf_file
 
-REF = os.environ.get("HORSES2D_REF", "/root/reference")
+REF = os.environ.get("HORSES2D_REF")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 MESHES = {
@@ -91,6 +91,9 @@ def parse_plugin(path):
 
 
 def main():
+    if not REF:
+        sys.stderr.write("set HORSES2D_REF to the root of the HORSES2D reference tree\n")
+        return 2
     for name, rel in MESHES.items():
         d = read_mesh(os.path.join(REF, rel))
         np.savez_compressed(os.path.join(HERE, f"{name}.mesh.npz"), **d)

@@ -55,6 +55,24 @@ def test_two_calls_in_a_row_match_hg_residuals():
         assert rc == 0 and np.array_equal(ob, rb)
 
 
+def test_calls_on_a_non_default_stream():
+    """The input is written on a fresh stream and the calls run on that stream: the partial and reduce
+    passes stay ordered after the write and before the read-back, and the result equals hg_residuals'."""
+    import torch
+    f = noalloc()
+    g = vortex_context(24, 5, 4)
+    q = g.compute_time_derivative(0.0)
+    r = g.residuals()
+    src = torch.from_numpy(q).pin_memory()
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        d = torch.empty(q.size, dtype=torch.float64, device="cuda")
+        d.copy_(src, non_blocking=True)
+        for _ in range(2):
+            rc, out = call(f, d.data_ptr(), d.numel(), s.cuda_stream)
+            assert rc == 0 and np.array_equal(out, r)
+
+
 def test_ragged_sizes_and_nan():
     import torch
     f = noalloc()
