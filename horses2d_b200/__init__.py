@@ -12,4 +12,5 @@ from .solver import GpuDGSEM, GpuGroup, HorsesGpuError  # noqa: F401
 from ._lib import (NODES_LG, NODES_LGL, ROE, HLL, EXACT, LXF, INTERIOR, SCHEME_EULER, SCHEME_RK3,  # noqa: F401
                    SCHEME_RK5, PREC_FP64, PREC_FP32, BC_PERIODIC, BC_DIRICHLET, BC_EULERWALL, BC_VISCOUSWALL,
                    BC_FARFIELD, BC_PRESSUREOUTLET, BC_NEWDIRICHLET, BR1, IP, SIPG, NIPG, IIPG,
-                   AV_NONE, AV_LAPLACIAN, AV_PHYSICAL, SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED)
+                   AV_NONE, AV_LAPLACIAN, AV_PHYSICAL, SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED,
+                   STATUS_CRASHED, HEALTH_NONFINITE, HEALTH_DENSITY, HEALTH_PRESSURE)

@@ -15,9 +15,14 @@
 
 static std::string g_create_err;
 
+// A stepped state that is no longer physical (health_check): status HG_STATUS_CRASHED.
+struct Crashed : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
 static int fail(hg_ctx* c, const std::exception& ex) {
   if (c) c->err = ex.what();
-  return 1;
+  return dynamic_cast<const Crashed*>(&ex) ? HG_STATUS_CRASHED : 1;
 }
 
 template <typename T>
@@ -48,12 +53,63 @@ void ctx_free(hg_ctx* c) {
   drop_graph(c);
   for (cudaEvent_t e : c->prof_pool) cudaEventDestroy(e);
   void* ptrs[] = {c->d_side, c->d_side_geo, c->d_vol_geo, c->d_mats, c->d_zones, c->d_Q, c->d_G, c->d_T[0], c->d_T[1],
-                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT,
-                  c->d_av_el, c->d_side_area, c->d_mu_av, c->d_mlp, c->d_feat_lo, c->d_feat_hi, c->d_dQ,
+                  c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT[0],
+                  c->d_GT[1], c->d_av_el, c->d_side_area, c->d_mu_av[0], c->d_mu_av[1], c->d_mlp, c->d_feat_lo,
+                  c->d_feat_hi, c->d_dQ,
                   c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG, c->d_exact_sides};
   for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
+  if (!c->health_shared) {
+    if (c->d_health) cudaFree(c->d_health);
+    if (c->h_health) cudaFreeHost(c->h_health);
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+}
+
+// ------------------------------------------------------------------ health of the stepped state
+// The stage kernels check every updated node (check_state, hg_stage.cuh) and set the device word
+// {bits, element} and the mapped host flag; the host reads the flag without a synchronisation before
+// each step call and after every synchronising call.
+static void health_alloc(hg_ctx* c) {
+  c->d_health = dalloc<int>(2);
+  const int clean[2] = {0, -1};
+  HG_CUDA(cudaMemcpy(c->d_health, clean, sizeof(clean), cudaMemcpyHostToDevice));
+  void* h = nullptr;
+  HG_CUDA(cudaHostAlloc(&h, sizeof(int), cudaHostAllocMapped));
+  c->h_health = static_cast<int*>(h);
+  *reinterpret_cast<volatile int*>(c->h_health) = 0;
+  void* dptr = nullptr;
+  HG_CUDA(cudaHostGetDevicePointer(&dptr, h, 0));
+  c->d_health_flag = static_cast<int*>(dptr);
+}
+
+static void health_share(hg_ctx* part, const hg_ctx* owner) {
+  part->d_health = owner->d_health;
+  part->h_health = owner->h_health;
+  part->d_health_flag = owner->d_health_flag;
+  part->health_shared = true;
+}
+
+static void health_reset(hg_ctx* c) {
+  const int clean[2] = {0, -1};
+  HG_CUDA(cudaMemcpyAsync(c->d_health, clean, sizeof(clean), cudaMemcpyHostToDevice, c->stream));
+  HG_CUDA(cudaStreamSynchronize(c->stream));
+  *reinterpret_cast<volatile int*>(c->h_health) = 0;
+}
+
+// Throws the reference's crash message if a stage has flagged the state (after synchronising, so that
+// the word is complete); a no-op while the host flag is clean.
+static void health_check(hg_ctx* c) {
+  if (!c->h_health || *reinterpret_cast<volatile int*>(c->h_health) == 0) return;
+  HG_CUDA(cudaStreamSynchronize(c->stream));
+  int w[2] = {0, -1};
+  HG_CUDA(cudaMemcpy(w, c->d_health, sizeof(w), cudaMemcpyDeviceToHost));
+  std::string what;
+  if (w[0] & HEALTH_NONFINITE) what += " a non-finite value";
+  if (w[0] & HEALTH_DENSITY) what += std::string(what.empty() ? "" : ",") + " a non-positive density";
+  if (w[0] & HEALTH_PRESSURE) what += std::string(what.empty() ? "" : ",") + " a non-positive pressure";
+  throw Crashed("The simulation has crashed: the state holds" + what + " (element " + std::to_string(w[1]) +
+                "); set a new state to continue");
 }
 
 static int epb_of(const hg_ctx* c, int variant) {
@@ -150,7 +206,8 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
   a.T_out = static_cast<real*>(c->d_T[c->cur ^ 1]);
-  a.GT = static_cast<real*>(c->d_GT);
+  a.GT = static_cast<real*>(c->d_GT[c->cur]);
+  a.GT_out = static_cast<real*>(c->d_GT[c->cur ^ 1]);
   a.dQ = static_cast<real*>(c->d_dQ);
   a.viscous = (c->pc.mu != 0.0 || c->av == HG_AV_PHYSICAL) ? 1 : 0;
   // BR1 always needs the lifted gradient; IP only for gradient traces (viscous fluxes) or the indicator
@@ -171,10 +228,22 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.av = c->av;
   a.av_el = c->d_av_el;
   a.side_area = c->d_side_area;
-  a.mu_av = c->d_mu_av;
+  if (!c->stepping) c->mu_step = c->cur;
+  a.mu_av = c->d_mu_av[c->mu_step];
+  a.mu_next = c->d_mu_av[c->cur ^ 1];
   a.sensor = sensor_args(c);
+  a.health = c->d_health;
+  a.health_host = c->d_health_flag;
   a.run_stage = c->ns_phase != 1;
   if (c->ns_phase == 2) a.run_gradient = 0;
+  a.fuse = (ns_fused(c) && !c->prologue) ? 1 : 0;
+  a.last = c->last_stage ? 1 : 0;
+  if (a.fuse) a.run_gradient = 0;   // the previous stage (or the prologue) left GT and mu_av of this state
+  if (c->prologue) {                // gradient traces and indicator of the resident state only
+    a.run_gradient = 1;
+    a.run_stage = 0;
+  }
+  c->mu_last = c->mu_step;
   if (c->exact && a.run_stage) launch_exact_flux<real>(c);
   HG_DISPATCH_P_NS(c->P, ns_dispatch, c, a);
   if (!a.run_stage) return;
@@ -201,6 +270,8 @@ static void run_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bo
   a.T_out = static_cast<real*>(c->d_T[c->cur ^ 1]);
   a.QDot = qdot;
   a.resid = resid ? c->d_resid : nullptr;
+  a.health = c->d_health;
+  a.health_host = c->d_health_flag;
   a.a = ca; a.b = cb; a.c = cc;
   a.first = first ? 1 : 0;
   a.update = update ? 1 : 0;
@@ -252,25 +323,49 @@ static void traces(hg_ctx* c) {
 }
 
 // One step of a reference scheme; residual maxima are collected on the last stage.
+// The indicator buffer of the step is the one of its starting trace parity (mu_step), and the last
+// stage is flagged (a fused interior-penalty stage then writes the next step's indicator).
 static void one_step(hg_ctx* c, int scheme, double t, double dt) {
   (void)t;
+  struct Step {
+    hg_ctx* c;
+    explicit Step(hg_ctx* c_) : c(c_) { c->stepping = true; c->mu_step = c->cur; }
+    ~Step() { c->stepping = false; c->last_stage = false; }
+  } guard(c);
   if (scheme == HG_SCHEME_EULER) {
+    c->last_stage = true;
     ctx_stage(c, 0.0, dt, 1.0, true, true, nullptr, true);
   } else if (scheme == HG_SCHEME_RK3) {
     const double am[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
     const double gm[3] = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
     for (int m = 0; m < 3; ++m) {
+      c->last_stage = m == 2;
       ctx_stage(c, am[m], 1.0, gm[m] * dt, m == 0, true, nullptr, m == 2);
     }
   } else if (scheme == HG_SCHEME_RK5) {
     const double am[5] = {0.0, -0.4178904745, -1.192151694643, -1.697784692471, -1.514183444257};
     const double gm[5] = {0.1496590219993, 0.3792103129999, 0.8229550293869, 0.6994504559488, 0.1530572479681};
     for (int m = 0; m < 5; ++m) {
+      c->last_stage = m == 4;
       ctx_stage(c, am[m], dt, gm[m], m == 0, true, nullptr, m == 4);
     }
   } else {
     throw std::runtime_error("unknown time scheme");
   }
+}
+
+// The fused interior-penalty path's prologue: gradient traces and indicator of the resident state (the
+// gradient kernel alone), after the state or the indicator has been replaced.
+static void ns_prologue(hg_ctx* c) {
+  if (!ns_fused(c) || !c->state_set) return;
+  c->prologue = true;
+  try {
+    ctx_stage(c, 0.0, 0.0, 0.0, true, false, nullptr, false);
+  } catch (...) {
+    c->prologue = false;
+    throw;
+  }
+  c->prologue = false;
 }
 
 // ------------------------------------------------------------------ dt estimate
@@ -528,14 +623,17 @@ void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, cons
     }
     c->d_av_el = dalloc<double>(avel.size());
     c->d_side_area = dalloc<double>(area.size());
-    c->d_mu_av = dalloc<double>(size_t(E));
+    for (auto& m_ : c->d_mu_av) {
+      m_ = dalloc<double>(size_t(E));
+      HG_CUDA(cudaMemset(m_, 0, size_t(E) * sizeof(double)));
+    }
     HG_CUDA(cudaMemcpy(c->d_av_el, avel.data(), avel.size() * sizeof(double), cudaMemcpyHostToDevice));
     HG_CUDA(cudaMemcpy(c->d_side_area, area.data(), area.size() * sizeof(double), cudaMemcpyHostToDevice));
   }
   if (c->ns) {
     if (c->ip && !m->edge_invh) throw std::runtime_error("interior penalty needs edge_invh");
     c->d_side_invh = dalloc<double>(sinvh.size());
-    c->d_GT = dalloc<char>(size_t(E) * 4 * P * 8 * rs);
+    for (auto& g_ : c->d_GT) g_ = dalloc<char>(size_t(E) * 4 * P * 8 * rs);
     c->d_dQ = dalloc<char>(size_t(c->ndof) * 2 * rs);
     HG_CUDA(cudaMemcpy(c->d_side_invh, sinvh.data(), sinvh.size() * sizeof(double), cudaMemcpyHostToDevice));
     if (!c->affine) {
@@ -578,6 +676,8 @@ extern "C" int hg_create(const hg_mesh_desc* mesh, const hg_physics_desc* phys, 
     for (int e = 1; e < mesh->n_elements && !mixed; ++e) mixed = mesh->N[e] != mesh->N[0];
     if (mixed) composite_build(c, mesh, phys, bcs, n_bcs);
     else ctx_build(c, mesh, phys, bcs, n_bcs, nullptr);
+    health_alloc(c);
+    for (hg_ctx* p : c->parts) health_share(p, c);
   } catch (const std::exception& ex) {
     g_create_err = ex.what();
     ctx_free(c);
@@ -668,17 +768,20 @@ extern "C" int hg_set_state(hg_ctx* c, const double* Q, int64_t ndof) {
   try {
     if (is_composite(c)) {
       check_ndof(c, ndof);
+      health_reset(c);
       composite_scatter(c, Q);
       c->cur = 0;
       c->state_set = true;
       return 0;
     }
     check_ndof(c, ndof);
+    health_reset(c);
     HG_CUDA(cudaMemcpyAsync(c->d_Q, Q, ndof * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     c->cur = 0;
     traces(c);
-    HG_CUDA(cudaGetLastError());
     c->state_set = true;
+    ns_prologue(c);
+    HG_CUDA(cudaGetLastError());
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -688,11 +791,13 @@ extern "C" int hg_get_state(hg_ctx* c, double* Q, int64_t ndof) {
     if (is_composite(c)) {
       check_ndof(c, ndof);
       composite_gather(c, Q, false);
+      health_check(c);
       return 0;
     }
     check_ndof(c, ndof);
     HG_CUDA(cudaMemcpyAsync(Q, c->d_Q, ndof * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
+    health_check(c);
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -704,6 +809,7 @@ static void require_state(hg_ctx* c) {
 extern "C" int hg_time_derivative(hg_ctx* c, double t, double* QDot) {
   try {
     require_state(c);
+    health_check(c);
     (void)t;
     ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), true);
     HG_CUDA(cudaGetLastError());
@@ -783,6 +889,7 @@ static void graph_one_step(hg_ctx* c, int scheme, double t, double dt) {
 extern "C" int hg_time_step(hg_ctx* c, int32_t scheme, double t, double dt) {
   try {
     require_state(c);
+    health_check(c);
     if (!c->prof && c->stream != nullptr &&
         (scheme == HG_SCHEME_EULER || scheme == HG_SCHEME_RK3 || scheme == HG_SCHEME_RK5))
       graph_one_step(c, scheme, t, dt);
@@ -841,6 +948,7 @@ static void graph_steps(hg_ctx* c, int scheme, int n_steps, double t0, double dt
 extern "C" int hg_time_steps(hg_ctx* c, int32_t scheme, int32_t n_steps, double t0, double dt) {
   try {
     require_state(c);
+    health_check(c);
     if (n_steps >= 5 && !c->prof && c->stream != nullptr) {
       graph_steps(c, scheme, n_steps, t0, dt);
     } else {
@@ -855,6 +963,7 @@ extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
   try {
     if (is_composite(c)) {
       composite_residuals(c, out);
+      health_check(c);
       return 0;
     }
     timed(c, HG_KERNEL_REDUCE,
@@ -863,6 +972,7 @@ extern "C" int hg_residuals(hg_ctx* c, double out[4]) {
     HG_CUDA(cudaGetLastError());
     HG_CUDA(cudaMemcpyAsync(out, c->d_resid_out, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
+    health_check(c);
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -887,6 +997,7 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
                                 c->stream));
       }
       HG_CUDA(cudaStreamSynchronize(c->stream));
+      health_check(c);
       double d = dt_cap;
       for (int e = 0; e < c->n_el; ++e) {
         const double* v = &em[c->el_part[e]][2 * size_t(c->el_local[e])];
@@ -906,6 +1017,7 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
     std::vector<double> em(size_t(c->n_el) * 2);
     HG_CUDA(cudaMemcpyAsync(em.data(), c->d_elmax, em.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
+    health_check(c);
     // running maxima over elements in mesh order, kept across calls
     double d = dt_cap;
     for (int e = 0; e < c->n_el; ++e) {
@@ -933,6 +1045,19 @@ extern "C" int hg_synchronize(hg_ctx* c) {
   try {
     HG_CUDA(cudaStreamSynchronize(c->stream));
     HG_CUDA(cudaGetLastError());
+    health_check(c);
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_health(hg_ctx* c, int32_t* bits, int32_t* element) {
+  try {
+    if (!c) return 1;
+    HG_CUDA(cudaStreamSynchronize(c->stream));
+    int w[2] = {0, -1};
+    HG_CUDA(cudaMemcpy(w, c->d_health, sizeof(w), cudaMemcpyDeviceToHost));
+    if (bits) *bits = w[0];
+    if (element) *element = w[1];
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -997,6 +1122,7 @@ extern "C" int hg_set_sensor(hg_ctx* c, int32_t kind, double s0, double kappa, c
     put(c->d_feat_lo, lo, HG_SENSOR_FEATURES);
     put(c->d_feat_hi, hi, HG_SENSOR_FEATURES);
     c->sensor_kind = kind;
+    ns_prologue(c);   // the fused path keeps the indicator of the resident state
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }
@@ -1037,8 +1163,9 @@ extern "C" int hg_sensor_eval(hg_ctx* c, float* features, double* out) {
 
 extern "C" int hg_element_viscosity(hg_ctx* c, double* mu) {
   try {
-    if (!c->d_mu_av) throw std::runtime_error("artificial dissipation is off for this context");
-    HG_CUDA(cudaMemcpyAsync(mu, c->d_mu_av, size_t(c->n_el) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (!c->d_mu_av[0]) throw std::runtime_error("artificial dissipation is off for this context");
+    HG_CUDA(cudaMemcpyAsync(mu, c->d_mu_av[c->mu_last], size_t(c->n_el) * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }

@@ -42,7 +42,15 @@ struct hg_ctx {
   int av = 0;                     // artificial dissipation HG_AV_*
   double* d_av_el = nullptr;      // [n_el][2] Ceps sqrt(Volume)/(N+1), sum of edge areas
   double* d_side_area = nullptr;  // [n_el*4] Area of each side's edge
-  double* d_mu_av = nullptr;      // [n_el] element artificial viscosity of the current stage
+  // element artificial viscosity [n_el], a pair: the indicator for the time step that starts at trace
+  // parity p lives in d_mu_av[p] (a fused interior-penalty stage writes the next step's into the other)
+  double* d_mu_av[2] = {nullptr, nullptr};
+  int mu_step = 0;                // buffer the stages of the current step (or a bare evaluation) read
+  int mu_last = 0;                // buffer the last evaluated stage read (hg_element_viscosity)
+  bool last_stage = false;        // the stage being launched is the last of its time step
+  bool stepping = false;          // inside one_step (mu_step fixed for the step)
+  bool prologue = false;          // the next Navier-Stokes launch is the fused path's prologue
+  bool is_part = false;           // an order part of a composite context
   // shock sensor (hg_sensor.cuh): indicator kind, modal ramp, learned-sensor weights and feature box
   int sensor_kind = 0;
   double sensor_s0 = 0.0, sensor_kappa = 1.0;
@@ -50,7 +58,7 @@ struct hg_ctx {
   float* d_feat_lo = nullptr;
   float* d_feat_hi = nullptr;
   void* d_jac = nullptr;          // [n_el][NP] J (curved meshes), context precision
-  void* d_GT = nullptr;           // gradient traces [n_el*4][P][2][4]
+  void* d_GT[2] = {nullptr, nullptr};   // gradient traces [n_el*4][P][2][4] per trace parity (as d_T)
   void* d_dQ = nullptr;           // element gradients [n_el][2][4][NP] (Navier-Stokes)
   int tiling = 0;                 // elements-per-CTA variant of the stage kernels (hg_autotune / hg_set_tiling)
   bool exact = false;             // some face uses the exact Riemann solver (globally or by zone)
@@ -83,6 +91,12 @@ struct hg_ctx {
   int last_T = 0;                             // trace buffer of the last residual evaluation's state
   bool state_set = false;
   int64_t launches = 0;
+  // health of the stepped state (check_state in hg_stage.cuh): device word {bits, element} and a mapped,
+  // pinned host flag that the kernels set beside it; a composite's parts share the composite's
+  int* d_health = nullptr;
+  int* h_health = nullptr;        // host address of the flag (its device address is d_health_flag)
+  int* d_health_flag = nullptr;
+  bool health_shared = false;
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
   double save_umax = 0.0, save_amax = 0.0;
   // CUDA graphs of two time steps (hg_time_steps), one per trace-buffer parity at their start (a
@@ -175,6 +189,12 @@ void composite_free(hg_ctx* c);
 enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1, MORTAR_FLUX_IP = 2 };
 void launch_mortar(hg_ctx* c, int mode);
 inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
+// Interior penalty with an element-local indicator (none, modal, learned) on a single-order context:
+// one fused kernel per stage (hg_ns.cuh); the gradient kernel runs only as the prologue after the
+// state or the indicator changes.
+inline bool ns_fused(const hg_ctx* c) {
+  return c->ns && c->ip && !c->is_part && !is_composite(c) && (c->av == HG_AV_NONE || c->sensor_kind != 0);
+}
 constexpr int HG_MAX_PARTS = 12;
 constexpr int HG_MAX_ORDER_EULER = 12;
 constexpr int HG_MAX_ORDER_NS = 10;

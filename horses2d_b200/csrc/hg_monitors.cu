@@ -117,10 +117,10 @@ void launch_surface_integrals(hg_ctx* c, int zone, double* d_out) {
   const int n_sides = int(c->zone_sides[z].size());
   const int NP = c->P * c->P;
   const double* w = c->d_mats + 2 * NP + 6 * c->P;   // hatD lb0 lb1 lbw0 lbw1 D dlbw0 dlbw1 w Vinv
-  const int viscous = (c->ns && c->pc.mu != 0.0 && c->d_GT) ? 1 : 0;
+  const int viscous = (c->ns && c->pc.mu != 0.0 && c->d_GT[c->last_T]) ? 1 : 0;
   surface_integral_kernel<real><<<1, SI_THREADS, 0, c->stream>>>(
       n_sides, c->d_zone_sides[z], c->P, c->affine ? 1 : 0, static_cast<const real*>(c->d_side_geo),
-      static_cast<const real*>(c->d_T[c->last_T]), static_cast<const real*>(c->d_GT), w, c->pc, viscous, d_out);
+      static_cast<const real*>(c->d_T[c->last_T]), static_cast<const real*>(c->d_GT[c->last_T]), w, c->pc, viscous, d_out);
   ++c->launches;
 }
 

@@ -319,7 +319,7 @@ void launch_mortar(hg_ctx* c, int mode) {
     for (size_t p = 0; p < c->parts.size(); ++p) {
       hg_ctx* q = c->parts[p];
       a.T[p] = static_cast<const real*>(q->d_T[q->cur]);
-      a.GT[p] = static_cast<const real*>(q->d_GT);
+      a.GT[p] = static_cast<const real*>(q->d_GT[q->cur]);
       a.NF[p] = static_cast<real*>(q->d_NF);
       a.NFG[p] = static_cast<real*>(q->d_NFG);
     }
@@ -600,6 +600,7 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
     sub.periodic_partner = epart.data();
     sub.edge_invh = m->edge_invh ? invh.data() : nullptr;
     hg_ctx* pc = new hg_ctx();
+    pc->is_part = true;
     pc->precision = c->precision;
     c->parts.push_back(pc);
     ctx_build(pc, &sub, ph, bcs, n_bcs, &flux_sides[p]);

@@ -12,6 +12,11 @@
 //        interior-penalty gradient is element-local and the stage kernel recomputes it, so with IP the
 //        gradient kernel runs only when something else needs it (gradient traces for viscous fluxes,
 //        the artificial-viscosity indicator);
+//   interior penalty with an element-local indicator (none, modal, learned): no gradient kernel per
+//        stage.  The stage kernel ends with the gradient traces of the state it wrote (GT_out, the
+//        other half of a ping-pong pair, as for the Q traces) and, on the last stage of a time step,
+//        the indicator of that state (mu_next): everything the next stage reads from its neighbours.
+//        The gradient kernel then runs only once after the state is replaced (hg_set_state);
 //   ns_stage_kernel     reads the BR1 dQ back (written once, read once per stage),
 //        F = Fi - Fv at the nodes (QDotVolumeLoop :243-268), face fluxes
 //        F* = (Fi* - Fv*) dS with the neighbours' Q and dQ traces (BR1: (FvL+FvR)/2 . n; IP adds
@@ -43,7 +48,8 @@ struct NSArgs {
   real* G;
   const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
   real* T_out;
-  real* GT;                 // dQ traces                      [n_el*4][P][2][4]
+  real* GT;                 // dQ traces of the current state [n_el*4][P][2][4]
+  real* GT_out;             // dQ traces of the updated state (fused interior-penalty stages)
   real* dQ;                 // element gradients              [n_el][2][4][NP]
   int viscous;              // viscous fluxes present: mu != 0 or the Physical artificial viscosity
   int run_gradient;         // host side: whether this stage needs the gradient kernel
@@ -62,6 +68,11 @@ struct NSArgs {
   const double* side_area;  // [n_el*4] Area of each side's edge
   double* mu_av;            // [n_el] element viscosity of the current state (written by the gradient kernel)
   SensorArgs sensor;        // which indicator sets it (jumps, modal, learned)
+  int fuse;                 // interior penalty, element-local indicator: the stage kernel writes GT_out and,
+  int last;                 //   on the last stage of a step (last), the indicator of its new state into
+  double* mu_next;          //   mu_next
+  int* health;              // device health word {bits, first element} (check_state)
+  int* health_host;         // mapped host flag set beside it
 };
 
 __host__ __device__ constexpr int epb_ns(int P) {
@@ -86,6 +97,7 @@ struct NSTiles {
   real Fc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
   real Gc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
   real face[12][EPB][FT];   // BR1 u* dS n (8) / F* (4) + gradient-face contravariant fluxes (8)
+  real gfd[ST ? 4 : 1][ST ? EPB : 1][ST ? FT : 1];   // gradient-face terms contracted along their side
   double red[32][4];
 };
 
@@ -617,6 +629,23 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     }
   }
   __syncthreads();
+  // The gradient-face terms enter the lift as hatD-contractions along their side, which depend on the
+  // node's index along that side only (Scalar_StdGradientFace): formed once per side node here (P
+  // multiply-adds each) instead of at every node of the element.
+  const bool gf = IP && a.grad_faces && visc;   // uniform over the launch
+  if (gf && active) {
+    for (int t = tid; t < FT; t += NP) {
+      const int sd_ = t / P, kk = t % P;
+      const int row = (sd_ & 1) ? 8 : 4;   // bottom / top: the xi component; right / left: the eta one
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        real d = real(0);
+#pragma unroll
+        for (int l = 0; l < P; ++l) d += hatD[kk * P + l] * s.face[row + k][le][sd_ * P + l];
+        s.gfd[k][le][t] = d;
+      }
+    }
+  }
   real qd[4] = {real(0), real(0), real(0), real(0)};
   if (active) {
 #pragma unroll
@@ -632,21 +661,16 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       qd[k] = qd[k] - s.face[k][le][2 * P + i] * lbw1[j];
       qd[k] = qd[k] - s.face[k][le][3 * P + j] * lbw0[i];
     }
-    if (IP && a.grad_faces && visc) {
+  }
+  if (gf) __syncthreads();
+  if (active) {
+    if (gf) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        real dFb = real(0), dGr = real(0), dFt = real(0), dGl = real(0);
-#pragma unroll
-        for (int l = 0; l < P; ++l) {
-          dFb += hatD[i * P + l] * s.face[4 + k][le][0 * P + l];
-          dGr += hatD[j * P + l] * s.face[8 + k][le][1 * P + l];
-          dFt += hatD[i * P + l] * s.face[4 + k][le][2 * P + l];
-          dGl += hatD[j * P + l] * s.face[8 + k][le][3 * P + l];
-        }
-        qd[k] = qd[k] - (dFb * lbw0[j] + s.face[8 + k][le][0 * P + i] * dlbw0[j]);
-        qd[k] = qd[k] - (s.face[4 + k][le][1 * P + j] * dlbw1[i] + dGr * lbw1[i]);
-        qd[k] = qd[k] - (dFt * lbw1[j] + s.face[8 + k][le][2 * P + i] * dlbw1[j]);
-        qd[k] = qd[k] - (s.face[4 + k][le][3 * P + j] * dlbw0[i] + dGl * lbw0[i]);
+        qd[k] = qd[k] - (s.gfd[k][le][0 * P + i] * lbw0[j] + s.face[8 + k][le][0 * P + i] * dlbw0[j]);
+        qd[k] = qd[k] - (s.face[4 + k][le][1 * P + j] * dlbw1[i] + s.gfd[k][le][1 * P + j] * lbw1[i]);
+        qd[k] = qd[k] - (s.gfd[k][le][2 * P + i] * lbw1[j] + s.face[8 + k][le][2 * P + i] * dlbw1[j]);
+        qd[k] = qd[k] - (s.face[4 + k][le][3 * P + j] * dlbw0[i] + s.gfd[k][le][3 * P + j] * lbw0[i]);
       }
     }
 #pragma unroll
@@ -670,6 +694,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       q23.x = q23.x + a.c * double(gn[2]);
       q23.y = q23.y + a.c * double(gn[3]);
       qp[0] = q01; qp[1] = q23;
+      check_state(a.health, a.health_host, q01.x, q01.y, q23.x, q23.y, e);
       s.Q[0][le][tid] = real(q01.x); s.Q[1][le][tid] = real(q01.y);
       s.Q[2][le][tid] = real(q23.x); s.Q[3][le][tid] = real(q23.y);
     }
@@ -701,6 +726,43 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, tr);
 #pragma unroll
       for (int k = 0; k < 4; ++k) tp[k] = tr[k];
+    }
+  }
+  if constexpr (IP) {
+    // Fused interior penalty: what the next stage's neighbours read of this element's new state --
+    // its gradient traces (the local gradient, ComputeInteriorGradient, interpolated to the sides) and,
+    // after the last stage of a step, its element-local indicator.  a.fuse, a.update, a.viscous and
+    // a.last are uniform over the launch.
+    if (a.fuse && a.update) {
+      __syncthreads();   // every node's new state is in s.Q
+      if (visc) {
+        element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
+        __syncthreads();
+        if (active) {
+          for (int t = tid; t < FT; t += NP) {
+            const int sd_ = t / P, kk = t % P;
+            const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+            real* gp = a.GT_out + ((size_t(e) * 4 + sd_) * P + kk) * 8;
+            real tx[4], ty[4];
+            trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, tx);
+            trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, ty);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) { gp[k] = tx[k]; gp[4 + k] = ty[k]; }
+          }
+        }
+      }
+      if (AV && a.last && a.sensor.kind != SENSOR_JUMPS) {
+        const int n_active = a.n_el - int(blockIdx.x) * EPB < EPB ? a.n_el - int(blockIdx.x) * EPB : EPB;
+        // the gradient, contravariant-flux and face tiles (contiguous) are dead here: where they are
+        // large enough they hold the indicator's scratch, which keeps the kernel's static shared memory
+        // within 48 KB (FP64 at high and low orders); otherwise the indicator declares its own
+        constexpr size_t dead = sizeof(s.dQ) + sizeof(s.Fc) + sizeof(s.Gc) + sizeof(s.face) + sizeof(s.gfd);
+        constexpr bool lend = dead >= sensor_ext_bytes<P, EPB, real>();
+        __syncthreads();   // the gradient traces above have read s.dQ
+        const SensorOut so = element_sensor<P, EPB, real, lend>(a.sensor, ph, s.Q, n_active, s.mat + 2 * NP + 7 * P,
+                                                                le, tid, active, nullptr, &s.dQ[0][0][0][0]);
+        if (active && tid == 0) a.mu_next[e] = a.av_el[2 * size_t(e)] * so.g;
+      }
     }
   }
 }

@@ -59,15 +59,27 @@ struct SensorOut {
 // shared memory, and each warp evaluates one element at a time with one lane per hidden unit: the
 // inputs are broadcast from the element's scratch row, the 32-input sums of the second layer run as
 // four interleaved partial sums, and the output unit is a warp shuffle tree.
+// Shared memory the indicator needs when the caller lends it (EXT): EPB scratch rows, then the weights.
 template <int P, int EPB, typename real>
+__host__ __device__ constexpr size_t sensor_ext_bytes() {
+  return size_t(EPB) * sensor_scratch(P) * sizeof(real) + size_t(MLP_PARAMS) * sizeof(float);
+}
+
+template <int P, int EPB, typename real, bool EXT = false>
 __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const Phys<real>& ph,
                                                     const real (*Q)[EPB][P * P], int n_active,
                                                     const real* Vinv, int le, int tid, bool active,
-                                                    float* feat_out) {
+                                                    float* feat_out, real* ext = nullptr) {
   constexpr int NP = P * P, N = P - 1, SS = sensor_scratch(P);
-  // scratch rows of the CTA's elements, declared here so that every access is a shared-memory one
-  __shared__ real s_scr[EPB * SS];
-  real* const scr_all = s_scr;
+  // scratch rows of the CTA's elements: declared here, or lent by the caller (EXT: shared memory the
+  // caller no longer needs, sensor_ext_bytes long), so that every access is a shared-memory one
+  real* scr_all;
+  if constexpr (EXT) {
+    scr_all = ext;
+  } else {
+    __shared__ real s_scr[EPB * SS];
+    scr_all = s_scr;
+  }
   real* scr = scr_all + (le < EPB ? le : 0) * SS;
   real* uh = scr;                 // [2][NP] modal coefficients of rho, p (k_eta * P + k_xi)
   real* en = scr + 2 * NP;        // [2][12]: Ex[4], Ey[4], E, EN, -, -
@@ -150,7 +162,13 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
   }
   if (sa.kind == SENSOR_LEARNED) {
     static_assert(MLP_H == 32, "one lane per hidden unit");
-    __shared__ float s_w[MLP_PARAMS];   // W1^T[16][32] b1 W2^T[32][32] b2 W3 b3
+    float* s_w;   // W1^T[16][32] b1 W2^T[32][32] b2 W3 b3
+    if constexpr (EXT) {
+      s_w = reinterpret_cast<float*>(ext + EPB * SS);
+    } else {
+      __shared__ float s_w_own[MLP_PARAMS];
+      s_w = s_w_own;
+    }
     for (int d = threadIdx.x; d < MLP_PARAMS; d += blockDim.x) s_w[d] = __ldg(sa.mlp + d);
     __syncthreads();
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;

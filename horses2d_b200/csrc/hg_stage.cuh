@@ -52,6 +52,8 @@ struct StageArgs {
   real* T_out;
   double* QDot;            // optional output (time derivative only)
   double* resid;           // optional per-CTA max |QDot| per variable: [gridDim.x][4]
+  int* health;             // device health word {bits, element} (check_state), may be null
+  int* health_host;        // mapped host flag set beside it, may be null
   double a, b, c;          // G = a G + b QDot ; Q += c G
   int first;               // a == 0: do not read G
   int update;              // 1: RK update, 0: only QDot (and traces of the unchanged Q)
@@ -73,6 +75,25 @@ __host__ __device__ constexpr int block_for(int P) { return block_of(P, epb_for(
 
 // max that keeps NaN (a residual that is NaN must stay visible)
 __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
+
+// Health of an updated node state.  The reference stops with "The simulation has crashed" when Q holds
+// a NaN (DGTimeIntegrator.f90:224-233); here every RK update checks its node: bit 1 a non-finite value,
+// bit 2 rho <= 0, bit 4 p <= 0 (tested as rho (rho E) - |rho u|^2 / 2 = rho p / (gamma - 1) <= 0, no
+// division).  health = {bits, an offending element (the first to arrive)}; the mapped host flag tells
+// the host without a synchronisation that the word is no longer clean.
+enum { HEALTH_NONFINITE = 1, HEALTH_DENSITY = 2, HEALTH_PRESSURE = 4 };
+__device__ __forceinline__ void check_state(int* health, int* health_host, double r, double ru, double rv,
+                                            double rE, int e) {
+  const bool finite = fabs(r) + fabs(ru) + fabs(rv) + fabs(rE) < 1.0e300;
+  const double k = r * rE - 0.5 * (ru * ru + rv * rv);
+  if (finite && r > 0.0 && k > 0.0) return;
+  const int bits = !finite ? HEALTH_NONFINITE : (r > 0.0 ? HEALTH_PRESSURE : HEALTH_DENSITY);
+  if (health) {
+    atomicOr(health, bits);
+    atomicCAS(health + 1, -1, e);
+  }
+  if (health_host) *reinterpret_cast<volatile int*>(health_host) = 1;
+}
 
 // AFFINE: metrics constant per element (vol_geo [n_el][5]) and normals/dS constant
 // per side (side_geo [n_el*4][3]), as for parallelogram elements with straight edges.
@@ -239,6 +260,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
       q23.x = q23.x + a.c * double(gn[2]);
       q23.y = q23.y + a.c * double(gn[3]);
       qp[0] = q01; qp[1] = q23;
+      check_state(a.health, a.health_host, q01.x, q01.y, q23.x, q23.y, e);
       s_Q[0][le][tid] = real(q01.x); s_Q[1][le][tid] = real(q01.y);
       s_Q[2][le][tid] = real(q23.x); s_Q[3][le][tid] = real(q23.y);
     }

@@ -30,6 +30,10 @@ from . import restart
 
 
 class HorsesGpuError(RuntimeError):
+    """An error status of the library; `status` is its code (L.STATUS_CRASHED: the stepped state is no
+    longer physical)."""
+    status = 1
+
     pass
 
 
@@ -109,7 +113,9 @@ class GpuDGSEM:
 
     def _check(self, rc):
         if rc != 0:
-            raise HorsesGpuError(self._lib.hg_last_error(self._h).decode())
+            err = HorsesGpuError(self._lib.hg_last_error(self._h).decode())
+            err.status = rc
+            raise err
 
     def close(self):
         if getattr(self, "_h", None):
@@ -151,6 +157,13 @@ class GpuDGSEM:
         r = np.zeros(4)
         self._check(self._lib.hg_residuals(self._h, r.ctypes.data_as(L.F64P)))
         return r
+
+    def health(self):
+        """(bits, element) of the device health word: HEALTH_* bits (0: clean) and one offending
+        element (-1 when clean)."""
+        b, e = C.c_int32(0), C.c_int32(-1)
+        self._check(self._lib.hg_health(self._h, C.byref(b), C.byref(e)))
+        return b.value, e.value
 
     def estimate_time_step(self, cfl, dt_cap):
         d = C.c_double(0.0)

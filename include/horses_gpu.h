@@ -15,6 +15,7 @@
  * Conventions
  *  - Every function returns 0 on success, non-zero on error; hg_last_error()
  *    returns the message (the shim turns it into the reference's `stop`).
+ *    HG_STATUS_CRASHED: the stepped state is no longer physical (see hg_health).
  *  - The state Q is the reference's flat Storage%Q (Generic/Storage.f90:31-73):
  *    element e holds 4*(N_e+1)^2 doubles at offset 4*cumP2(e), ordered
  *    Q[e][eta][xi][var] (var fastest).  hg_set_state / hg_get_state copy it
@@ -137,6 +138,18 @@ int  hg_time_step(hg_ctx* ctx, int32_t scheme, double t, double dt);
 int  hg_time_steps(hg_ctx* ctx, int32_t scheme, int32_t n_steps, double t0, double dt);
 /* == Mesh_ComputeResiduals: max |QDot| per variable of the last stage. */
 int  hg_residuals(hg_ctx* ctx, double out[4]);
+/* Health of the stepped state (the reference's "The simulation has crashed", printed when Q holds a
+ * NaN: DGTimeIntegrator.f90:224-233).  Every RK update on the device checks its nodes for a
+ * non-finite value, rho <= 0 or p <= 0 and records HG_HEALTH_* bits and one offending element
+ * (0-based).  hg_time_step / hg_time_steps return HG_STATUS_CRASHED, with the message in
+ * hg_last_error, once a flagged step has completed (checked without a synchronisation at the start
+ * of each step call, so the call after the bad step reports it); the synchronising calls
+ * (hg_residuals, hg_get_state, hg_estimate_dt, hg_synchronize) report it at once.  The flag stays
+ * until hg_set_state replaces the state.  hg_health synchronises and returns the bits (0: clean) and
+ * the element (-1 when clean). */
+enum { HG_STATUS_CRASHED = 2 };
+enum { HG_HEALTH_NONFINITE = 1, HG_HEALTH_DENSITY = 2, HG_HEALTH_PRESSURE = 4 };
+int  hg_health(hg_ctx* ctx, int32_t* bits, int32_t* element);
 /* == EstimateTimeStep, including the reference's running maxima (SAVE). */
 int  hg_estimate_dt(hg_ctx* ctx, double cfl, double dt_cap, double* dt);
 
