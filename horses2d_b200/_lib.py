@@ -59,7 +59,7 @@ EXPORTED = ("hg_create", "hg_destroy", "hg_last_error", "hg_set_state", "hg_get_
             "hg_group_time_steps", "hg_group_last_error", "hg_surface_integrals", "hg_probes",
             "hg_mesh_connectivity", "hg_mesh_last_error", "hg_write_restart", "hg_read_restart",
             "hg_save_restart", "hg_load_restart", "hg_restart_last_error", "hg_save_restart_async",
-            "hg_restart_wait", "hg_health")
+            "hg_restart_wait", "hg_health", "hg_set_health_policy")
 SENSOR_JUMPS, SENSOR_MODAL, SENSOR_LEARNED = 0, 1, 2
 SENSOR_FEATURES, MLP_PARAMS = 16, 1633
 F32P = C.POINTER(C.c_float)
@@ -95,6 +95,7 @@ def load():
     L.hg_set_stream.argtypes = [vp, vp]
     L.hg_synchronize.argtypes = [vp]
     L.hg_health.argtypes = [vp, I32P, I32P]
+    L.hg_set_health_policy.argtypes = [vp, C.c_int32]
     L.hg_device_state.restype = C.c_void_p
     L.hg_device_state.argtypes = [vp]
     L.hg_launch_count.restype = C.c_int64

@@ -97,13 +97,19 @@ static void health_reset(hg_ctx* c) {
   *reinterpret_cast<volatile int*>(c->h_health) = 0;
 }
 
-// Throws the reference's crash message if a stage has flagged the state (after synchronising, so that
-// the word is complete); a no-op while the host flag is clean.
+// Throws the reference's crash message if a stage has flagged the state with a fatal condition (after
+// synchronising, so that the word is complete); a no-op while the host flag is clean.  Conditions that
+// are recorded but not fatal clear the host flag again, so that later calls do not synchronise until a
+// new event.
 static void health_check(hg_ctx* c) {
   if (!c->h_health || *reinterpret_cast<volatile int*>(c->h_health) == 0) return;
   HG_CUDA(cudaStreamSynchronize(c->stream));
   int w[2] = {0, -1};
   HG_CUDA(cudaMemcpy(w, c->d_health, sizeof(w), cudaMemcpyDeviceToHost));
+  if ((w[0] & c->health_fatal) == 0) {
+    *reinterpret_cast<volatile int*>(c->h_health) = 0;
+    return;
+  }
   std::string what;
   if (w[0] & HEALTH_NONFINITE) what += " a non-finite value";
   if (w[0] & HEALTH_DENSITY) what += std::string(what.empty() ? "" : ",") + " a non-positive density";
@@ -1046,6 +1052,18 @@ extern "C" int hg_synchronize(hg_ctx* c) {
     HG_CUDA(cudaStreamSynchronize(c->stream));
     HG_CUDA(cudaGetLastError());
     health_check(c);
+    return 0;
+  } catch (const std::exception& ex) { return fail(c, ex); }
+}
+
+extern "C" int hg_set_health_policy(hg_ctx* c, int32_t fatal_bits) {
+  try {
+    if (!c) return 1;
+    if (fatal_bits & ~(HEALTH_NONFINITE | HEALTH_DENSITY | HEALTH_PRESSURE))
+      throw std::runtime_error("unknown health bits");
+    c->health_fatal = fatal_bits;
+    for (hg_ctx* p : c->parts) p->health_fatal = fatal_bits;
+    *reinterpret_cast<volatile int*>(c->h_health) = 1;   // re-examine the word under the new policy
     return 0;
   } catch (const std::exception& ex) { return fail(c, ex); }
 }

@@ -97,6 +97,7 @@ struct hg_ctx {
   int* h_health = nullptr;        // host address of the flag (its device address is d_health_flag)
   int* d_health_flag = nullptr;
   bool health_shared = false;
+  int health_fatal = 1;           // HG_HEALTH_* bits that fail the step calls (hg_set_health_policy)
   std::vector<double> dx;         // per-element min corner distance (EstimateTimeStep)
   double save_umax = 0.0, save_amax = 0.0;
   // CUDA graphs of two time steps (hg_time_steps), one per trace-buffer parity at their start (a

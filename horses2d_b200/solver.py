@@ -165,6 +165,10 @@ class GpuDGSEM:
         self._check(self._lib.hg_health(self._h, C.byref(b), C.byref(e)))
         return b.value, e.value
 
+    def set_health_policy(self, fatal_bits):
+        """HEALTH_* bits that make the step calls fail (default HEALTH_NONFINITE)."""
+        self._check(self._lib.hg_set_health_policy(self._h, fatal_bits))
+
     def estimate_time_step(self, cfl, dt_cap):
         d = C.c_double(0.0)
         self._check(self._lib.hg_estimate_dt(self._h, cfl, dt_cap, C.byref(d)))

@@ -141,15 +141,16 @@ int  hg_residuals(hg_ctx* ctx, double out[4]);
 /* Health of the stepped state (the reference's "The simulation has crashed", printed when Q holds a
  * NaN: DGTimeIntegrator.f90:224-233).  Every RK update on the device checks its nodes for a
  * non-finite value, rho <= 0 or p <= 0 and records HG_HEALTH_* bits and one offending element
- * (0-based).  hg_time_step / hg_time_steps return HG_STATUS_CRASHED, with the message in
- * hg_last_error, once a flagged step has completed (checked without a synchronisation at the start
- * of each step call, so the call after the bad step reports it); the synchronising calls
- * (hg_residuals, hg_get_state, hg_estimate_dt, hg_synchronize) report it at once.  The flag stays
- * until hg_set_state replaces the state.  hg_health synchronises and returns the bits (0: clean) and
- * the element (-1 when clean). */
-enum { HG_STATUS_CRASHED = 2 };
-enum { HG_HEALTH_NONFINITE = 1, HG_HEALTH_DENSITY = 2, HG_HEALTH_PRESSURE = 4 };
+ * (0-based).  The bits in the fatal set (hg_set_health_policy; default HG_HEALTH_NONFINITE, the
+ * reference's criterion: transient nodes of negative pressure occur in its own benchmarks, e.g.
+ * CylinderMach2) make hg_time_step / hg_time_steps return HG_STATUS_CRASHED, with the message in
+ * hg_last_error, once the flagged step has completed: checked without a synchronisation at the start
+ * of each step call (so the call after the bad step reports it), and at once by the synchronising
+ * calls (hg_residuals, hg_get_state, hg_estimate_dt, hg_synchronize).  The record stays until
+ * hg_set_state replaces the state.  hg_health synchronises and returns the bits (0: clean) and the
+ * element (-1 when clean). */
 int  hg_health(hg_ctx* ctx, int32_t* bits, int32_t* element);
+int  hg_set_health_policy(hg_ctx* ctx, int32_t fatal_bits);
 /* == EstimateTimeStep, including the reference's running maxima (SAVE). */
 int  hg_estimate_dt(hg_ctx* ctx, double cfl, double dt_cap, double* dt);
 

@@ -122,6 +122,16 @@ extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
   o.av_hold = false;
 }
 
+// How the running maxima and the minimum of EstimateTimeStep treat a NaN (a node whose internal energy
+// has gone negative gives sqrt(NaN) for its sound speed).  Fortran leaves MAX / MIN with a NaN argument
+// to the processor.  Mode 0: the NaN is ignored (IEEE fmax / fmin).  Mode 1: MAX(a, b) = (a > b) ? a : b
+// and MIN(a, b) = (a < b) ? a : b with a the running value, as a single x86 maxsd / minsd computes it:
+// a NaN operand replaces the running value, and the next ordinary value replaces the NaN.
+static int g_minmax_nan = 0;
+extern "C" void or_set_minmax_nan(int mode) { g_minmax_nan = mode; }
+static inline double run_max(double a, double b) { return g_minmax_nan ? (a > b ? a : b) : std::fmax(a, b); }
+static inline double run_min(double a, double b) { return g_minmax_nan ? (a < b ? a : b) : std::fmin(a, b); }
+
 extern "C" double or_estimate_dt(void* h, double cfl, double dt_cap) {
   Oracle& o = *static_cast<Oracle*>(h);
   const Physics& ph = o.ph;
@@ -132,9 +142,9 @@ extern "C" double or_estimate_dt(void* h, double cfl, double dt_cap) {
       for (int j = 0; j < e.P; ++j) {
         const double* q = &Q[4 * (j * e.P + i)];
         const double nrm = std::sqrt(q[1] * q[1] + q[2] * q[2]);
-        o.save_umax = std::fmax(o.save_umax, nrm / q[0]);
+        o.save_umax = run_max(o.save_umax, nrm / q[0]);
         const double u = q[1] / q[0], v = q[2] / q[0];
-        o.save_amax = std::fmax(o.save_amax, std::sqrt(ph.gamma * ph.gm1 * (q[3] / q[0] - 0.5 * (u * u) - 0.5 * (v * v))));
+        o.save_amax = run_max(o.save_amax, std::sqrt(ph.gamma * ph.gm1 * (q[3] / q[0] - 0.5 * (u * u) - 0.5 * (v * v))));
       }
     auto dist = [&](int a, int b) {
       const double dx = o.nodeX[2 * e.nodes[a]] - o.nodeX[2 * e.nodes[b]];
@@ -142,7 +152,7 @@ extern "C" double or_estimate_dt(void* h, double cfl, double dt_cap) {
       return std::sqrt(dx * dx + dy * dy);
     };
     const double dx = std::fmin(std::fmin(dist(0, 1), dist(1, 2)), std::fmin(dist(2, 3), dist(0, 3)));
-    dt = std::fmin(dt, ph.Mach * std::sqrt(ph.gamma) * cfl * dx / (o.save_umax + o.save_amax) / (e.N + 1));
+    dt = run_min(dt, ph.Mach * std::sqrt(ph.gamma) * cfl * dx / (o.save_umax + o.save_amax) / (e.N + 1));
   }
   return dt;
 }

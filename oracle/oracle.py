@@ -84,6 +84,7 @@ def lib():
         L.or_ref_values.argtypes = [vp, dp]
         L.or_set_threads.argtypes = [C.c_int]
         L.or_set_av_g.argtypes = [vp, dp]
+        L.or_set_minmax_nan.argtypes = [C.c_int]
         L.or_zone_state.argtypes = [vp, C.c_int, dp]
         L.or_av_viscosity.argtypes = [vp, dp]
         L.or_element_geometry.argtypes = [vp, dp, dp, dp]

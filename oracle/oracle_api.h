@@ -94,6 +94,7 @@ void    or_get_qdot(void* h, double* QDot);
 void    or_time_derivative(void* h, double t);
 void    or_time_step(void* h, int scheme, double t, double dt);
 double  or_estimate_dt(void* h, double cfl, double dt_cap);
+void    or_set_minmax_nan(int mode);   /* NaN handling of the dt estimate's MAX / MIN (api.cpp) */
 void    or_residuals(void* h, double out[4]);
 /* Reference TimeIntegrator_Integrate (Approximation/DGTimeIntegrator.f90:159-255):
  * mode 1 transient, 0 steady.  Returns the number of iterations run. */

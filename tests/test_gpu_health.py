@@ -27,39 +27,56 @@ def poisoned(Q, kind, element=11, P=5):
         Q[element, 7, 1] = np.nan
     elif kind == "density":
         Q[element, :, 0] = -0.5
-    else:   # pressure: kinetic energy above the total energy
-        Q[element, :, 3] = 0.1 * Q[element, :, 3]
+    else:   # pressure: total energy below the kinetic energy
+        Q[element, :, 3] = 0.01 * Q[element, :, 3]
     return Q.ravel()
 
 
 @pytest.mark.parametrize("ns", [False, True])
-@pytest.mark.parametrize("kind,bit", [("nan", hg.HEALTH_NONFINITE), ("density", hg.HEALTH_DENSITY),
-                                      ("pressure", hg.HEALTH_PRESSURE)])
-def test_bad_state_is_reported_by_the_next_call(ns, kind, bit):
+def test_nan_fails_the_next_call_and_a_new_state_clears_it(ns):
     g, Q = vortex(ns)
     g.set_state(Q)
     g.time_step(hg.SCHEME_RK3, 0.0, 1e-3)
     assert g.health() == (0, -1)                       # a clean run stays clean
-    g.set_state(poisoned(Q, kind))
+    g.set_state(poisoned(Q, "nan"))
     g.time_step(hg.SCHEME_RK3, 0.0, 1e-3)              # asynchronous: the step itself is queued
     bits, el = g.health()
-    assert bits & bit and 0 <= el < 64
+    assert bits & hg.HEALTH_NONFINITE and 0 <= el < 64
     with pytest.raises(hg.HorsesGpuError) as ex:
         g.time_step(hg.SCHEME_RK3, 1e-3, 1e-3)
     assert ex.value.status == hg.STATUS_CRASHED and "crashed" in str(ex.value)
     with pytest.raises(hg.HorsesGpuError):
         g.residuals()
-    g.set_state(Q)                                    # a new state clears the flag
+    g.set_state(Q)                                    # a new state clears the record
     assert g.health() == (0, -1)
     g.time_steps(hg.SCHEME_RK3, 6, 0.0, 1e-3)
     assert np.all(np.isfinite(g.residuals()))
 
 
+@pytest.mark.parametrize("ns", [False, True])
+@pytest.mark.parametrize("kind,bit", [("density", hg.HEALTH_DENSITY), ("pressure", hg.HEALTH_PRESSURE)])
+def test_negative_density_and_pressure_are_recorded_and_fatal_on_request(ns, kind, bit):
+    g, Q = vortex(ns)
+    g.set_state(poisoned(Q, kind))
+    g.time_step(hg.SCHEME_RK3, 0.0, 1e-3)
+    bits, el = g.health()
+    assert bits & (bit | hg.HEALTH_NONFINITE) and 0 <= el < 64
+    if not bits & hg.HEALTH_NONFINITE:                 # recorded, not fatal under the default policy
+        g.time_step(hg.SCHEME_RK3, 1e-3, 1e-3)
+    g.set_health_policy(hg.HEALTH_NONFINITE | hg.HEALTH_DENSITY | hg.HEALTH_PRESSURE)
+    with pytest.raises(hg.HorsesGpuError) as ex:
+        g.time_step(hg.SCHEME_RK3, 2e-3, 1e-3)
+    assert ex.value.status == hg.STATUS_CRASHED
+    g.set_state(Q)
+    g.time_steps(hg.SCHEME_RK3, 6, 0.0, 1e-3)         # clean under the strict policy
+    assert g.health() == (0, -1)
+
+
 def test_multi_step_call_and_fp32_path_report_it():
     g, Q = vortex(False, hg.PREC_FP32)
-    g.set_state(poisoned(Q, "density"))
+    g.set_state(poisoned(Q, "nan"))
     g.time_steps(hg.SCHEME_RK3, 8, 0.0, 1e-3)
     with pytest.raises(hg.HorsesGpuError) as ex:
         g.synchronize()
     assert ex.value.status == hg.STATUS_CRASHED
-    assert g.health()[0] & hg.HEALTH_DENSITY
+    assert g.health()[0] & hg.HEALTH_NONFINITE
