@@ -149,6 +149,8 @@ int  hg_residuals(hg_ctx* ctx, double out[4]);
  * calls (hg_residuals, hg_get_state, hg_estimate_dt, hg_synchronize).  The record stays until
  * hg_set_state replaces the state.  hg_health synchronises and returns the bits (0: clean) and the
  * element (-1 when clean). */
+enum { HG_STATUS_CRASHED = 2 };
+enum { HG_HEALTH_NONFINITE = 1, HG_HEALTH_DENSITY = 2, HG_HEALTH_PRESSURE = 4 };
 int  hg_health(hg_ctx* ctx, int32_t* bits, int32_t* element);
 int  hg_set_health_policy(hg_ctx* ctx, int32_t fatal_bits);
 /* == EstimateTimeStep, including the reference's running maxima (SAVE). */
