@@ -375,20 +375,43 @@ static void ns_prologue(hg_ctx* c) {
 }
 
 // ------------------------------------------------------------------ dt estimate
-__global__ void element_speed_kernel(int n_el, int NP, const double* Q, double gamma, double gm1, double* out) {
+// TimeIntegrator_EstimateTimeStep (DGTimeIntegrator.f90:462-511) keeps running maxima of |u| and a over
+// the nodes (iXi outer, iEta inner) of the elements in mesh order, SAVEd across calls, and takes
+// dt = MIN(dt, M sqrt(gamma) CFL dx / (umax + amax) / (N + 1)) after each element.  A node whose internal
+// energy has gone negative (transients of the CylinderMach2 benchmark) gives a = sqrt(<0) = NaN.  The
+// reference's compiled MAX / MIN behave as one x86 maxsd / minsd with the running value first: a NaN
+// operand replaces the running value and the next ordinary value replaces the NaN -- with that rule the
+// benchmark's asserted iteration count (15599) is reproduced.  Per element this kernel reports, for
+// |u| and a, the plain maximum (flag 0: no NaN among its nodes) or the maximum after its last NaN node,
+// NaN if that is the last node (flag 1): the running value after the element is then run_max(R, value)
+// or that value; the host applies the element sequence.
+__global__ void element_speed_kernel(int n_el, int P, const double* Q, double gamma, double gm1, double* out) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= n_el) return;
-  double um = 0.0, am = 0.0;
-  const double* q = Q + size_t(e) * NP * 4;
-  for (int n = 0; n < NP; ++n, q += 4) {
-    const double nrm = sqrt(q[1] * q[1] + q[2] * q[2]);
-    um = fmax(um, nrm / q[0]);
-    const double u = q[1] / q[0], v = q[2] / q[0];
-    am = fmax(am, sqrt(gamma * gm1 * (q[3] / q[0] - 0.5 * (u * u) - 0.5 * (v * v))));
-  }
-  out[2 * e] = um;
-  out[2 * e + 1] = am;
+  const double* qe = Q + size_t(e) * P * P * 4;
+  double ua = -INFINITY, uafter = -INFINITY, aa = -INFINITY, aafter = -INFINITY;
+  bool unan = false, ulast = false, anan = false, alast = false;
+  for (int i = 0; i < P; ++i)
+    for (int j = 0; j < P; ++j) {
+      const double* q = qe + 4 * (j * P + i);
+      const double u = sqrt(q[1] * q[1] + q[2] * q[2]) / q[0];
+      const double uu = q[1] / q[0], vv = q[2] / q[0];
+      const double a = sqrt(gamma * gm1 * (q[3] / q[0] - 0.5 * (uu * uu) - 0.5 * (vv * vv)));
+      if (u != u) { unan = ulast = true; uafter = -INFINITY; }
+      else { ulast = false; ua = u > ua ? u : ua; uafter = u > uafter ? u : uafter; }
+      if (a != a) { anan = alast = true; aafter = -INFINITY; }
+      else { alast = false; aa = a > aa ? a : aa; aafter = a > aafter ? a : aafter; }
+    }
+  out[4 * size_t(e) + 0] = unan ? (ulast ? NAN : uafter) : ua;
+  out[4 * size_t(e) + 1] = unan ? 1.0 : 0.0;
+  out[4 * size_t(e) + 2] = anan ? (alast ? NAN : aafter) : aa;
+  out[4 * size_t(e) + 3] = anan ? 1.0 : 0.0;
 }
+
+// The reference's MAX / MIN on the running value a and a new operand b (see element_speed_kernel).
+static inline double run_max(double a, double b) { return a > b ? a : b; }
+static inline double run_min(double a, double b) { return a < b ? a : b; }
+static inline double element_running(double R, const double* v) { return v[1] != 0.0 ? v[0] : run_max(R, v[0]); }
 
 // ------------------------------------------------------------------ creation
 void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs,
@@ -608,7 +631,7 @@ void ctx_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, cons
   c->d_QDot = dalloc<double>(c->ndof);
   c->d_resid = dalloc<double>(size_t(max_grid(c)) * 4);
   c->d_resid_out = dalloc<double>(4);
-  c->d_elmax = dalloc<double>(size_t(E) * 2);
+  c->d_elmax = dalloc<double>(size_t(E) * 4);
   if (c->av != HG_AV_NONE) {
     // Edge_t%Area = sum_p dS(p) w(p) in the edge's node order (QuadMesh_Construct.incf:270-303), per side;
     // per element Ceps sqrt(Volume)/(N+1) and the sum of the four areas (JumpsBasedElementViscosity)
@@ -994,11 +1017,11 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
         hg_ctx* p = c->parts[pi];
         timed(c, HG_KERNEL_SPEED, [&] {
           element_speed_kernel<<<(p->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
-              p->n_el, p->P * p->P, p->d_Q, c->gamma, c->gamma - 1.0, p->d_elmax);
+              p->n_el, p->P, p->d_Q, c->gamma, c->gamma - 1.0, p->d_elmax);
         });
         ++c->launches;
         HG_CUDA(cudaGetLastError());
-        em[pi].resize(size_t(p->n_el) * 2);
+        em[pi].resize(size_t(p->n_el) * 4);
         HG_CUDA(cudaMemcpyAsync(em[pi].data(), p->d_elmax, em[pi].size() * sizeof(double), cudaMemcpyDeviceToHost,
                                 c->stream));
       }
@@ -1006,30 +1029,30 @@ extern "C" int hg_estimate_dt(hg_ctx* c, double cfl, double dt_cap, double* dt) 
       health_check(c);
       double d = dt_cap;
       for (int e = 0; e < c->n_el; ++e) {
-        const double* v = &em[c->el_part[e]][2 * size_t(c->el_local[e])];
-        c->save_umax = std::fmax(c->save_umax, v[0]);
-        c->save_amax = std::fmax(c->save_amax, v[1]);
-        d = std::fmin(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->el_N[e] + 1));
+        const double* v = &em[c->el_part[e]][4 * size_t(c->el_local[e])];
+        c->save_umax = element_running(c->save_umax, v);
+        c->save_amax = element_running(c->save_amax, v + 2);
+        d = run_min(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->el_N[e] + 1));
       }
       *dt = d;
       return 0;
     }
     timed(c, HG_KERNEL_SPEED, [&] {
       element_speed_kernel<<<(c->n_el + threads - 1) / threads, threads, 0, c->stream>>>(
-          c->n_el, c->P * c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
+          c->n_el, c->P, c->d_Q, c->gamma, c->gamma - 1.0, c->d_elmax);
     });
     ++c->launches;
     HG_CUDA(cudaGetLastError());
-    std::vector<double> em(size_t(c->n_el) * 2);
+    std::vector<double> em(size_t(c->n_el) * 4);
     HG_CUDA(cudaMemcpyAsync(em.data(), c->d_elmax, em.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HG_CUDA(cudaStreamSynchronize(c->stream));
     health_check(c);
     // running maxima over elements in mesh order, kept across calls
     double d = dt_cap;
     for (int e = 0; e < c->n_el; ++e) {
-      c->save_umax = std::fmax(c->save_umax, em[2 * e]);
-      c->save_amax = std::fmax(c->save_amax, em[2 * e + 1]);
-      d = std::fmin(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->N + 1));
+      c->save_umax = element_running(c->save_umax, &em[4 * size_t(e)]);
+      c->save_amax = element_running(c->save_amax, &em[4 * size_t(e) + 2]);
+      d = run_min(d, c->mach * std::sqrt(c->gamma) * cfl * c->dx[e] / (c->save_umax + c->save_amax) / (c->N + 1));
     }
     *dt = d;
     return 0;

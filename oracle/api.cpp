@@ -122,12 +122,15 @@ extern "C" void or_time_step(void* h, int scheme, double t, double dt) {
   o.av_hold = false;
 }
 
-// How the running maxima and the minimum of EstimateTimeStep treat a NaN (a node whose internal energy
-// has gone negative gives sqrt(NaN) for its sound speed).  Fortran leaves MAX / MIN with a NaN argument
-// to the processor.  Mode 0: the NaN is ignored (IEEE fmax / fmin).  Mode 1: MAX(a, b) = (a > b) ? a : b
-// and MIN(a, b) = (a < b) ? a : b with a the running value, as a single x86 maxsd / minsd computes it:
-// a NaN operand replaces the running value, and the next ordinary value replaces the NaN.
-static int g_minmax_nan = 0;
+// How the running maxima and the minimum of EstimateTimeStep (DGTimeIntegrator.f90:462-511) treat a NaN:
+// a node whose internal energy has gone negative gives sqrt(<0) = NaN for its sound speed, which happens in
+// the transient of the CylinderMach2 benchmark.  Fortran leaves MAX / MIN with a NaN argument to the
+// processor.  Mode 1 (default): MAX(a, b) = (a > b) ? a : b and MIN(a, b) = (a < b) ? a : b with a the
+// running value, as one x86 maxsd / minsd computes it -- a NaN operand replaces the running value and the
+// next ordinary value replaces the NaN.  With it the oracle reproduces the benchmark's asserted iteration
+// count (15599), residuals and lift / drag (TestCases/Benchmark/Simulations/CylinderMach2/SETUP/
+// ProblemFile.f90:79-95); with mode 0 (IEEE fmax / fmin: the NaN is ignored) it takes 16079 steps.
+static int g_minmax_nan = 1;
 extern "C" void or_set_minmax_nan(int mode) { g_minmax_nan = mode; }
 static inline double run_max(double a, double b) { return g_minmax_nan ? (a > b ? a : b) : std::fmax(a, b); }
 static inline double run_min(double a, double b) { return g_minmax_nan ? (a < b ? a : b) : std::fmin(a, b); }

@@ -1,0 +1,158 @@
+"""Parity at the benchmark configurations' own sizes (the residual path of
+Approximation/DGSpatialDiscretizationMethods.f90:94-235 and the RK schemes of DGTimeIntegrator.f90:263-365),
+CUDA against the FP64 oracle on the same mesh and state:
+
+* C2: Navier-Stokes past a cylinder on the full O-grid of 64 radial x 128 azimuthal curved quads (r 0.5 -> 30,
+  stretching 1.05), N = 5, BR1, Roe, adiabatic wall, far field: residual <= 1e-12, 100 RK3 steps <= 1e-10;
+* C3: the Mach-3 shock workload at 512 x 64, N = 3, HLL, SIPG at Re = 0, modal-decay Laplacian dissipation:
+  residual <= 1e-12, 10 RK3 steps <= 1e-10; FP32 bulk after 200 steps against the oracle's run
+  (tests/golden/shock_c3_oracle.npz) and FP32 + learned sensor after 50 steps against the oracle driven by
+  the FP64 restatement of the learned indicator: density <= 1e-5 relative L2;
+* C5: a 128 x 128 sample of the Kelvin-Helmholtz workload (N = 7, Re 1e4, M 0.3, SIPG, Roe, modal-decay
+  Laplacian dissipation): residual <= 1e-12, 10 RK3 steps <= 1e-10, FP32 after 10 steps <= 1e-5;
+* C1: the 16 x 16 vortex at N = 4: FP32 bulk after the configuration's 100 RK3 steps, density <= 1e-5.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from oracle import mlp as omlp
+import horses2d_b200 as hg
+from horses2d_b200 import mesh as hmesh, cases, sensor as S
+from cases_util import rel_l2, perturbed, dirichlet_state, vortex_case, GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL_STAGE, TOL_STEPS, TOL_FP32 = 1e-12, 1e-10, 1e-5
+SEED = 20261203
+
+
+@pytest.fixture(autouse=True, scope="module")
+def oracle_threads():
+    O.lib().or_set_threads(os.cpu_count() or 1)
+
+
+def residual_and_steps(orc, g, Q, dt, steps):
+    orc.set_state(Q)
+    g.set_state(Q)
+    ref = orc.time_derivative(0.0)
+    out = g.compute_time_derivative(0.0)
+    r_stage = rel_l2(out, ref)
+    for s in range(steps):
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, steps, 0.0, dt)
+    return r_stage, rel_l2(g.state(), orc.state())
+
+
+def test_c2_full_ogrid_br1():
+    m = hmesh.ogrid(64, 128, 0.5, 30.0, 1.05)
+    orc = O.Oracle(m, 5, nodes=O.LG, riemann=O.ROE, mach=0.2, reynolds=100.0, prandtl=0.72, navier_stokes=1,
+                   viscous=O.BR1, bcs=[dict(type=O.BC_VISCOUSWALL, wall_type=2), dict(type=O.BC_FARFIELD)])
+    q = dirichlet_state(orc, 0.2)
+    g = hg.GpuDGSEM(hmesh.build_descriptor(m, 5, hg.NODES_LG), mach=0.2, reynolds=100.0, navier_stokes=1,
+                    viscous=hg.BR1, node_type=hg.NODES_LG, riemann=hg.ROE,
+                    bcs=[dict(type=hg.BC_VISCOUSWALL, wall_type=2), dict(type=hg.BC_FARFIELD, state=q)])
+    assert g.ndof == 4 * 64 * 128 * 36
+    Q = perturbed(np.tile(q, orc.ndof // 4), 1e-3, seed=SEED)
+    orc.set_state(Q)
+    dt = orc.estimate_dt(0.05, 1.0)
+    r_stage, r_steps = residual_and_steps(orc, g, Q, dt, 100)
+    assert r_stage <= TOL_STAGE
+    assert r_steps <= TOL_STEPS
+
+
+def shock_pair(precision=hg.PREC_FP64, indicator=O.IND_MODAL, sensor=hg.SENSOR_MODAL, learned=None):
+    import sys
+    sys.path.insert(0, GOLDEN)
+    from make_shock_oracle import shock_oracle
+    orc, Q0 = shock_oracle(indicator)
+    qin, qout = orc.zone_state(3), orc.zone_state(4)
+    kw = dict(mach=3.0, reynolds=0.0, navier_stokes=1, viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0,
+              node_type=hg.NODES_LG, riemann=hg.HLL, av_type=hg.AV_LAPLACIAN, av_intensity=1.0,
+              bcs=[dict(type=hg.BC_EULERWALL), dict(type=hg.BC_EULERWALL), dict(type=hg.BC_DIRICHLET, state=qin),
+                   dict(type=hg.BC_NEWDIRICHLET, state=qout)])
+    g = hg.GpuDGSEM(orc.export_mesh(), precision=precision, **kw)
+    if learned is None:
+        g.set_sensor(sensor)
+    else:
+        g.set_sensor(hg.SENSOR_LEARNED, mlp=learned[0], lo=learned[1], hi=learned[2])
+    return orc, g, Q0
+
+
+def test_c3_full_shock_modal():
+    orc, g, Q0 = shock_pair()
+    assert g.ndof == 4 * 512 * 64 * 16
+    orc.set_state(Q0)
+    dt = orc.estimate_dt(0.1, 1.0)
+    r_stage, r_steps = residual_and_steps(orc, g, Q0, dt, 10)
+    assert r_stage <= TOL_STAGE
+    assert r_steps <= TOL_STEPS
+    assert np.max(orc.av_viscosity()) > 0.0          # the shock is flagged: the dissipation is exercised
+
+
+def test_c3_fp32_after_200_steps_against_the_oracle_run():
+    fx = np.load(os.path.join(GOLDEN, "shock_c3_oracle.npz"))
+    _, g, Q0 = shock_pair(precision=hg.PREC_FP32)
+    g.set_state(Q0)
+    g.time_steps(hg.SCHEME_RK3, int(fx["steps"][0]), 0.0, float(fx["dt"][0]))
+    rho = g.state()[0::4]
+    ref = fx["rho"].astype(np.float64)
+    assert rel_l2(rho, ref) <= TOL_FP32
+
+
+def test_c3_fp32_learned_against_the_oracle_with_the_learned_indicator():
+    params, lo, hi, info = S.train_two_rounds(16, 11, nx=512, ny=64, N=3, steps=100, epochs=12, batch=4096)
+    orc, g, Q0 = shock_pair(precision=hg.PREC_FP32, indicator=O.IND_EXTERNAL, learned=(params, lo, hi))
+    orc.set_state(Q0)
+    g.set_state(Q0)
+    dt = orc.estimate_dt(0.1, 1.0)
+    xi = omlp.gauss_nodes(4)
+    s0 = np.log10(1.0 / 4 ** 4)
+    flagged = 0
+    for s in range(50):
+        G, _ = omlp.learned_indicator(params, lo, hi, orc.state().reshape(-1, 16, 4), xi, s0)
+        flagged = max(flagged, int((G > S.TROUBLED).sum()))
+        orc.set_av_g(G)
+        orc.time_step(O.RK3, s * dt, dt)
+    g.time_steps(hg.SCHEME_RK3, 50, 0.0, dt)
+    assert flagged > 0                                 # the learned indicator drives the dissipation
+    assert rel_l2(g.state()[0::4], orc.state()[0::4]) <= TOL_FP32
+
+
+def kh_sample(n=128, precision=hg.PREC_FP64):
+    m = hmesh.cartesian(n, n, 0.0, 1.0, 0.0, 1.0)
+    orc = O.Oracle(m, 7, nodes=O.LG, riemann=O.ROE, mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=O.IP,
+                   ip_method=0, sigma0_ip=10.0, bcs=hmesh.periodic_bcs_cartesian(), av_type=O.AV_LAPLACIAN,
+                   av_intensity=1.0, av_indicator=O.IND_MODAL)
+    X = orc.coords()
+    Q = cases.kelvin_helmholtz(X[:, 0], X[:, 1], seed=SEED).ravel()
+    g = hg.GpuDGSEM(orc.export_mesh(), precision=precision, mach=0.3, reynolds=1.0e4, navier_stokes=1,
+                    viscous=hg.IP, ip_method=hg.SIPG, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.ROE,
+                    av_type=hg.AV_LAPLACIAN, av_intensity=1.0, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    g.set_sensor(hg.SENSOR_MODAL)
+    return orc, g, Q, 0.05 / n ** 2
+
+
+def test_c5_sample_sipg_modal():
+    orc, g, Q, dt = kh_sample()
+    r_stage, r_steps = residual_and_steps(orc, g, Q, dt, 10)
+    assert r_stage <= TOL_STAGE
+    assert r_steps <= TOL_STEPS
+    orc32, g32, _, _ = kh_sample(precision=hg.PREC_FP32)
+    g32.set_state(Q)
+    g32.time_steps(hg.SCHEME_RK3, 10, 0.0, dt)
+    assert rel_l2(g32.state()[0::4], orc.state()[0::4]) <= TOL_FP32
+
+
+def test_c1_fp32_after_100_steps():
+    orc, Q0, kw = vortex_case(16, 4)
+    orc.set_state(Q0)
+    dt = orc.estimate_dt(0.4, 1.0)
+    for s in range(100):
+        orc.time_step(O.RK3, s * dt, dt)
+    g = hg.GpuDGSEM(orc.export_mesh(), precision=hg.PREC_FP32, **kw)
+    g.set_state(Q0)
+    g.time_steps(hg.SCHEME_RK3, 100, 0.0, dt)
+    assert rel_l2(g.state()[0::4], orc.state()[0::4]) <= TOL_FP32

@@ -5,14 +5,14 @@ inflow, a partially non-reflective pressure outlet, transient Williamson RK5 to 
 (dt cap 1e-2, re-estimated every 100 iterations), built with the package's own mesh builder and driven
 by GpuDGSEM.integrate (the reference's integration loop).
 
+* Against the reference's own benchmark check (ProblemFile.f90:79-95, tests/golden/benchmarks.json):
+  the final iteration 15599, residuals to 1e-9 and lift and drag to 1e-12, as the reference asserts.
+  The iteration count depends on how the dt estimate's running maxima treat the NaN sound speed of
+  nodes whose internal energy turns negative in the transient (hg_estimate_dt follows the reference's
+  compiled MAX / MIN; with NaN-ignoring maxima the run takes 16079 steps).
 * Against the oracle's run of the same setup (tests/golden/cylinder_mach2_oracle.json, written by
-  make_cylinder_mach2_oracle.py): the same number of iterations (16,079), final residuals to 1e-10
-  relative, lift and drag to 1e-12 -- after 80,000 residual evaluations through a forming bow shock.
-* Against the reference's own benchmark check (benchmarks.json): lift to 1e-12 as the reference
-  asserts; drag to 5e-8 and the residuals to 5e-5 (the reference asserts 1e-12 / 1e-11).  The
-  reference's run took 15,599 steps to reach t = 10, 3 % larger on average than this dt rule (the
-  reference's, with its saved running maxima, which reproduces the VortexTransport and Ramp
-  iteration counts) gives here and in the oracle alike; the flow at t = 10 agrees to the figures above.
+  make_cylinder_mach2_oracle.py): the same iterations, residuals to 1e-10 relative, lift and drag to
+  1e-12 -- after 78,000 residual evaluations through a forming bow shock.
 """
 import json
 import os
@@ -50,11 +50,12 @@ def test_cylinder_mach2_benchmark_on_device():
     rho, V, p_ref = 101325.0 / (287.15 * 273.15), mach * np.sqrt(1.4 * 287.15 * 273.15), 101325.0
     force = si["pressure_force"] * p_ref / (0.5 * rho * V * V)     # Re = 0: no viscous force
     cl, cd = force[1], force[0]
+    # the reference's benchmark check
+    assert it == ref["expected_iter"] == 15599
+    assert np.max(np.abs(res - np.array(ref["residuals"]))) <= 1e-9
+    assert abs(cl - ref["cl"]) <= 1e-12
+    assert abs(cd - ref["cd"]) <= 1e-12
     # the oracle's run
     assert it == orc["iterations"]
     np.testing.assert_allclose(res, orc["residuals"], rtol=1e-10, atol=0)
     assert abs(cl - orc["cl"]) <= 1e-12 and abs(cd - orc["cd"]) <= 1e-12
-    # the reference's benchmark check
-    assert abs(cl - ref["cl"]) <= 1e-12
-    assert abs(cd - ref["cd"]) <= 5e-8
-    assert np.max(np.abs(res - np.array(ref["residuals"]))) <= 5e-5

@@ -258,3 +258,17 @@ def test_ramp_benchmark_golden():
                           residual_target=1e-8)
     assert it == golden["expected_iter"]
     assert np.max(np.abs(orc.residuals() - np.array(golden["residuals"]))) <= 1e-11
+
+
+def test_cylinder_mach2_oracle_run_meets_the_reference_check():
+    """CylinderMach2 (TestCases/Benchmark/Simulations/CylinderMach2/SETUP/ProblemFile.f90:79-95): the committed
+    oracle run (tests/golden/make_cylinder_mach2_oracle.py, about 13 minutes on 8 threads) passes the
+    reference's own assertions -- final iteration 15599, residuals to 1e-9, lift and drag to 1e-12.  The
+    iteration count hinges on the dt estimate's MAX / MIN with the NaN sound speed of transient negative-
+    pressure nodes (oracle/api.cpp run_max / run_min); NaN-ignoring maxima give 16079 steps."""
+    import json
+    ref = json.load(open(os.path.join(GOLDEN, "benchmarks.json")))["CylinderMach2"]
+    run = json.load(open(os.path.join(GOLDEN, "cylinder_mach2_oracle.json")))
+    assert run["iterations"] == ref["expected_iter"] == 15599 and run["t"] == 10.0
+    assert np.max(np.abs(np.array(run["residuals"]) - np.array(ref["residuals"]))) <= 1e-9
+    assert abs(run["cl"] - ref["cl"]) <= 1e-12 and abs(run["cd"] - ref["cd"]) <= 1e-12
