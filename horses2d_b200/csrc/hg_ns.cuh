@@ -106,9 +106,9 @@ __device__ __forceinline__ real trace_of(const NSTiles<P, EPB, real, AFFINE, ST>
                                          int le, int side, int kk, const real* lbv) {
   real t = real(0);
 #pragma unroll
-  for (int l = 0; l < P; ++l) {
-    const int node = (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
-    t += src[k][le][node] * lbv[l];
+  for (int m = 0; m < P; ++m) {
+    const int l = trace_step<real>(P, m, kk);
+    t += src[k][le][face_node(P, side, l, kk)] * lbv[l];
   }
   return t;
 }
@@ -120,8 +120,9 @@ __device__ __forceinline__ void trace4(const real (*src)[EPB][P * P], int le, in
 #pragma unroll
   for (int k = 0; k < 4; ++k) out[k] = real(0);
 #pragma unroll
-  for (int l = 0; l < P; ++l) {
-    const int node = (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
+  for (int m = 0; m < P; ++m) {
+    const int l = trace_step<real>(P, m, kk);
+    const int node = face_node(P, side, l, kk);
     const real w = lbv[l];
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] += src[k][le][node] * w;
@@ -134,12 +135,12 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
                                                  const Phys<real>& ph, int le, int tid, int e, bool active,
                                                  const real* geoE) {
   constexpr int NP = P * P, FT = 4 * P;
-  const real* hatD = s.mat;
+  const real* hatDT = s.mat;   // transposed: hatDT[l * P + i] = hatD(i, l)
   const real* lb0 = s.mat + NP;
   const real* lb1 = lb0 + P;
   const real* lbw0 = lb1 + P;
   const real* lbw1 = lbw0 + P;
-  const real* D = lbw1 + P;
+  const real* DT = lbw1 + P;   // transposed D
   const int i = tid % P, j = tid / P;
   if (!IP) {
     // BR1 face terms u* dS n (outward normal of this element)
@@ -162,7 +163,8 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
         real us[4];
         if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
           const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
-          const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+          real tp[4];
+          ld4(a.T_in + (size_t(sd.x) * P + kn) * 4, tp);
 #pragma unroll
           for (int k = 0; k < 4; ++k) us[k] = kind == SIDE_RIGHT ? real(0.5) * (tp[k] + qo[k]) : real(0.5) * (qo[k] + tp[k]);
         } else {
@@ -189,7 +191,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
       real dxi[4] = {real(0), real(0), real(0), real(0)}, deta[4] = {real(0), real(0), real(0), real(0)};
 #pragma unroll
       for (int l = 0; l < P; ++l) {
-        const real di = D[i * P + l], dj = D[j * P + l];
+        const real di = DT[l * P + i], dj = DT[l * P + j];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           dxi[k] += di * s.Q[k][le][j * P + l];
@@ -207,7 +209,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
         real axi[4] = {real(0), real(0), real(0), real(0)}, aeta[4] = {real(0), real(0), real(0), real(0)};
 #pragma unroll
         for (int l = 0; l < P; ++l) {
-          const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+          const real hi = hatDT[l * P + i], hj = hatDT[l * P + j];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
             axi[k] += hi * s.Q[k][le][j * P + l];
@@ -223,7 +225,7 @@ __device__ __forceinline__ void element_gradient(const NSArgs<real>& a, NSTiles<
 #pragma unroll
         for (int l = 0; l < P; ++l) {
           const int nx_ = j * P + l, ny_ = l * P + i;
-          const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+          const real hi = hatDT[l * P + i], hj = hatDT[l * P + j];
           const real j0 = s.Ja[0][le][nx_], j1 = s.Ja[1][le][ny_], j2 = s.Ja[2][le][nx_], j3 = s.Ja[3][le][ny_];
 #pragma unroll
           for (int k = 0; k < 4; ++k) {
@@ -250,7 +252,14 @@ template <int P, int EPB, typename real, bool AFFINE, bool ST>
 __device__ __forceinline__ void load_tiles(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE, ST>& s, int flat, int le,
                                            int tid, int e, bool active, real* geoE) {
   constexpr int NP = P * P;
-  for (int k = flat; k < 3 * NP + 7 * P; k += blockDim.x) s.mat[k] = real(a.mats[k]);
+  // hatD and D are held transposed (column l contiguous): a warp then reads hatD(i, l) over its nodes'
+  // i from consecutive words instead of a stride of P (bank conflicts)
+  for (int k = flat; k < 3 * NP + 7 * P; k += blockDim.x) {
+    int src = k;
+    if (k < NP) src = (k % P) * P + k / P;
+    else if (k >= NP + 4 * P && k < 2 * NP + 4 * P) { const int m = k - NP - 4 * P; src = NP + 4 * P + (m % P) * P + m / P; }
+    s.mat[k] = real(a.mats[src]);
+  }
   if (active) {
     const double2* qp = reinterpret_cast<const double2*>(a.Q + (size_t(e) * NP + tid) * 4);
     const double2 q01 = qp[0], q23 = qp[1];
@@ -389,8 +398,221 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_gradient_kernel(NSArgs<re
     real tx[4], ty[4];
     trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, tx);
     trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, ty);
+    st4(gp, tx);
+    st4(gp + 4, ty);
+  }
+}
+
+// Volume flux of node n of element le: F = Fi - (mu + mu_a) Fv (- mu_a grad Q for the Laplacian
+// dissipation), contravariant, into s.Fc and s.Gc (QDotVolumeLoop, DGSpatialDiscretizationMethods.f90:
+// 243-268).  Reads the node's Q and gradient from the tiles.
+template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
+__device__ __forceinline__ void ns_volume_flux(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+                                               const Phys<real>& ph, int le, int n, real mu_e, bool need_grad,
+                                               bool visc, const real* geoE) {
+  constexpr int NP = P * P;
+  const int i = n % P, j = n / P;
+  const real mu = ph.mu;
+  real Ja00, Ja01, Ja10, Ja11;
+  if constexpr (AFFINE) { Ja00 = geoE[0]; Ja01 = geoE[1]; Ja10 = geoE[2]; Ja11 = geoE[3]; }
+  else { Ja00 = s.Ja[0][le][n]; Ja01 = s.Ja[1][le][n]; Ja10 = s.Ja[2][le][n]; Ja11 = s.Ja[3][le][n]; }
+  real q[4], gx[4], gy[4], fi[4], gi[4], fv[4], gv[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) { gp[k] = tx[k]; gp[4 + k] = ty[k]; }
+  for (int k = 0; k < 4; ++k) { q[k] = s.Q[k][le][n]; gx[k] = s.dQ[0][k][le][n]; gy[k] = s.dQ[1][k][le][n]; }
+  inviscid_flux(ph, q, fi, gi);
+  if (visc) viscous_flux(ph, q, gx, gy, fv, gv);
+  else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { fv[k] = real(0); gv[k] = real(0); }
+  }
+  const real mu_v = (AV && a.av == 2) ? mu + mu_e : mu;
+  real ax[4] = {real(0), real(0), real(0), real(0)}, ay[4] = {real(0), real(0), real(0), real(0)};
+  if (AV && a.av == 1 && need_grad) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
+    if (IP) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { ax[k] = gx[k]; ay[k] = gy[k]; }
+    } else {
+      const real* DT = s.mat + NP + 4 * P;   // D (transposed) follows hatD, lb0, lb1, lbw0, lbw1
+      const real iJl = AFFINE ? geoE[4] : real(1) / s.Ja[4][le][n];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        real dxi = real(0), deta = real(0);
+#pragma unroll
+        for (int l = 0; l < P; ++l) {
+          dxi += DT[l * P + i] * s.Q[k][le][j * P + l];
+          deta += DT[l * P + j] * s.Q[k][le][l * P + i];
+        }
+        ax[k] = (dxi * Ja00 + deta * Ja01) * iJl;
+        ay[k] = (dxi * Ja10 + deta * Ja11) * iJl;
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    real f = fi[k] - mu_v * fv[k], g = gi[k] - mu_v * gv[k];
+    if (AV && a.av == 1) { f = f - mu_e * ax[k]; g = g - mu_e * ay[k]; }
+    s.Fc[k][le][n] = f * Ja00 + g * Ja10;
+    s.Gc[k][le][n] = f * Ja01 + g * Ja11;
+  }
+}
+
+// Face node t (= side * P + kk) of element le: the side's flux F* dS (signed for a RIGHT side) into
+// s.face[0..3] and, with SIPG / NIPG, the contravariant gradient-face terms into s.face[4..11]
+// (ComputeRiemannSolver_* and the viscous face loops, DGSpatialDiscretizationMethods.f90:545-1511;
+// DGViscous_BR1.f90:311-371, DGViscous_IP.f90:120-134, 240-247; DGArtificialDissipation.f90:208-249).
+template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
+__device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+                                             const Phys<real>& ph, int le, int e, int t, real mu_e, bool visc,
+                                             const real* geoE) {
+  constexpr int NP = P * P;
+  const real mu = ph.mu;
+  const real* lb0 = s.mat + NP;
+  const real* lb1 = lb0 + P;
+  const int sd_ = t / P, kk = t % P;
+  const int4 sd = a.side[size_t(e) * 4 + sd_];
+  const int kind = sd.y & 15;
+  if (kind == SIDE_FLUX) {   // inviscid and viscous flux of the mortar kernel, and its gradient-face terms
+    real fp[4];
+    ld4(a.NF + (size_t(sd.x) * P + kk) * 4, fp);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s.face[k][le][t] = fp[k];
+    if (IP && a.grad_faces && visc) {
+      const real* gp = a.NFG + (size_t(sd.x) * P + kk) * 8;
+      const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+      real fJa00, fJa01, fJa10, fJa11, fJ;
+      if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+      else {
+        fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
+        fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
+        fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
+        fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
+        fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        s.face[4 + k][le][t] = (gp[k] * fJa00 + gp[4 + k] * fJa10) / fJ;
+        s.face[8 + k][le][t] = (gp[k] * fJa01 + gp[4 + k] * fJa11) / fJ;
+      }
+    }
+    return;
+  }
+  const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
+  real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
+  trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
+  if (visc) {
+    trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, gox);
+    trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, goy);
+  }
+  const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
+  const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
+  const real invh = real(a.side_invh[size_t(e) * 4 + sd_]);
+  // edge viscosity (JumpsBasedEdgeViscosity): mean over the edge's elements; boundary and
+  // periodic edges have one element
+  real mu_ed = mu_e;
+  if (AV && (kind == SIDE_LEFT || kind == SIDE_RIGHT) && sd.z < 0)
+    mu_ed = (real(a.mu_av[sd.x >> 2]) + mu_e) / real(2);
+  const real mu_f = (AV && a.av == 2) ? mu + mu_ed : mu;
+  const real lap = (AV && a.av == 1) ? mu_ed * real(a.side_area[size_t(e) * 4 + sd_]) : real(0);
+  const real penalty = IP ? real(a.sigma0) * mu_f * real(P - 1) * real(P - 1) * invh : real(0);
+  real F[4], Gx[4] = {real(0), real(0), real(0), real(0)}, Gy[4] = {real(0), real(0), real(0), real(0)};
+  if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
+    const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+    real qn[4], gnx[4] = {real(0), real(0), real(0), real(0)}, gny[4] = {real(0), real(0), real(0), real(0)};
+    ld4(a.T_in + (size_t(sd.x) * P + kn) * 4, qn);
+    if (visc) {
+      const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
+      ld4(gp, gnx);
+      ld4(gp + 4, gny);
+    }
+    const bool right = kind == SIDE_RIGHT;
+    const real* QL = right ? qn : qo;
+    const real* QR = right ? qo : qn;
+    int solver = a.riemann;
+    if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
+    real Fi[4], FLx[4] = {real(0), real(0), real(0), real(0)}, FLy[4] = {real(0), real(0), real(0), real(0)};
+    real FRx[4] = {real(0), real(0), real(0), real(0)}, FRy[4] = {real(0), real(0), real(0), real(0)};
+    face_riemann(solver, ph, QL, QR, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
+    if (visc) {
+      viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
+      viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      real fv = real(0.5) * (mu_f * FLx[k] + mu_f * FRx[k]) * nx + real(0.5) * (mu_f * FLy[k] + mu_f * FRy[k]) * ny;
+      if (IP) fv = fv - penalty * (QL[k] - QR[k]);
+      if (AV) {
+        const real fa = -(lap * (QL[k] - QR[k]));
+        F[k] = (Fi[k] - fv - fa) * dS;
+      } else {
+        F[k] = (Fi[k] - fv) * dS;
+      }
+      if (right) F[k] = -F[k];
+    }
+    if (IP && a.grad_faces && visc) {
+      real fgx[4], fgy[4], Ax[4], Ay[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { fgx[k] = (QL[k] - QR[k]) * nx; fgy[k] = (QL[k] - QR[k]) * ny; }
+      viscous_flux(ph, right ? QR : QL, fgx, fgy, Ax, Ay);
+      const real cf = (right ? real(-0.5) : real(0.5)) * real(a.epsilon) * mu_f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { Gx[k] = cf * Ax[k] * dS; Gy[k] = cf * Ay[k] * dS; }
+    }
+  } else {
+    const Zone& z = a.zones[sd.z];
+    real uB[4], uSB[4];
+    const int vbc = bc_states(ph, z, qo, nx, ny, uB, uSB, sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
+    real Fi[4];
+    if (kind == SIDE_WALL) {
+      euler_wall_flux(ph, qo, nx, ny, dS, Fi);
+    } else {
+      const int solver = z.riemann >= 0 ? z.riemann : a.riemann;
+      face_riemann(solver, ph, qo, uB, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) Fi[k] = Fi[k] * dS;
+    }
+    real fv[4] = {real(0), real(0), real(0), real(0)};
+    if (vbc != VBC_NEUMANN && visc) {
+      real Fx[4], Fy[4];
+      if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, gox, goy, Fx, Fy);
+      else viscous_flux(ph, qo, gox, goy, Fx, Fy);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        fv[k] = (mu_f * Fx[k]) * nx + (mu_f * Fy[k]) * ny;
+        if (IP) fv[k] = fv[k] - penalty * (qo[k] - uSB[k]);
+        fv[k] = fv[k] * dS;
+      }
+      if (IP && a.grad_faces) {
+        real fgx[4], fgy[4], Ax[4], Ay[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { fgx[k] = (qo[k] - uSB[k]) * nx; fgy[k] = (qo[k] - uSB[k]) * ny; }
+        if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, fgx, fgy, Ax, Ay);
+        else viscous_flux(ph, qo, fgx, fgy, Ax, Ay);
+        const real cf = real(a.epsilon) * mu_f;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) { Gx[k] = (cf * Ax[k]) * dS; Gy[k] = (cf * Ay[k]) * dS; }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) F[k] = AV ? Fi[k] - fv[k] - (-(lap * (qo[k] - uSB[k]))) * dS : Fi[k] - fv[k];
+  }
+#pragma unroll
+  for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];
+  if (IP && a.grad_faces && visc) {
+    // metrics at the face node (interpolated along the other direction) and contravariant G
+    real fJa00, fJa01, fJa10, fJa11, fJ;
+    if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+    else {
+      fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
+      fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
+      fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
+      fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
+      fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      s.face[4 + k][le][t] = (Gx[k] * fJa00 + Gy[k] * fJa10) / fJ;
+      s.face[8 + k][le][t] = (Gx[k] * fJa01 + Gy[k] * fJa11) / fJ;
+    }
   }
 }
 
@@ -424,209 +646,32 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   }
   __syncthreads();
   const int i = tid % P, j = tid / P;
-  const real* hatD = s.mat;
+  const real* hatDT = s.mat;   // transposed: hatDT[l * P + i] = hatD(i, l)
   const real* lb0 = s.mat + NP;
   const real* lb1 = lb0 + P;
   const real* lbw0 = lb1 + P;
   const real* lbw1 = lbw0 + P;
   const real* dlbw0 = lbw1 + P + NP;
   const real* dlbw1 = dlbw0 + P;
-  // volume flux F = Fi - mu Fv at this node, contravariant
-  real Ja00, Ja01, Ja10, Ja11, iJ;
-  if (active) {
-    if constexpr (AFFINE) { Ja00 = geoE[0]; Ja01 = geoE[1]; Ja10 = geoE[2]; Ja11 = geoE[3]; iJ = geoE[4]; }
-    else { Ja00 = s.Ja[0][le][tid]; Ja01 = s.Ja[1][le][tid]; Ja10 = s.Ja[2][le][tid]; Ja11 = s.Ja[3][le][tid]; iJ = geoE[4]; }
-    real q[4], gx[4], gy[4], fi[4], gi[4], fv[4], gv[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) { q[k] = s.Q[k][le][tid]; gx[k] = s.dQ[0][k][le][tid]; gy[k] = s.dQ[1][k][le][tid]; }
-    inviscid_flux(ph, q, fi, gi);
-    if (visc) viscous_flux(ph, q, gx, gy, fv, gv);
-    else {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) { fv[k] = real(0); gv[k] = real(0); }
+  real iJ;
+  if (active) iJ = geoE[4];
+  // Volume fluxes and face fluxes are independent: where an element has at least a quarter of its
+  // threads beyond its 4(N+1) face nodes (N >= 5), those threads form the volume fluxes of all its nodes
+  // while the first 4(N+1) threads form the face fluxes (one barrier fewer, and no thread idles through
+  // the face phase); otherwise each thread forms its own node's volume flux, then the face fluxes.
+  constexpr bool OVERLAP = 4 * (NP - FT) >= NP;
+  if constexpr (OVERLAP) {
+    if (active) {
+      if (tid < FT) ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, tid, mu_e, visc, geoE);
+      else
+        for (int n = tid - FT; n < NP; n += NP - FT)
+          ns_volume_flux<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, n, mu_e, need_grad, visc, geoE);
     }
-    const real mu_v = (AV && a.av == 2) ? mu + mu_e : mu;
-    real ax[4] = {real(0), real(0), real(0), real(0)}, ay[4] = {real(0), real(0), real(0), real(0)};
-    if (AV && a.av == 1 && need_grad) {   // Laplacian: mu_e times the element-local gradient (ComputeInteriorGradient)
-      if (IP) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) { ax[k] = gx[k]; ay[k] = gy[k]; }
-      } else {
-        const real* D = s.mat + NP + 4 * P;   // D follows hatD, lb0, lb1, lbw0, lbw1
-        const real iJl = AFFINE ? geoE[4] : real(1) / s.Ja[4][le][tid];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          real dxi = real(0), deta = real(0);
-#pragma unroll
-          for (int l = 0; l < P; ++l) {
-            dxi += D[i * P + l] * s.Q[k][le][j * P + l];
-            deta += D[j * P + l] * s.Q[k][le][l * P + i];
-          }
-          ax[k] = (dxi * Ja00 + deta * Ja01) * iJl;
-          ay[k] = (dxi * Ja10 + deta * Ja11) * iJl;
-        }
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      real f = fi[k] - mu_v * fv[k], g = gi[k] - mu_v * gv[k];
-      if (AV && a.av == 1) { f = f - mu_e * ax[k]; g = g - mu_e * ay[k]; }
-      s.Fc[k][le][tid] = f * Ja00 + g * Ja10;
-      s.Gc[k][le][tid] = f * Ja01 + g * Ja11;
-    }
-  }
-  __syncthreads();
-  // face fluxes
-  if (active) {
-    for (int t = tid; t < FT; t += NP) {
-      const int sd_ = t / P, kk = t % P;
-      const int4 sd = a.side[size_t(e) * 4 + sd_];
-      const int kind = sd.y & 15;
-      if (kind == SIDE_FLUX) {   // inviscid and viscous flux of the mortar kernel, and its gradient-face terms
-        const real* fp = a.NF + (size_t(sd.x) * P + kk) * 4;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) s.face[k][le][t] = fp[k];
-        if (IP && a.grad_faces && visc) {
-          const real* gp = a.NFG + (size_t(sd.x) * P + kk) * 8;
-          const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
-          real fJa00, fJa01, fJa10, fJa11, fJ;
-          if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
-          else {
-            fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
-            fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
-            fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
-            fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
-            fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
-          }
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            s.face[4 + k][le][t] = (gp[k] * fJa00 + gp[4 + k] * fJa10) / fJ;
-            s.face[8 + k][le][t] = (gp[k] * fJa01 + gp[4 + k] * fJa11) / fJ;
-          }
-        }
-        continue;
-      }
-      const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
-      real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
-      trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
-      if (visc) {
-        trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, gox);
-        trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, goy);
-      }
-      const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
-      const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
-      const real invh = real(a.side_invh[size_t(e) * 4 + sd_]);
-      // edge viscosity (JumpsBasedEdgeViscosity): mean over the edge's elements; boundary and
-      // periodic edges have one element
-      real mu_ed = mu_e;
-      if (AV && (kind == SIDE_LEFT || kind == SIDE_RIGHT) && sd.z < 0)
-        mu_ed = (real(a.mu_av[sd.x >> 2]) + mu_e) / real(2);
-      const real mu_f = (AV && a.av == 2) ? mu + mu_ed : mu;
-      const real lap = (AV && a.av == 1) ? mu_ed * real(a.side_area[size_t(e) * 4 + sd_]) : real(0);
-      const real penalty = IP ? real(a.sigma0) * mu_f * real(P - 1) * real(P - 1) * invh : real(0);
-      real F[4], Gx[4] = {real(0), real(0), real(0), real(0)}, Gy[4] = {real(0), real(0), real(0), real(0)};
-      if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
-        const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
-        const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
-        real qn[4], gnx[4] = {real(0), real(0), real(0), real(0)}, gny[4] = {real(0), real(0), real(0), real(0)};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) qn[k] = tp[k];
-        if (visc) {
-          const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) { gnx[k] = gp[k]; gny[k] = gp[4 + k]; }
-        }
-        const bool right = kind == SIDE_RIGHT;
-        const real* QL = right ? qn : qo;
-        const real* QR = right ? qo : qn;
-        int solver = a.riemann;
-        if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
-        real Fi[4], FLx[4] = {real(0), real(0), real(0), real(0)}, FLy[4] = {real(0), real(0), real(0), real(0)};
-        real FRx[4] = {real(0), real(0), real(0), real(0)}, FRy[4] = {real(0), real(0), real(0), real(0)};
-        face_riemann(solver, ph, QL, QR, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
-        if (visc) {
-          viscous_flux(ph, QL, right ? gnx : gox, right ? gny : goy, FLx, FLy);
-          viscous_flux(ph, QR, right ? gox : gnx, right ? goy : gny, FRx, FRy);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          real fv = real(0.5) * (mu_f * FLx[k] + mu_f * FRx[k]) * nx + real(0.5) * (mu_f * FLy[k] + mu_f * FRy[k]) * ny;
-          if (IP) fv = fv - penalty * (QL[k] - QR[k]);
-          if (AV) {
-            const real fa = -(lap * (QL[k] - QR[k]));
-            F[k] = (Fi[k] - fv - fa) * dS;
-          } else {
-            F[k] = (Fi[k] - fv) * dS;
-          }
-          if (right) F[k] = -F[k];
-        }
-        if (IP && a.grad_faces && visc) {
-          real fgx[4], fgy[4], Ax[4], Ay[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) { fgx[k] = (QL[k] - QR[k]) * nx; fgy[k] = (QL[k] - QR[k]) * ny; }
-          viscous_flux(ph, right ? QR : QL, fgx, fgy, Ax, Ay);
-          const real cf = (right ? real(-0.5) : real(0.5)) * real(a.epsilon) * mu_f;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) { Gx[k] = cf * Ax[k] * dS; Gy[k] = cf * Ay[k] * dS; }
-        }
-      } else {
-        const Zone& z = a.zones[sd.z];
-        real uB[4], uSB[4];
-        const int vbc = bc_states(ph, z, qo, nx, ny, uB, uSB, sd.w >= 0 ? a.bq + (size_t(sd.w) * P + kk) * 4 : nullptr);
-        real Fi[4];
-        if (kind == SIDE_WALL) {
-          euler_wall_flux(ph, qo, nx, ny, dS, Fi);
-        } else {
-          const int solver = z.riemann >= 0 ? z.riemann : a.riemann;
-          face_riemann(solver, ph, qo, uB, nx, ny, a.FX, (size_t(e) * 4 + sd_) * P + kk, Fi);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) Fi[k] = Fi[k] * dS;
-        }
-        real fv[4] = {real(0), real(0), real(0), real(0)};
-        if (vbc != VBC_NEUMANN && visc) {
-          real Fx[4], Fy[4];
-          if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, gox, goy, Fx, Fy);
-          else viscous_flux(ph, qo, gox, goy, Fx, Fy);
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            fv[k] = (mu_f * Fx[k]) * nx + (mu_f * Fy[k]) * ny;
-            if (IP) fv[k] = fv[k] - penalty * (qo[k] - uSB[k]);
-            fv[k] = fv[k] * dS;
-          }
-          if (IP && a.grad_faces) {
-            real fgx[4], fgy[4], Ax[4], Ay[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) { fgx[k] = (qo[k] - uSB[k]) * nx; fgy[k] = (qo[k] - uSB[k]) * ny; }
-            if (vbc == VBC_ADIABATIC) viscous_flux_adiabatic(ph, qo, qo, fgx, fgy, Ax, Ay);
-            else viscous_flux(ph, qo, fgx, fgy, Ax, Ay);
-            const real cf = real(a.epsilon) * mu_f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) { Gx[k] = (cf * Ax[k]) * dS; Gy[k] = (cf * Ay[k]) * dS; }
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) F[k] = AV ? Fi[k] - fv[k] - (-(lap * (qo[k] - uSB[k]))) * dS : Fi[k] - fv[k];
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];
-      if (IP && a.grad_faces && visc) {
-        // metrics at the face node (interpolated along the other direction) and contravariant G
-        real fJa00, fJa01, fJa10, fJa11, fJ;
-        if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
-        else {
-          fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
-          fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
-          fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
-          fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
-          fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          s.face[4 + k][le][t] = (Gx[k] * fJa00 + Gy[k] * fJa10) / fJ;
-          s.face[8 + k][le][t] = (Gx[k] * fJa01 + Gy[k] * fJa11) / fJ;
-        }
-      }
-    }
+  } else {
+    if (active) ns_volume_flux<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, tid, mu_e, need_grad, visc, geoE);
+    __syncthreads();
+    if (active)
+      for (int t = tid; t < FT; t += NP) ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, t, mu_e, visc, geoE);
   }
   __syncthreads();
   // The gradient-face terms enter the lift as hatD-contractions along their side, which depend on the
@@ -641,7 +686,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       for (int k = 0; k < 4; ++k) {
         real d = real(0);
 #pragma unroll
-        for (int l = 0; l < P; ++l) d += hatD[kk * P + l] * s.face[row + k][le][sd_ * P + l];
+        for (int l = 0; l < P; ++l) d += hatDT[l * P + kk] * s.face[row + k][le][sd_ * P + l];
         s.gfd[k][le][t] = d;
       }
     }
@@ -650,7 +695,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   if (active) {
 #pragma unroll
     for (int l = 0; l < P; ++l) {
-      const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+      const real hi = hatDT[l * P + i], hj = hatDT[l * P + j];
 #pragma unroll
       for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s.Fc[k][le][j * P + l] + hj * s.Gc[k][le][l * P + i];
     }
@@ -683,10 +728,16 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     }
     if (a.update) {
       real gn[4];
+      if (a.first) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) gn[k] = a.first ? real(a.b) * qd[k] : real(a.a) * a.G[off + k] + real(a.b) * qd[k];
+        for (int k = 0; k < 4; ++k) gn[k] = real(a.b) * qd[k];
+      } else {
+        real go[4];
+        ld4(a.G + off, go);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) a.G[off + k] = gn[k];
+        for (int k = 0; k < 4; ++k) gn[k] = real(a.a) * go[k] + real(a.b) * qd[k];
+      }
+      st4(a.G + off, gn);
       double2* qp = reinterpret_cast<double2*>(a.Q + off);
       double2 q01 = qp[0], q23 = qp[1];
       q01.x = q01.x + a.c * double(gn[0]);
@@ -721,11 +772,9 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     for (int t = tid; t < FT; t += NP) {
       const int sd_ = t / P, kk = t % P;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
-      real* tp = a.T_out + ((size_t(e) * 4 + sd_) * P + kk) * 4;
       real tr[4];
       trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, tr);
-#pragma unroll
-      for (int k = 0; k < 4; ++k) tp[k] = tr[k];
+      st4(a.T_out + ((size_t(e) * 4 + sd_) * P + kk) * 4, tr);
     }
   }
   if constexpr (IP) {
@@ -746,8 +795,8 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
             real tx[4], ty[4];
             trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, tx);
             trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, ty);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) { gp[k] = tx[k]; gp[4 + k] = ty[k]; }
+            st4(gp, tx);
+            st4(gp + 4, ty);
           }
         }
       }

@@ -73,6 +73,24 @@ __host__ __device__ constexpr int epb_stage(int P, int variant) { return variant
 __host__ __device__ constexpr int block_of(int P, int EPB) { return ((P * P * EPB + 31) / 32) * 32; }
 __host__ __device__ constexpr int block_for(int P) { return block_of(P, epb_for(P)); }
 
+// Four consecutive values of a record that starts at a multiple of 4 values from a cudaMalloc'd base
+// (16-byte aligned in float, 32-byte in double): one 128-bit access in float, two in double.
+__device__ __forceinline__ void ld4(const float* p, float* o) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+__device__ __forceinline__ void ld4(const double* p, double* o) {
+  const double2 a = reinterpret_cast<const double2*>(p)[0], b = reinterpret_cast<const double2*>(p)[1];
+  o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+}
+__device__ __forceinline__ void st4(float* p, const float* v) {
+  *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st4(double* p, const double* v) {
+  reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
+}
+
 // max that keeps NaN (a residual that is NaN must stay visible)
 __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
 
@@ -103,6 +121,16 @@ __device__ __forceinline__ void check_state(int* health, int* health_host, doubl
 __host__ __device__ constexpr int face_node(int P, int side, int l, int kk) {
   return (side == 0 || side == 2) ? (l * P + kk) : (kk * P + l);
 }
+// Order of the P terms of a trace at face node kk: step m takes line node l = (m + kk) mod P.  The face
+// nodes of a side sit in consecutive lanes; without the rotation the lanes of a right or left side (a
+// column of the tile) would read one column at a time, P words apart, into the same banks.  Every Q
+// trace of a state (stage, gradient and trace kernels) sums in this order, so an element's own trace and
+// the copy its neighbour reads stay equal bit for bit.
+__host__ __device__ constexpr int trace_l(int P, int m, int kk) { return (m + kk) % P; }
+// The rotation is used in double, where a column side's lanes collide 4 ways; in float they collide 2
+// ways and the rotated (runtime) addressing costs more registers than the conflicts cost time.
+template <typename real>
+__host__ __device__ constexpr int trace_step(int P, int m, int kk) { return sizeof(real) == 8 ? trace_l(P, m, kk) : m; }
 
 template <int P, int EPB, typename real, bool AFFINE, bool LGL>
 __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real> a) {
@@ -119,7 +147,8 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
   const int flat = threadIdx.x;
   const int le = flat / NP;               // element in block
   const int tid = flat - le * NP;         // node in element
-  for (int k = flat; k < NP + 4 * P; k += blockDim.x) s_mat[k] = real(a.mats[k]);
+  // hatD held transposed (column l contiguous): conflict-free reads of hatD(i, l) across a warp's nodes
+  for (int k = flat; k < NP + 4 * P; k += blockDim.x) s_mat[k] = real(a.mats[k < NP ? (k % P) * P + k / P : k]);
   const int e = blockIdx.x * EPB + le;
   const bool active = le < EPB && e < a.n_el;
   Phys<real> ph;
@@ -145,7 +174,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
     }
   }
   __syncthreads();
-  const real* hatD = s_mat;
+  const real* hatDT = s_mat;   // transposed: hatDT[l * P + i] = hatD(i, l)
   const real* lb0 = s_mat + NP;
   const real* lb1 = lb0 + P;
   const real* lbw0 = lb1 + P;
@@ -158,7 +187,8 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
       const int4 sd = a.side[size_t(e) * 4 + s];
       const int kind = sd.y & 15;
       if (kind == SIDE_FLUX) {
-        const real* fp = a.NF + (size_t(sd.x) * P + kk) * 4;
+        real fp[4];
+        ld4(a.NF + (size_t(sd.x) * P + kk) * 4, fp);
 #pragma unroll
         for (int k = 0; k < 4; ++k) s_F[k][le][t] = fp[k];
         continue;
@@ -171,7 +201,8 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
         for (int k = 0; k < 4; ++k) qo[k] = s_Q[k][le][node];
       } else {
 #pragma unroll
-        for (int l = 0; l < P; ++l) {
+        for (int m = 0; m < P; ++m) {
+          const int l = trace_step<real>(P, m, kk);
           const int node = face_node(P, s, l, kk);
 #pragma unroll
           for (int k = 0; k < 4; ++k) qo[k] += s_Q[k][le][node] * lbv[l];
@@ -192,9 +223,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
           if (z.riemann >= 0) solver = z.riemann;
         } else {
           const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
-          const real* tp = a.T_in + (size_t(sd.x) * P + kn) * 4;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) qn[k] = tp[k];
+          ld4(a.T_in + (size_t(sd.x) * P + kn) * 4, qn);
           if (sd.z >= 0) { const int zr = a.zones[sd.z].riemann; if (zr >= 0) solver = zr; }
         }
         if (kind == SIDE_RIGHT) {
@@ -217,7 +246,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
   if (active) {
 #pragma unroll
     for (int l = 0; l < P; ++l) {
-      const real hi = hatD[i * P + l], hj = hatD[j * P + l];
+      const real hi = hatDT[l * P + i], hj = hatDT[l * P + j];
 #pragma unroll
       for (int k = 0; k < 4; ++k) qd[k] = qd[k] + hi * s_Fc[k][le][j * P + l] + hj * s_Gc[k][le][l * P + i];
     }
@@ -248,11 +277,12 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
 #pragma unroll
         for (int k = 0; k < 4; ++k) gn[k] = real(a.b) * qd[k];
       } else {
+        real go[4];
+        ld4(a.G + off, go);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) gn[k] = real(a.a) * a.G[off + k] + real(a.b) * qd[k];
+        for (int k = 0; k < 4; ++k) gn[k] = real(a.a) * go[k] + real(a.b) * qd[k];
       }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) a.G[off + k] = gn[k];
+      st4(a.G + off, gn);
       double2* qp = reinterpret_cast<double2*>(a.Q + off);
       double2 q01 = qp[0], q23 = qp[1];
       q01.x = q01.x + a.c * double(gn[0]);
@@ -296,15 +326,14 @@ __global__ void __launch_bounds__(block_of(P, EPB)) stage_kernel(StageArgs<real>
         for (int k = 0; k < 4; ++k) tr[k] = s_Q[k][le][node];
       } else {
 #pragma unroll
-        for (int l = 0; l < P; ++l) {
+        for (int m = 0; m < P; ++m) {
+          const int l = trace_step<real>(P, m, kk);
           const int node = face_node(P, s, l, kk);
 #pragma unroll
           for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
         }
       }
-      real* tp = a.T_out + ((size_t(e) * 4 + s) * P + kk) * 4;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) tp[k] = tr[k];
+      st4(a.T_out + ((size_t(e) * 4 + s) * P + kk) * 4, tr);
     }
   }
 }
@@ -330,8 +359,9 @@ __global__ void __launch_bounds__(block_for(P)) trace_kernel(int n_el, const dou
     const int s = t / P, kk = t % P;
     const real* lbv = (s == 0 || s == 3) ? s_lb : s_lb + P;
     real tr[4] = {real(0), real(0), real(0), real(0)};
-    for (int l = 0; l < P; ++l) {
-      const int node = (s == 0 || s == 2) ? (l * P + kk) : (kk * P + l);
+    for (int m = 0; m < P; ++m) {
+      const int l = trace_step<real>(P, m, kk);
+      const int node = face_node(P, s, l, kk);
 #pragma unroll
       for (int k = 0; k < 4; ++k) tr[k] += s_Q[k][le][node] * lbv[l];
     }

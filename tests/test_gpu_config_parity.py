@@ -136,9 +136,15 @@ def kh_sample(n=128, precision=hg.PREC_FP64):
 
 
 def test_c5_sample_sipg_modal():
+    """The shear layer is an exact steady solution of the Euler equations: its residual is some 500 times
+    smaller than a generic state's (cancellation), so the per-residual check runs on the state with a
+    1e-3 perturbation, and the steps from the configuration's own state."""
     orc, g, Q, dt = kh_sample()
-    r_stage, r_steps = residual_and_steps(orc, g, Q, dt, 10)
-    assert r_stage <= TOL_STAGE
+    Qp = perturbed(Q, 1e-3, seed=SEED)
+    orc.set_state(Qp)
+    g.set_state(Qp)
+    assert rel_l2(g.compute_time_derivative(0.0), orc.time_derivative(0.0)) <= TOL_STAGE
+    _, r_steps = residual_and_steps(orc, g, Q, dt, 10)
     assert r_steps <= TOL_STEPS
     orc32, g32, _, _ = kh_sample(precision=hg.PREC_FP32)
     g32.set_state(Q)

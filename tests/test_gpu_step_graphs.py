@@ -65,6 +65,7 @@ def test_boundary_states_between_steps_reach_the_replayed_graphs():
     b.profile(True)            # timing mode: plain launches only
     for g in (a, b):
         g.set_state(Q)
+    orc.set_state(Q)
     dt = orc.estimate_dt(0.2, 1.0)
     t = 0.0
     for k in range(12):
