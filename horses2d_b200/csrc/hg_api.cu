@@ -56,7 +56,7 @@ void ctx_free(hg_ctx* c) {
                   c->d_QDot, c->d_resid, c->d_resid_out, c->d_elmax, c->d_side_invh, c->d_jac, c->d_GT[0],
                   c->d_GT[1], c->d_av_el, c->d_side_area, c->d_mu_av[0], c->d_mu_av[1], c->d_mlp, c->d_feat_lo,
                   c->d_feat_hi, c->d_dQ,
-                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG, c->d_exact_sides};
+                  c->d_FX, c->d_bq, c->d_si_out, c->d_NF, c->d_NFG, c->d_NJ, c->d_exact_sides};
   for (int* p : c->d_zone_sides) if (p) cudaFree(p);
   for (void* p : ptrs) if (p) cudaFree(p);
   if (!c->health_shared) {
@@ -208,6 +208,7 @@ static void run_ns_stage(hg_ctx* c, double ca, double cb, double cc, bool first,
   a.FX = static_cast<const real*>(c->d_FX);
   a.NF = static_cast<const real*>(c->d_NF);
   a.NFG = static_cast<const real*>(c->d_NFG);
+  a.NJ = static_cast<const real*>(c->d_NJ);
   a.Q = c->d_Q;
   a.G = static_cast<real*>(c->d_G);
   a.T_in = static_cast<const real*>(c->d_T[c->cur]);
@@ -308,6 +309,7 @@ void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool upda
     };
     if (c->ns) {
       if (!c->ip) launch_mortar(c, MORTAR_GRADIENT);   // the interior-penalty gradient is element-local
+      if (c->av != HG_AV_NONE) launch_mortar(c, MORTAR_JUMPS);   // jumps of the faces between parts
       parts_stage(1);
       launch_mortar(c, MORTAR_FLUX);
       parts_stage(2);
@@ -1204,6 +1206,19 @@ extern "C" int hg_sensor_eval(hg_ctx* c, float* features, double* out) {
 
 extern "C" int hg_element_viscosity(hg_ctx* c, double* mu) {
   try {
+    if (is_composite(c)) {   // each part's elements, back in mesh order
+      if (c->av == HG_AV_NONE) throw std::runtime_error("artificial dissipation is off for this context");
+      std::vector<std::vector<double>> pm(c->parts.size());
+      for (size_t p = 0; p < c->parts.size(); ++p) {
+        hg_ctx* q = c->parts[p];
+        pm[p].resize(size_t(q->n_el));
+        HG_CUDA(cudaMemcpyAsync(pm[p].data(), q->d_mu_av[q->mu_last], pm[p].size() * sizeof(double),
+                                cudaMemcpyDeviceToHost, c->stream));
+      }
+      HG_CUDA(cudaStreamSynchronize(c->stream));
+      for (int e = 0; e < c->n_el; ++e) mu[e] = pm[c->el_part[e]][c->el_local[e]];
+      return 0;
+    }
     if (!c->d_mu_av[0]) throw std::runtime_error("artificial dissipation is off for this context");
     HG_CUDA(cudaMemcpyAsync(mu, c->d_mu_av[c->mu_last], size_t(c->n_el) * sizeof(double), cudaMemcpyDeviceToHost,
                             c->stream));

@@ -67,6 +67,7 @@ struct hg_ctx {
   int n_exact_sides = 0;
   void* d_NF = nullptr;           // mortar fluxes of the SIDE_FLUX sides [slots][P][4], context precision
   void* d_NFG = nullptr;          // mortar BR1 gradient face terms of the SIDE_FLUX sides [slots][P][2][4]
+  void* d_NJ = nullptr;           // mortar jump sums of the SIDE_FLUX sides [slots][2] (rho, rhoE; dissipation)
   int ns_phase = 0;               // a composite's Navier-Stokes part: 0 whole stage, 1 gradient kernel, 2 stage kernel
   // Mixed orders and subdivided edges: the context is a composite of one part per polynomial order
   // (each an ordinary context over its elements, on this context's stream); the faces between parts
@@ -187,7 +188,7 @@ void ctx_free(hg_ctx* c);
 void ctx_stage(hg_ctx* c, double ca, double cb, double cc, bool first, bool update, double* qdot, bool resid);
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs);
 void composite_free(hg_ctx* c);
-enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1, MORTAR_FLUX_IP = 2 };
+enum { MORTAR_FLUX = 0, MORTAR_GRADIENT = 1, MORTAR_FLUX_IP = 2, MORTAR_JUMPS = 3 };
 void launch_mortar(hg_ctx* c, int mode);
 inline bool is_composite(const hg_ctx* c) { return !c->parts.empty(); }
 // Interior penalty with an element-local indicator (none, modal, learned) on a single-order context:

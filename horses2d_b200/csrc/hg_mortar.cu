@@ -31,12 +31,14 @@ namespace {
 // offsets into the matrix pool, row-major [rows][cols].
 struct MortarFace {
   double invh;    // interior penalty: Area / min(volume) of the face's elements
+  double area;    // the edge's Area (artificial dissipation's Laplacian face term)
   int kind;
   int part[3], el[3], side[3], slot[3], P[3];
   int PE[2];      // edge nodes (kind 0), or north and south half nodes (kind 1)
   int inv;        // kind 0: RIGHT traverses the edge backwards
   int tf[4], tb[4];
   int geo[2];     // rows {nx, ny, dS} of the edge (kind 0) or of the north and south halves (kind 1)
+  int wq[2];      // offsets of the edge's (halves') quadrature weights in the matrix pool (jumps)
 };
 
 template <typename real>
@@ -49,7 +51,10 @@ struct MortarArgs {
   const real* GT[HG_MAX_PARTS];    // gradient traces (Navier-Stokes)
   real* NF[HG_MAX_PARTS];          // MORTAR_FLUX output
   real* NFG[HG_MAX_PARTS];         // MORTAR_GRADIENT output
-  int mode;                        // MORTAR_FLUX, MORTAR_FLUX_IP or MORTAR_GRADIENT
+  real* NJ[HG_MAX_PARTS];          // MORTAR_JUMPS output: per side slot {rho, rhoE} jump sums of its face
+  const double* mu[HG_MAX_PARTS];  // element artificial viscosity of the parts' current state
+  int av;                          // artificial dissipation HG_AV_* (fluxes: edge viscosity terms)
+  int mode;                        // MORTAR_FLUX, MORTAR_FLUX_IP, MORTAR_GRADIENT or MORTAR_JUMPS
   int visc;                        // fluxes: add the viscous flux (BR1 average; IP adds the penalty)
   int grad_faces;                  // MORTAR_FLUX_IP: SIPG / NIPG gradient-face terms
   double sigma0, epsilon;          // interior penalty parameter and the method's epsilon (-1, 1, 0)
@@ -89,7 +94,7 @@ __device__ __forceinline__ void project_row(const real* mat, int m, int cols, in
 template <int MODE, typename real>
 __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys<real>& ph, const real* qL,
                                            const real* qR, const real* dL, const real* dR, const real* g,
-                                           real penalty, real* out) {
+                                           real penalty, real mu_ed, real area, real* out) {
   if constexpr (MODE == MORTAR_GRADIENT) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -101,7 +106,10 @@ __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys
     real F[4];
     if (a.riemann == RIEMANN_EXACT) exact(ph, qL, qR, g[0], g[1], F);
     else riemann(a.riemann, ph, qL, qR, g[0], g[1], F);
-    const real mu = real(a.pc.mu);
+    // the edge's viscosity: Physical dissipation adds the edge viscosity to mu in the viscous flux and the
+    // penalty (penalty arrives with mu + mu_ed); Laplacian adds -mu_ed Area (qL - qR)
+    // (DGArtificialDissipation.f90:208-249, JumpsBasedEdgeViscosity)
+    const real mu = a.av == HG_AV_PHYSICAL ? real(a.pc.mu) + mu_ed : real(a.pc.mu);
     if (a.visc) {
       real FLx[4], FLy[4], FRx[4], FRy[4];
       viscous_flux(ph, qL, dL, dL + 4, FLx, FLy);
@@ -112,6 +120,10 @@ __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys
         if (MODE == MORTAR_FLUX_IP) fv = fv - penalty * (qL[k] - qR[k]);
         F[k] = F[k] - fv;
       }
+    }
+    if (a.av == HG_AV_LAPLACIAN) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) F[k] = F[k] - (-(mu_ed * area * (qL[k] - qR[k])));
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) out[k] = F[k] * g[2];
@@ -136,7 +148,7 @@ __device__ __forceinline__ void node_value(const MortarArgs<real>& a, const Phys
 
 template <typename real, int MODE>
 __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
-  constexpr int NC = MODE == MORTAR_GRADIENT ? 8 : (MODE == MORTAR_FLUX_IP ? 20 : 4);   // values per edge node
+  constexpr int NC = MODE == MORTAR_GRADIENT ? 8 : (MODE == MORTAR_FLUX_IP ? 20 : (MODE == MORTAR_JUMPS ? 2 : 4));
   __shared__ real sT[MW][3][MP][4];   // Q traces of the face's element sides
   __shared__ real sG[MW][3][MP][8];   // their gradient traces (x then y), viscous fluxes only
   __shared__ real sF[MW][2][MP][NC];  // values at the edge (half) nodes
@@ -145,7 +157,7 @@ __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
   if (fi >= a.n) return;   // whole warps leave together; the kernel synchronises warps only
   const MortarFace& f = a.f[fi];
   const int ns = f.kind == 0 ? 2 : 3;
-  const bool grads = MODE != MORTAR_GRADIENT && a.visc;
+  const bool grads = MODE != MORTAR_GRADIENT && MODE != MORTAR_JUMPS && a.visc;
   for (int t = lane; t < ns * MP; t += 32) {
     const int s = t / MP, k = t % MP;
     if (k < f.P[s]) {
@@ -181,14 +193,51 @@ __global__ void __launch_bounds__(MW * 32) mortar_kernel(MortarArgs<real> a) {
         project_row<8, 8>(a.mat, mL, f.P[0], i, &sG[w][0][0][0], dL);
         project_row<8, 8>(a.mat, mR, f.P[sR], rR, &sG[w][sR][0][0], dR);
       }
-      // penalty sigma0 mu N^2 invh at the edge's (half edge's) order
-      const real penalty = real(a.sigma0 * a.pc.mu * double(PE - 1) * double(PE - 1) * f.invh);
-      node_value<MODE>(a, ph, qL, qR, dL, dR, a.geo + size_t(f.geo[h] + i) * 3, penalty, v);
+      const real* g = a.geo + size_t(f.geo[h] + i) * 3;
+      if constexpr (MODE == MORTAR_JUMPS) {
+        // Edge_ComputeJumps at edge node i: w (2 (qL - qR) / (qL + qR))^2 dS for rho and rhoE
+        // (Mesh/QuadElement_EdgeProcedures.incf:1348-1394; subdivided edges: each half at its own nodes)
+        const real wi = a.mat[f.wq[h] + i];
+        const real jr = real(2) * (qL[0] - qR[0]) / (qL[0] + qR[0]);
+        const real je = real(2) * (qL[3] - qR[3]) / (qL[3] + qR[3]);
+        sF[w][h][i][0] = wi * jr * jr * g[2];
+        sF[w][h][i][1] = wi * je * je * g[2];
+      } else {
+        // the edge viscosity (JumpsBasedEdgeViscosity): the mean over the face's elements
+        double mu_ed = 0.0;
+        if (a.av != HG_AV_NONE) {
+          const double mL = a.mu[f.part[0]][f.el[0]], m1 = a.mu[f.part[1]][f.el[1]];
+          mu_ed = f.kind == 0 ? (m1 + mL) / 2.0 : ((m1 + mL) + a.mu[f.part[2]][f.el[2]]) / 3.0;
+        }
+        // penalty sigma0 (mu + mu_a) N^2 invh at the edge's (half edge's) order
+        const double mu_p = a.pc.mu + (a.av == HG_AV_PHYSICAL ? mu_ed : 0.0);
+        const real penalty = real(a.sigma0 * mu_p * double(PE - 1) * double(PE - 1) * f.invh);
+        node_value<MODE>(a, ph, qL, qR, dL, dR, g, penalty, real(mu_ed), real(f.area), v);
 #pragma unroll
-      for (int k = 0; k < NC; ++k) sF[w][h][i][k] = v[k];
+        for (int k = 0; k < NC; ++k) sF[w][h][i][k] = v[k];
+      }
     }
   }
   __syncwarp();
+  if constexpr (MODE == MORTAR_JUMPS) {
+    // the face's jump sums, in the edge's node order (north half, then south half): every element side
+    // of the face takes the whole edge's value, as each element sums the jumps of its four edges
+    if (lane == 0) {
+      real sr = real(0), se = real(0);
+      for (int hh = 0; hh < (f.kind == 0 ? 1 : 2); ++hh) {
+        real hr = real(0), he = real(0);
+        for (int i = 0; i < f.PE[hh]; ++i) { hr = hr + sF[w][hh][i][0]; he = he + sF[w][hh][i][1]; }
+        sr = sr + hr;
+        se = se + he;
+      }
+      for (int s = 0; s < ns; ++s) {
+        real* jp = a.NJ[f.part[s]] + size_t(f.slot[s]) * 2;
+        jp[0] = sr;
+        jp[1] = se;
+      }
+    }
+    return;
+  }
   // back to the elements: LEFT + Tb F (both halves of a subdivided edge), RIGHT - Tb F in its own order;
   // MORTAR_FLUX_IP: also the gradient-face terms, LEFT's from values 4-11, RIGHT's from 12-19 (no sign)
   auto store = [&](int s, int i, const real* v, real sign) {
@@ -322,10 +371,13 @@ void launch_mortar(hg_ctx* c, int mode) {
       a.GT[p] = static_cast<const real*>(q->d_GT[q->cur]);
       a.NF[p] = static_cast<real*>(q->d_NF);
       a.NFG[p] = static_cast<real*>(q->d_NFG);
+      a.NJ[p] = static_cast<real*>(q->d_NJ);
+      a.mu[p] = q->d_mu_av[q->cur];   // the parts' gradient kernels of this stage wrote it (jumps indicator)
     }
     if (mode == MORTAR_FLUX && c->ns && c->ip) mode = MORTAR_FLUX_IP;
     a.mode = mode;
-    a.visc = c->ns && c->pc.mu != 0.0;
+    a.av = c->av;
+    a.visc = c->ns && (c->pc.mu != 0.0 || c->av == HG_AV_PHYSICAL);
     a.grad_faces = c->grad_faces ? 1 : 0;
     a.sigma0 = c->sigma0;
     a.epsilon = c->epsilon;
@@ -334,6 +386,7 @@ void launch_mortar(hg_ctx* c, int mode) {
     timed(c, HG_KERNEL_MORTAR, [&] {
       if (mode == MORTAR_GRADIENT) mortar_kernel<real, MORTAR_GRADIENT><<<grid, MW * 32, 0, c->stream>>>(a);
       else if (mode == MORTAR_FLUX_IP) mortar_kernel<real, MORTAR_FLUX_IP><<<grid, MW * 32, 0, c->stream>>>(a);
+      else if (mode == MORTAR_JUMPS) mortar_kernel<real, MORTAR_JUMPS><<<grid, MW * 32, 0, c->stream>>>(a);
       else mortar_kernel<real, MORTAR_FLUX><<<grid, MW * 32, 0, c->stream>>>(a);
     });
   };
@@ -354,9 +407,9 @@ void composite_free(hg_ctx* c) {
 }
 
 void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph, const hg_bc_desc* bcs, int n_bcs) {
-  if (ph->navier_stokes && ph->av_type != HG_AV_NONE)
-    throw std::runtime_error("mixed orders and subdivided edges in the Navier-Stokes build take no "
-                             "artificial dissipation");
+  if (ph->av_type < HG_AV_NONE || ph->av_type > HG_AV_PHYSICAL) throw std::runtime_error("unknown artificial dissipation type");
+  if (ph->navier_stokes && ph->av_type != HG_AV_NONE && !m->volume)
+    throw std::runtime_error("artificial dissipation needs element volumes");
   const int E = m->n_elements;
   if (E <= 0) throw std::runtime_error("mesh has no elements");
   c->el_N.assign(m->N, m->N + E);
@@ -395,7 +448,8 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
   c->P = c->N + 1;
   c->node_type = ph->node_type;
   c->riemann = ph->riemann;
-  c->ns = ph->navier_stokes != 0 && ph->reynolds != 0.0;
+  c->av = ph->navier_stokes ? ph->av_type : HG_AV_NONE;
+  c->ns = ph->navier_stokes != 0 && (ph->reynolds != 0.0 || c->av != HG_AV_NONE);
   c->ip = ph->viscous == 1;
   c->grad_faces = c->ip && ph->ip_method != 2;
   c->sigma0 = ph->sigma0_ip;
@@ -450,6 +504,18 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
   // mortar faces, their projection matrices and geometry; SIDE_FLUX slots per part
   MatPool pool;
   pool.node_type = ph->node_type;
+  // Area of every edge, sum_p dS(p) w(p) at the edge's order (QuadMesh_Construct.incf:270-303), and per
+  // element side (the artificial dissipation's indicator and Laplacian face term)
+  std::vector<double> edge_area(F, 0.0), side_area_mesh(size_t(E) * 4, 0.0);
+  for (int f = 0; f < F; ++f) {
+    const int NE = int(enode[f + 1] - enode[f]) - 1;
+    const std::vector<double>& w = pool.op(NE).w;
+    double A = 0.0;
+    for (int p = 0; p <= NE; ++p) A += m->edge_dS[enode[f] + p] * w[p];
+    edge_area[f] = A;
+    side_area_mesh[size_t(m->edge_elem[2 * f]) * 4 + m->edge_side[2 * f] - 1] = A;
+    if (m->edge_marker[f] == 0) side_area_mesh[size_t(m->edge_elem[2 * f + 1]) * 4 + m->edge_side[2 * f + 1] - 1] = A;
+  }
   std::vector<double> geo;
   std::vector<MortarFace> faces;
   std::vector<std::vector<int2>> flux_sides(NPART);
@@ -497,6 +563,9 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
       geo.push_back(m->edge_n[2 * n + 1]);
       geo.push_back(m->edge_dS[n]);
     }
+    mf.wq[0] = pool.add(pool.op(NE).w);
+    mf.wq[1] = 0;
+    mf.area = edge_area[f];
     faces.push_back(mf);
   }
   int64_t mnode = 0;
@@ -540,6 +609,27 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
       geo.push_back(m->mortar_n[2 * mnode]);
       geo.push_back(m->mortar_n[2 * mnode + 1]);
       geo.push_back(m->mortar_dS[mnode]);
+    }
+    mf.wq[0] = pool.add(pool.op(NN).w);
+    mf.wq[1] = pool.add(pool.op(NS).w);
+    // Area of the whole edge, sum_p dS(p) w(p) at the LEFT element's order (QuadMesh_Construct.incf:
+    // 270-303): a straight edge's dS is twice each half's; a curved one's is recovered from
+    // invh = Area / min(volumes) (to rounding)
+    {
+      const double* dN = &geo[size_t(mf.geo[0]) * 3];
+      const double* dSo = &geo[size_t(mf.geo[1]) * 3];
+      bool straight = dN[2] == dSo[2];
+      for (int p = 0; p < NN + 1 && straight; ++p) straight = dN[3 * p + 2] == dN[2];
+      for (int p = 0; p < NS + 1 && straight; ++p) straight = dSo[3 * p + 2] == dN[2];
+      double A = 0.0;
+      if (straight) {
+        const std::vector<double>& wL = pool.op(NL).w;
+        for (int p = 0; p < NL + 1; ++p) A += (2.0 * dN[2]) * wL[p];
+      } else if (m->volume) {
+        A = mf.invh * std::min({m->volume[el[0]], m->volume[el[1]], m->volume[el[2]]});
+      }
+      mf.area = A;
+      for (int k = 0; k < 3; ++k) side_area_mesh[size_t(el[k]) * 4 + sd[k] - 1] = A;
     }
     faces.push_back(mf);
   }
@@ -614,6 +704,23 @@ void composite_build(hg_ctx* c, const hg_mesh_desc* m, const hg_physics_desc* ph
     if (c->ns) {
       pc->d_NFG = dalloc_n<char>(flux_sides[p].size() * Pp * 8 * rs);
       HG_CUDA(cudaMemset(pc->d_NFG, 0, std::max<size_t>(flux_sides[p].size() * Pp * 8 * rs, 1)));
+    }
+    if (c->av != HG_AV_NONE) {
+      pc->d_NJ = dalloc_n<char>(flux_sides[p].size() * 2 * rs);
+      HG_CUDA(cudaMemset(pc->d_NJ, 0, std::max<size_t>(flux_sides[p].size() * 2 * rs, 1)));
+      // the jumps indicator divides by the element's four edge Areas: the part built them from its own
+      // (conforming) edges only, so they are replaced by the whole mesh's, edges between orders and
+      // subdivided edges included (JumpsBasedElementViscosity, DGArtificialDissipation.f90:277-338)
+      std::vector<double> avel(size_t(Ep) * 2), sarea(size_t(Ep) * 4);
+      for (int k = 0; k < Ep; ++k) {
+        const int e = els[k];
+        const double* A = &side_area_mesh[size_t(e) * 4];
+        avel[2 * size_t(k)] = ph->av_intensity * (std::sqrt(m->volume[e]) / (Np + 1));
+        avel[2 * size_t(k) + 1] = A[0] + A[1] + A[2] + A[3];
+        for (int sd_ = 0; sd_ < 4; ++sd_) sarea[size_t(k) * 4 + sd_] = A[sd_];
+      }
+      HG_CUDA(cudaMemcpy(pc->d_av_el, avel.data(), avel.size() * sizeof(double), cudaMemcpyHostToDevice));
+      HG_CUDA(cudaMemcpy(pc->d_side_area, sarea.data(), sarea.size() * sizeof(double), cudaMemcpyHostToDevice));
     }
   }
   // per-element corner distances of the whole mesh (EstimateTimeStep runs over mesh order)

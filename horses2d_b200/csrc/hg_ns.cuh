@@ -44,6 +44,7 @@ struct NSArgs {
   const real* FX;           // exact-solver face fluxes [n_el*4][P][4] of this stage (RIEMANN_EXACT faces)
   const real* NF;           // mortar face fluxes [slots][P][4] of the SIDE_FLUX sides (stage kernel)
   const real* NFG;          // mortar BR1 gradient face terms [slots][P][2][4] of the SIDE_FLUX sides
+  const real* NJ;           // mortar jump sums [slots][2] of the SIDE_FLUX sides (dissipation indicator)
   double* Q;
   real* G;
   const real* T_in;         // Q traces of the current state  [n_el*4][P][4]
@@ -306,6 +307,11 @@ __device__ __forceinline__ void element_viscosity(const NSArgs<real>& a, NSTiles
       const int sd_ = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + sd_];
       const int kind = sd.y & 15;
+      if (kind == SIDE_FLUX) {   // edge between orders or subdivided edge: the mortar kernel's jump sums
+        s.face[0][le][t] = kk == 0 ? a.NJ[size_t(sd.x) * 2] : real(0);
+        s.face[1][le][t] = kk == 0 ? a.NJ[size_t(sd.x) * 2 + 1] : real(0);
+        continue;
+      }
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
       real qo[4];
       trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);

@@ -87,11 +87,13 @@ def shock_labels(Q, nx, ny, mach=3.0):
 
 
 def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, precision=L.PREC_FP64,
-                       neg_ratio=8, learned=None):
+                       neg_ratio=8, learned=None, hard_weight=4.0):
     """Plain-solver snapshots (modal-decay sensor) of seeded shock positions x_s = 5 + U(-0.5, 0.5)
     (moved to the nearest element face) and bump amplitudes U(0.1, 0.3).  Returns a dict with the
-    sampled training set (all troubled elements + neg_ratio times as many smooth ones per snapshot,
-    class-balanced weights); snapshots whose state is not finite are left out and counted.
+    sampled training set (all troubled elements, the smooth elements two to four elements from the
+    band on either side, and neg_ratio times as many other smooth ones per snapshot; class-balanced
+    weights, the near-band smooth elements weighted hard_weight times more); snapshots whose state is not
+    finite are left out and counted.
     learned = (params, lo, hi) runs the solver with the learned indicator instead (the second round
     of training sees the states the learned sensor itself produces)."""
     rng = np.random.default_rng(seed)
@@ -103,7 +105,7 @@ def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, pre
         g.set_sensor(L.SENSOR_LEARNED, mlp=learned[0], lo=learned[1], hi=learned[2])
     g.set_state(shock_state(desc))
     dt = g.estimate_time_step(cfl, 1.0)
-    Xs, ts, meta = [], [], []
+    Xs, ts, hs, meta = [], [], [], []
     dropped = 0
     for _ in range(n_snap):
         xs, amp = snap_to_face(5.0 + rng.uniform(-0.5, 0.5), nx), rng.uniform(0.1, 0.3)
@@ -114,17 +116,24 @@ def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, pre
             dropped += 1
             continue
         feats, _ = g.sensor_eval()
-        lab, _ = shock_labels(Q, nx, ny)
+        lab, col = shock_labels(Q, nx, ny)
         pos = np.flatnonzero(lab > 0.5)
-        neg = np.flatnonzero(lab < 0.5)
+        # hard negatives: the smooth cells two to four elements from the labelled band on either side
+        # (the post-shock oscillation makes the downstream ones look troubled), always in the set
+        off = np.array([-4, -3, -2, 2, 3, 4])
+        near = (np.arange(ny)[:, None] * nx + np.clip(col[:, None] + off[None, :], 0, nx - 1)).ravel()
+        near = np.unique(near[lab[near] < 0.5])
+        neg = np.setdiff1d(np.flatnonzero(lab < 0.5), near)
         neg = rng.choice(neg, size=min(len(neg), neg_ratio * len(pos)), replace=False)
-        idx = np.concatenate([pos, neg])
+        idx = np.concatenate([pos, near, neg])
         Xs.append(feats[idx])
         ts.append(lab[idx])
+        hs.append(np.concatenate([np.zeros(len(pos)), np.ones(len(near)), np.zeros(len(neg))]))
         meta.append((xs, amp))
     X = np.concatenate(Xs).astype(np.float32)
     t = np.concatenate(ts).astype(np.float32)
-    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12)).astype(np.float32)
+    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12))
+    w = (w * np.where(np.concatenate(hs) > 0.5, hard_weight, 1.0)).astype(np.float32)
     g.close()
     return dict(X=X, t=t, w=w, meta=meta, dt=dt, steps=steps, dropped=dropped)
 
@@ -138,7 +147,8 @@ def train_two_rounds(n_snap, seed, nx=512, ny=64, N=3, steps=200, epochs=40, bat
     d2 = generate_snapshots(n_snap, seed + 1, nx, ny, N, steps, learned=(p1, lo, hi))
     X = np.concatenate([d1["X"], d2["X"]])
     t = np.concatenate([d1["t"], d2["t"]])
-    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12)).astype(np.float32)
+    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12))
+    w = (w * np.where(np.concatenate(hs) > 0.5, hard_weight, 1.0)).astype(np.float32)
     p2, h2 = train(X, t, w, epochs, batch, lr, seed + 1)
     lo, hi = feature_box(X)
     return p2, lo, hi, dict(samples=len(t), dropped=d1["dropped"] + d2["dropped"], loss_round1=h1.tolist(),

@@ -48,9 +48,8 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
 
 
 def test_mixed_order_descriptor_validation():
-    """Mixed orders are checked before any device call: artificial dissipation in the Navier-Stokes
-    build and Euler orders above 12 are refused with the reason (CPU; the oracle's export gives the
-    descriptor)."""
+    """Mixed orders are checked before any device call: Euler orders above 12 are refused with the
+    reason (CPU; the oracle's export gives the descriptor)."""
     import numpy as np
     import pytest
     import horses2d_b200 as hg
@@ -62,9 +61,6 @@ def test_mixed_order_descriptor_validation():
     d = orc.export_mesh()
     assert len(d["edge_n"]) == 2 * sum(max(d["N"][a], d["N"][b] if b >= 0 else 0) + 1
                                        for a, b in d["edge_elem"].reshape(-1, 2))
-    with pytest.raises(hg.HorsesGpuError, match="take no artificial dissipation"):
-        hg.GpuDGSEM(d, mach=0.5, navier_stokes=1, reynolds=100.0, viscous=hg.IP, av_type=hg.AV_LAPLACIAN,
-                    bcs=[dict(type=hg.BC_PERIODIC)] * 4)
     d13 = dict(d, N=np.where(d["N"] == 3, 13, d["N"]).astype(np.int32))
     with pytest.raises(hg.HorsesGpuError, match="1..12"):
         hg.GpuDGSEM(d13, mach=0.5, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
