@@ -25,6 +25,7 @@ from . import mesh as hmesh
 from .solver import GpuDGSEM
 
 GAMMA = 1.4
+HARD_WEIGHT = 4.0   # weight of the smooth elements next to the shock band in training (hard negatives)
 
 
 def rankine_hugoniot(mach, gamma=GAMMA):
@@ -87,7 +88,7 @@ def shock_labels(Q, nx, ny, mach=3.0):
 
 
 def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, precision=L.PREC_FP64,
-                       neg_ratio=8, learned=None, hard_weight=4.0):
+                       neg_ratio=8, learned=None, hard_weight=None):
     """Plain-solver snapshots (modal-decay sensor) of seeded shock positions x_s = 5 + U(-0.5, 0.5)
     (moved to the nearest element face) and bump amplitudes U(0.1, 0.3).  Returns a dict with the
     sampled training set (all troubled elements, the smooth elements two to four elements from the
@@ -96,6 +97,7 @@ def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, pre
     finite are left out and counted.
     learned = (params, lo, hi) runs the solver with the learned indicator instead (the second round
     of training sees the states the learned sensor itself produces)."""
+    hard_weight = HARD_WEIGHT if hard_weight is None else hard_weight
     rng = np.random.default_rng(seed)
     desc, kw = shock_case(nx, ny, N)
     g = GpuDGSEM(desc, precision=precision, **kw)
@@ -132,10 +134,17 @@ def generate_snapshots(n_snap, seed, nx=512, ny=64, N=3, steps=200, cfl=0.1, pre
         meta.append((xs, amp))
     X = np.concatenate(Xs).astype(np.float32)
     t = np.concatenate(ts).astype(np.float32)
-    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12))
-    w = (w * np.where(np.concatenate(hs) > 0.5, hard_weight, 1.0)).astype(np.float32)
+    hard = np.concatenate(hs)
+    w = sample_weights(t, hard, hard_weight)
     g.close()
-    return dict(X=X, t=t, w=w, meta=meta, dt=dt, steps=steps, dropped=dropped)
+    return dict(X=X, t=t, w=w, hard=hard, meta=meta, dt=dt, steps=steps, dropped=dropped)
+
+
+def sample_weights(t, hard, hard_weight=HARD_WEIGHT):
+    """Class-balanced weights (each class sums to half), the near-band smooth samples hard_weight times
+    heavier."""
+    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12))
+    return (w * np.where(hard > 0.5, hard_weight, 1.0)).astype(np.float32)
 
 
 def train_two_rounds(n_snap, seed, nx=512, ny=64, N=3, steps=200, epochs=40, batch=4096, lr=2e-3):
@@ -147,8 +156,7 @@ def train_two_rounds(n_snap, seed, nx=512, ny=64, N=3, steps=200, epochs=40, bat
     d2 = generate_snapshots(n_snap, seed + 1, nx, ny, N, steps, learned=(p1, lo, hi))
     X = np.concatenate([d1["X"], d2["X"]])
     t = np.concatenate([d1["t"], d2["t"]])
-    w = np.where(t > 0.5, 0.5 / max(t.mean(), 1e-12), 0.5 / max(1.0 - t.mean(), 1e-12))
-    w = (w * np.where(np.concatenate(hs) > 0.5, hard_weight, 1.0)).astype(np.float32)
+    w = sample_weights(t, np.concatenate([d1["hard"], d2["hard"]]))
     p2, h2 = train(X, t, w, epochs, batch, lr, seed + 1)
     lo, hi = feature_box(X)
     return p2, lo, hi, dict(samples=len(t), dropped=d1["dropped"] + d2["dropped"], loss_round1=h1.tolist(),
