@@ -584,7 +584,8 @@ def run_shock(args, rank, world, local, dist):
     params, lo, hi, info = S.train_two_rounds(100, SEED, nx=nx, ny=ny, N=N, steps=100, epochs=30, batch=4096)
     train_s = time.perf_counter() - t0
     desc, kw = S.shock_case(nx, ny, N)
-    Q0 = S.shock_state(desc, S.snap_to_face(5.0, nx), 0.2)
+    x_shock = S.snap_to_face(5.0, nx)
+    Q0 = S.shock_state(desc, x_shock, 0.2)
     stream = torch.cuda.Stream()
     parts = [(desc, Q0, N, 1, kw, 0.1)]
 
@@ -617,8 +618,8 @@ def run_shock(args, rank, world, local, dist):
     rho_err = float(np.linalg.norm(Q32[0::4] - Q64l[0::4]) / np.linalg.norm(Q64l[0::4]))
     _, out32 = c32[0]["g"].sensor_eval()
     _, out64 = c64[0]["g"].sensor_eval()
-    m_learned = S.shock_metrics(Q32, out32[:, 3], nx, ny)
-    m_modal = S.shock_metrics(Q64, out64[:, 3], nx, ny)
+    m_learned = S.shock_metrics(Q32, out32[:, 3], nx, ny, x_shock)
+    m_modal = S.shock_metrics(Q64, out64[:, 3], nx, ny, x_shock)
     # end to end through the public API with host buffers (FP32 + learned)
     g = c32[0]["g"]
     Qpin = torch.empty(g.ndof, dtype=torch.float64).pin_memory()

@@ -8,8 +8,11 @@
 //            higher index is N; G = ramp(s; s0, kappa), the same sine ramp as the jumps indicator;
 //   learned  an MLP 16 -> 32 -> 32 -> 1 (tanh hidden layers, sigmoid output) on 16 modal features
 //            (for rho and p: log10 of the energy fraction in modal index k = 0..3 along xi and along
-//            eta, higher indices folded into 3, floored at 1e-10); G = sigmoid output, or the modal G
-//            when a feature lies outside the box seen in training (out-of-distribution fallback).
+//            eta, higher indices folded into 3, floored at 1e-10); G = the sigmoid output y mapped
+//            to max(0, (y - c) / (1 - c)), c = LEARNED_CUT (an exact zero below 1 % of the maximum
+//            viscosity, as the modal ramp has below s0 - kappa: elements without viscosity skip the
+//            dissipation's gradient work), or the modal G when a feature lies outside the box seen in
+//            training (out-of-distribution fallback).
 // No reference counterpart exists for modal and learned.
 #pragma once
 #include "hg_physics.cuh"
@@ -29,7 +32,13 @@ struct SensorArgs {
   const float* hi;     // [16]
 };
 
-__host__ __device__ constexpr int sensor_scratch(int P) { return 2 * P * P + 24 + MLP_IN + 2 * MLP_H + 4; }
+// Scratch row of one element (reals): the 16 features, the first hidden layer (as floats), the two
+// modal-decay indicators and the learned G, 16 out-of-box flags, the per-index energy sums of rho and p
+// along xi and eta (4P), the modal energies of rho and p (2 P^2); rows are a multiple of 4 reals long so
+// that the features and the hidden layer are read with 16-byte loads.
+constexpr int SR_FT = 0, SR_H = SR_FT + MLP_IN, SR_PN = SR_H + MLP_H, SR_OOD = SR_PN + 4, SR_SUM = SR_OOD + MLP_IN;
+__host__ __device__ constexpr int sensor_uh(int P) { return SR_SUM + 4 * P; }
+__host__ __device__ constexpr int sensor_scratch(int P) { return (sensor_uh(P) + 2 * P * P + 3) / 4 * 4; }
 
 __device__ __forceinline__ double sensor_ramp(double s, double s0, double k) {
   if (s < s0 - k) return 0.0;
@@ -38,6 +47,8 @@ __device__ __forceinline__ double sensor_ramp(double s, double s0, double k) {
 }
 
 __device__ __forceinline__ float mlp_sigmoid(float z) { return 1.0f / (1.0f + expf(-z)); }
+constexpr float LEARNED_CUT = 0.01f;
+__device__ __forceinline__ float learned_g(float y) { return y > LEARNED_CUT ? (y - LEARNED_CUT) / (1.0f - LEARNED_CUT) : 0.0f; }
 
 // smallest energy fraction a feature resolves (log10 floor -10: FP32 round-off, ~1e-14, stays below)
 constexpr double SENSOR_FLOOR = 1e-10;
@@ -56,13 +67,47 @@ struct SensorOut {
 // results are valid in thread tid == 0 of each element.
 //
 // Network inference: the weights (stored with the hidden unit fastest) are copied once per CTA into
-// shared memory, and each warp evaluates one element at a time with one lane per hidden unit: the
-// inputs are broadcast from the element's scratch row, the 32-input sums of the second layer run as
-// four interleaved partial sums, and the output unit is a warp shuffle tree.
+// shared memory by asynchronous copies issued on entry, so that they arrive during the modal
+// transform; each warp evaluates one element at a time with one lane per hidden unit: the inputs and
+// the first hidden layer are broadcast from the element's scratch row as 16-byte loads, the 32-input
+// sums of the second layer run as four interleaved partial sums, and the output unit is a warp
+// shuffle tree.  The out-of-box test runs per feature in the thread that forms it.
 // Shared memory the indicator needs when the caller lends it (EXT): EPB scratch rows, then the weights.
 template <int P, int EPB, typename real>
 __host__ __device__ constexpr size_t sensor_ext_bytes() {
-  return size_t(EPB) * sensor_scratch(P) * sizeof(real) + size_t(MLP_PARAMS) * sizeof(float);
+  return 16 + size_t(EPB) * sensor_scratch(P) * sizeof(real) + size_t(MLP_PARAMS) * sizeof(float);
+}
+
+// The network's weights into shared memory (16-byte aligned) as asynchronous copies: 16-byte chunks,
+// the odd last float as a 4-byte copy.  Each thread waits for its own with sensor_weights_wait; a
+// barrier after that makes all of them visible.
+__device__ __forceinline__ void sensor_weights_async(float* s_w, const float* g, int t, int nt) {
+  constexpr int C16 = MLP_PARAMS / 4;
+  const unsigned base = static_cast<unsigned>(__cvta_generic_to_shared(s_w));
+  for (int c = t; c < C16; c += nt)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(base + 16u * unsigned(c)), "l"(g + 4 * c)
+                 : "memory");
+  if (t == 0)
+    for (int d = 4 * C16; d < MLP_PARAMS; ++d)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(base + 4u * unsigned(d)), "l"(g + d) : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void sensor_weights_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// 16 consecutive reals of a 16-byte aligned shared row as floats
+__device__ __forceinline__ void load16(const float* r, float* f) {
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 v = reinterpret_cast<const float4*>(r)[k];
+    f[4 * k] = v.x; f[4 * k + 1] = v.y; f[4 * k + 2] = v.z; f[4 * k + 3] = v.w;
+  }
+}
+__device__ __forceinline__ void load16(const double* r, float* f) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const double2 v = reinterpret_cast<const double2*>(r)[k];
+    f[2 * k] = float(v.x); f[2 * k + 1] = float(v.y);
+  }
 }
 
 template <int P, int EPB, typename real, bool EXT = false>
@@ -70,23 +115,28 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
                                                     const real (*Q)[EPB][P * P], int n_active,
                                                     const real* Vinv, int le, int tid, bool active,
                                                     float* feat_out, real* ext = nullptr) {
-  constexpr int NP = P * P, N = P - 1, SS = sensor_scratch(P);
-  // scratch rows of the CTA's elements: declared here, or lent by the caller (EXT: shared memory the
-  // caller no longer needs, sensor_ext_bytes long), so that every access is a shared-memory one
+  constexpr int NP = P * P, N = P - 1, SS = sensor_scratch(P), UH = sensor_uh(P);
+  // scratch rows of the CTA's elements, then the weights: declared here, or lent by the caller (EXT:
+  // shared memory the caller no longer needs, sensor_ext_bytes long), so that every access is a
+  // shared-memory one
   real* scr_all;
+  float* s_w;   // W1^T[16][32] b1 W2^T[32][32] b2 W3 b3
   if constexpr (EXT) {
-    scr_all = ext;
+    scr_all = reinterpret_cast<real*>((reinterpret_cast<uintptr_t>(ext) + 15) & ~uintptr_t(15));
+    s_w = reinterpret_cast<float*>(scr_all + EPB * SS);
   } else {
-    __shared__ real s_scr[EPB * SS];
+    __shared__ __align__(16) real s_scr[EPB * SS];
+    __shared__ __align__(16) float s_w_own[MLP_PARAMS];
     scr_all = s_scr;
+    s_w = s_w_own;
   }
+  const bool learned = sa.kind == SENSOR_LEARNED;
+  // the weights travel while the modal transform runs
+  if (learned) sensor_weights_async(s_w, sa.mlp, threadIdx.x, blockDim.x);
   real* scr = scr_all + (le < EPB ? le : 0) * SS;
-  real* uh = scr;                 // [2][NP] modal coefficients of rho, p (k_eta * P + k_xi)
-  real* en = scr + 2 * NP;        // [2][12]: Ex[4], Ey[4], E, EN, -, -
-  real* ft = en + 24;             // [16] features
-  real* h1 = ft + MLP_IN;         // [32]
-  real* h2 = h1 + MLP_H;          // [32]
-  real* pn = h2 + MLP_H;          // [2] modal-decay indicators of rho and p, [2] learned G
+  real* uh = scr + UH;            // [2][NP] modal coefficients, then energies, of rho, p (k_eta * P + k_xi)
+  real* sum = scr + SR_SUM;       // [2 variables][2 directions][P] energies per modal index
+  real* pn = scr + SR_PN;         // [2] modal-decay indicators of rho and p, [2] learned G
   SensorOut out{0.0, 0.0, 0.0, 0};
   // nodal pressure into uh[NP..) as a staging area, then the transform in place per variable
   real pnode = real(0);
@@ -123,29 +173,45 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
   __syncthreads();
   if (active) { uh[tid] = c0 * c0; uh[NP + tid] = c1 * c1; }   // modal energies
   __syncthreads();
-  // features q < 16 and the two modal-decay indicators (q = 16, 17), one per thread
+  // energies per modal index: t = (v * 2 + dir) * P + k sums over the other index
+  if (active)
+    for (int t = tid; t < 4 * P; t += NP) {
+      const int v = t / (2 * P), dir = (t / P) & 1, k = t % P;
+      const real* c2 = uh + v * NP;
+      real a = real(0);
+#pragma unroll
+      for (int j = 0; j < P; ++j) a += c2[dir == 0 ? j * P + k : k * P + j];
+      sum[t] = a;
+    }
+  __syncthreads();
+  // features q < 16 (with their out-of-box flags) and the two modal-decay indicators (q = 16, 17)
   if (active)
     for (int q = tid; q < MLP_IN + 2; q += NP) {
       const int v = q < MLP_IN ? q >> 3 : q - MLP_IN;
-      const real* c2 = uh + v * NP;
-      real E = real(0), part = real(0);
+      const real* sv = sum + 2 * v * P;   // along xi: sv[m]; along eta: sv[P + n]
+      real E = real(0);
+#pragma unroll
+      for (int m = 0; m < P; ++m) E += sv[m];
       if (q < MLP_IN) {
         const int dir = (q >> 2) & 1, k = q & 3;
-        for (int n = 0; n < P; ++n)
-          for (int m = 0; m < P; ++m) {
-            const real x = c2[n * P + m];
-            const int idx = dir == 0 ? m : n;
-            E += x;
-            if ((idx < 3 ? idx : 3) == k) part += x;
-          }
-        ft[q] = log10_r(fmax_r(E > real(0) ? part / E : real(0), real(SENSOR_FLOOR)));
+        real part = real(0);
+        if (k < 3) {
+          if (k < P) part = sv[dir * P + k];
+        } else {
+          for (int m = 3; m < P; ++m) part += sv[dir * P + m];
+        }
+        const real f = log10_r(fmax_r(E > real(0) ? part / E : real(0), real(SENSOR_FLOOR)));
+        scr[SR_FT + q] = f;
+        if (feat_out) feat_out[q] = float(f);
+        scr[SR_OOD + q] = (sa.lo && (float(f) < __ldg(sa.lo + q) || float(f) > __ldg(sa.hi + q))) ? real(1) : real(0);
       } else {
-        for (int n = 0; n < P; ++n)
-          for (int m = 0; m < P; ++m) {
-            const real x = c2[n * P + m];
-            E += x;
-            if (m == N || n == N) part += x;
-          }
+        // the modes whose higher index is N: row N along eta plus column N below it
+        const real* c2 = uh + v * NP;
+        real part = real(0);
+#pragma unroll
+        for (int m = 0; m < P; ++m) part += c2[N * P + m];
+#pragma unroll
+        for (int n = 0; n < N; ++n) part += c2[n * P + N];
         pn[v] = (E > real(0) && part > real(0)) ? log10_r(part / E) : real(-1e30);
       }
     }
@@ -153,48 +219,47 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
   if (active && tid == 0) {
     const double smax = double(pn[0] > pn[1] ? pn[0] : pn[1]);
     out.g_modal = sensor_ramp(smax, sa.s0, sa.kappa);
-    int ood = 0;
-    for (int q = 0; q < MLP_IN; ++q) {
-      if (feat_out) feat_out[q] = float(ft[q]);
-      if (sa.lo && (float(ft[q]) < sa.lo[q] || float(ft[q]) > sa.hi[q])) ood = 1;
-    }
-    out.ood = ood;
+    real ood = real(0);
+#pragma unroll
+    for (int q = 0; q < MLP_IN; ++q) ood += scr[SR_OOD + q];
+    out.ood = ood > real(0);
   }
-  if (sa.kind == SENSOR_LEARNED) {
+  if (learned) {
     static_assert(MLP_H == 32, "one lane per hidden unit");
-    float* s_w;   // W1^T[16][32] b1 W2^T[32][32] b2 W3 b3
-    if constexpr (EXT) {
-      s_w = reinterpret_cast<float*>(ext + EPB * SS);
-    } else {
-      __shared__ float s_w_own[MLP_PARAMS];
-      s_w = s_w_own;
-    }
-    for (int d = threadIdx.x; d < MLP_PARAMS; d += blockDim.x) s_w[d] = __ldg(sa.mlp + d);
+    sensor_weights_wait();
     __syncthreads();
+    // one warp per element, one lane per hidden unit; inputs and the first hidden layer are read back
+    // as broadcast 16-byte loads, the output unit is a shuffle tree
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     for (int el = threadIdx.x >> 5; el < n_active; el += nw) {
       real* r = scr_all + el * SS;
-      const real* f = r + 2 * NP + 24;
-      real* g1 = r + 2 * NP + 24 + MLP_IN;
+      float f[MLP_IN];
+      load16(r + SR_FT, f);
       float z = s_w[MLP_B1 + lane];
 #pragma unroll
-      for (int q = 0; q < MLP_IN; ++q) z += s_w[MLP_W1 + q * MLP_H + lane] * float(f[q]);
-      g1[lane] = real(tanhf(z));
+      for (int q = 0; q < MLP_IN; ++q) z += s_w[MLP_W1 + q * MLP_H + lane] * f[q];
+      float* h1 = reinterpret_cast<float*>(r + SR_H);
+      h1[lane] = tanhf(z);
       __syncwarp();
       float zp[4] = {s_w[MLP_B2 + lane], 0.0f, 0.0f, 0.0f};
-#pragma unroll
-      for (int q = 0; q < MLP_H; ++q) zp[q & 3] += s_w[MLP_W2 + q * MLP_H + lane] * float(g1[q]);
+#pragma unroll 2
+      for (int q4 = 0; q4 < MLP_H / 4; ++q4) {
+        const float4 h = reinterpret_cast<const float4*>(h1)[q4];
+        zp[0] += s_w[MLP_W2 + (4 * q4 + 0) * MLP_H + lane] * h.x;
+        zp[1] += s_w[MLP_W2 + (4 * q4 + 1) * MLP_H + lane] * h.y;
+        zp[2] += s_w[MLP_W2 + (4 * q4 + 2) * MLP_H + lane] * h.z;
+        zp[3] += s_w[MLP_W2 + (4 * q4 + 3) * MLP_H + lane] * h.w;
+      }
       const float h = tanhf((zp[0] + zp[1]) + (zp[2] + zp[3]));
       float y = s_w[MLP_W3 + lane] * h;
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) y += __shfl_xor_sync(0xffffffffu, y, off);
-      if (lane == 0) r[2 * NP + 24 + MLP_IN + 2 * MLP_H + 2] = real(mlp_sigmoid(y + s_w[MLP_B3]));
-      __syncwarp();
+      if (lane == 0) r[SR_PN + 2] = real(learned_g(mlp_sigmoid(y + s_w[MLP_B3])));
     }
     __syncthreads();
     if (active && tid == 0) out.g_learned = double(pn[2]);
   }
-  out.g = sa.kind == SENSOR_LEARNED ? (out.ood ? out.g_modal : out.g_learned) : out.g_modal;
+  out.g = learned ? (out.ood ? out.g_modal : out.g_learned) : out.g_modal;
   return out;
 }
 

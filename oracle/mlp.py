@@ -105,16 +105,25 @@ def gauss_nodes(P):
     return 0.5 * (x + 1.0)
 
 
+LEARNED_CUT = 0.01
+
+
+def learned_g(y, cut=LEARNED_CUT):
+    """The indicator's G from the network's sigmoid output y: max(0, (y - cut) / (1 - cut))."""
+    y = np.asarray(y, dtype=np.float64)
+    return np.where(y > cut, (y - cut) / (1.0 - cut), 0.0)
+
+
 def learned_indicator(params, lo, hi, Q, xi, s0, kappa=1.0):
     """Per-element G of the learned indicator, as the device forms it (hg_sensor.cuh element_sensor):
-    the network's sigmoid output on the element's 16 features, or the modal-decay G (sine ramp of the
-    modal indicator around s0, half width kappa) where a feature, rounded to FP32, lies outside the
-    training box [lo, hi] (the out-of-distribution fallback).  FP64 throughout."""
+    learned_g of the network's sigmoid output on the element's 16 features, or the modal-decay G (sine
+    ramp of the modal indicator around s0, half width kappa) where a feature, rounded to FP32, lies
+    outside the training box [lo, hi] (the out-of-distribution fallback).  FP64 throughout."""
     X, s = element_features(Q, xi)
     g_modal = ramp(s, s0, kappa)
     X32 = X.astype(np.float32)
     ood = np.any((X32 < np.asarray(lo, np.float32)) | (X32 > np.asarray(hi, np.float32)), axis=1)
-    return np.where(ood, g_modal, predict(params, X)), ood
+    return np.where(ood, g_modal, learned_g(predict(params, X))), ood
 
 
 def step_learned(orc, params, lo, hi, xi, scheme, t, dt, s0, kappa=1.0):

@@ -116,7 +116,7 @@ def test_learned_sensor_residual_parity_and_fallback():
     assert 0 < ood.sum() < len(ood)
     np.testing.assert_array_equal(out[ood, 3], out[ood, 0])        # fallback: modal G
     np.testing.assert_allclose(out[~ood, 3], out[~ood, 1], rtol=0, atol=0)
-    np.testing.assert_allclose(out[:, 1], S.mlp_forward(p, feats), rtol=0, atol=1e-6)
+    np.testing.assert_allclose(out[:, 1], omlp.learned_g(S.mlp_forward(p, feats)), rtol=0, atol=1e-6)
     orc.set_av_g(out[:, 3])
     orc.set_state(Q)
     ref = orc.time_derivative(0.0)
@@ -127,7 +127,9 @@ def test_learned_sensor_residual_parity_and_fallback():
 def test_learned_sensor_end_to_end_gain_over_modal():
     """Train on plain-solver snapshots (two rounds), then run held-out shock cases with each indicator
     driving the artificial viscosity.  The learned indicator finds the whole shock band (the modal one,
-    at its default calibration, flags only the element holding the jump) with few false positives."""
+    at its default calibration, flags only the element holding the jump) with few false positives, and
+    the standing shock of the solution moves no further from where it started than with the modal
+    indicator."""
     nx, ny = 128, 8
     params, lo, hi, info = S.train_two_rounds(30, 11, nx=nx, ny=ny, N=3, steps=150, epochs=40, batch=2048)
     assert info["dropped"] == 0
@@ -148,11 +150,15 @@ def test_learned_sensor_end_to_end_gain_over_modal():
             Q = g.state()
             assert np.all(np.isfinite(Q))
             _, out = g.sensor_eval()
-            stats[name] = S.shock_metrics(Q, out[:, 3], nx, ny)
+            stats[name] = S.shock_metrics(Q, out[:, 3], nx, ny, xs)
             if kind == hg.SENSOR_LEARNED:
                 stats["disagreement"] = S.disagreement(out[:, 0], out[:, 3])
         assert stats["learned"]["recall"] >= 0.9
         assert stats["learned"]["recall"] >= stats["modal"]["recall"] + 0.3
         assert stats["learned"]["false_positive_rate"] <= 0.05
-        assert stats["learned"]["shock_position_error"] <= 0.3
+        assert stats["learned"]["band_offset"] <= 0.3
+        # the shock of the solution stays where it stood at least as well as with the modal indicator
+        print(f"shock position error: learned {stats['learned']['shock_position_error']:.3e}, "
+              f"modal {stats['modal']['shock_position_error']:.3e}")
+        assert stats["learned"]["shock_position_error"] <= stats["modal"]["shock_position_error"] * 1.02 + 1e-6
         assert stats["disagreement"] <= 0.1
