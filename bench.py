@@ -835,7 +835,8 @@ def run_kh(args, rank, world, local, dist):
                                         "ood_fraction": float(out32[:, 2].mean()),
                                         "disagreement_vs_modal": S.disagreement(out32[:, 0], out32[:, 3]),
                                         "note": ("the learned indicator runs every step (inference fused into the "
-                                                 "gradient pass); the shear layer is smooth, and it flags "
+                                                 "epilogue of each step's last stage); the shear layer is smooth, "
+                                                 "and it flags "
                                                  f"{troubled:.1%} of the elements (the modal indicator: "
                                                  f"{float((out32[:, 0] > S.TROUBLED).mean()):.1%})")}},
             "clocks": clk}

@@ -522,13 +522,14 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
   const real penalty = IP ? real(a.sigma0) * mu_f * real(P - 1) * real(P - 1) * invh : real(0);
   real F[4], Gx[4] = {real(0), real(0), real(0), real(0)}, Gy[4] = {real(0), real(0), real(0), real(0)};
   if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
-    const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
     real qn[4], gnx[4] = {real(0), real(0), real(0), real(0)}, gny[4] = {real(0), real(0), real(0), real(0)};
-    ld4(a.T_in + (size_t(sd.x) * P + kn) * 4, qn);
+    // the neighbour's traces, prefetched into this task's own face slots (prefetch_neighbour_traces)
+    cp_async_wait_all();
+#pragma unroll
+    for (int k = 0; k < 4; ++k) qn[k] = s.face[k][le][t];
     if (visc) {
-      const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
-      ld4(gp, gnx);
-      ld4(gp + 4, gny);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { gnx[k] = s.face[4 + k][le][t]; gny[k] = s.face[8 + k][le][t]; }
     }
     const bool right = kind == SIDE_RIGHT;
     const real* QL = right ? qn : qo;
@@ -622,6 +623,35 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
   }
 }
 
+// The neighbour traces that the face tasks of this thread read (Q traces, and the gradient traces
+// when viscous), copied asynchronously at the start of the launch into the task's own face slots:
+// face[0..3][le][t] and face[4..11][le][t] belong to face task t alone, which reads them before it
+// writes its fluxes there, so the copies need no barrier and their latency overlaps the volume phase.
+// The thread-to-task map is that of the face phase (t = tid, tid + NP, ...).
+template <int P, int EPB, typename real, bool AFFINE>
+__device__ __forceinline__ void prefetch_neighbour_traces(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
+                                                          int le, int e, int tid, bool active, bool visc) {
+  constexpr int NP = P * P, FT = 4 * P;
+  if (active)
+    for (int t = tid; t < FT; t += NP) {
+      const int sd_ = t / P, kk = t % P;
+      const int4 sd = a.side[size_t(e) * 4 + sd_];
+      const int kind = sd.y & 15;
+      if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
+        const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
+        const real* qp = a.T_in + (size_t(sd.x) * P + kn) * 4;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cp_async_real(&s.face[k][le][t], qp + k);
+        if (visc) {
+          const real* gp = a.GT + (size_t(sd.x) * P + kn) * 8;
+#pragma unroll
+          for (int k = 0; k < 8; ++k) cp_async_real(&s.face[4 + k][le][t], gp + k);
+        }
+      }
+    }
+  cp_async_commit();
+}
+
 template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
 __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real> a) {
   constexpr int NP = P * P, FT = 4 * P;
@@ -634,9 +664,10 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   ph.load(a.pc);
   const real mu = ph.mu;
   real geoE[5];
+  const bool visc = a.viscous != 0;
+  prefetch_neighbour_traces<P, EPB, real, AFFINE>(a, s, le, e, tid, active, visc);
   load_tiles(a, s, flat, le, tid, e, active, geoE);
   const real mu_e = (AV && active) ? real(a.mu_av[e]) : real(0);
-  const bool visc = a.viscous != 0;
   // the element gradient feeds the viscous fluxes and the Laplacian dissipation's volume term; an
   // element without either (mu_e = 0: that term is exactly zero) skips it
   const bool need_grad = visc || (AV && a.av == 1 && mu_e != real(0));

@@ -9,7 +9,7 @@
 //   learned  an MLP 16 -> 32 -> 32 -> 1 (tanh hidden layers, sigmoid output) on 16 modal features
 //            (for rho and p: log10 of the energy fraction in modal index k = 0..3 along xi and along
 //            eta, higher indices folded into 3, floored at 1e-10); G = the sigmoid output y mapped
-//            to max(0, (y - c) / (1 - c)), c = LEARNED_CUT (an exact zero below 1 % of the maximum
+//            to max(0, (y - c) / (1 - c)), c = LEARNED_CUT (an exact zero below 5 % of the maximum
 //            viscosity, as the modal ramp has below s0 - kappa: elements without viscosity skip the
 //            dissipation's gradient work), or the modal G when a feature lies outside the box seen in
 //            training (out-of-distribution fallback).
@@ -47,7 +47,7 @@ __device__ __forceinline__ double sensor_ramp(double s, double s0, double k) {
 }
 
 __device__ __forceinline__ float mlp_sigmoid(float z) { return 1.0f / (1.0f + expf(-z)); }
-constexpr float LEARNED_CUT = 0.01f;
+constexpr float LEARNED_CUT = 0.05f;
 __device__ __forceinline__ float learned_g(float y) { return y > LEARNED_CUT ? (y - LEARNED_CUT) / (1.0f - LEARNED_CUT) : 0.0f; }
 
 // smallest energy fraction a feature resolves (log10 floor -10: FP32 round-off, ~1e-14, stays below)

@@ -91,6 +91,19 @@ __device__ __forceinline__ void st4(double* p, const double* v) {
   reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
 }
 
+// One value from global into shared memory as an asynchronous copy (4 or 8 bytes); the issuing thread
+// sees it after cp_async_wait_all.
+__device__ __forceinline__ void cp_async_real(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_real(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(static_cast<unsigned>(__cvta_generic_to_shared(dst))),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // max that keeps NaN (a residual that is NaN must stay visible)
 __device__ __forceinline__ double nanmax(double m, double v) { return (v > m || v != v) ? v : m; }
 

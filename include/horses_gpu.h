@@ -223,8 +223,8 @@ int  hg_residuals_noalloc(const double* qdot, int64_t ndof, void* cuda_stream, d
  *   HG_SENSOR_MODAL    G = ramp(s; s0, kappa), s = max over rho, p of log10(E_N/E) of the element's
  *                      orthonormal-Legendre modal energies (modal decay); the ramp is the reference's
  *                      sine ramp; s0 = NaN keeps log10((N+1)^-4), kappa = NaN keeps 1.
- *   HG_SENSOR_LEARNED  G = max(0, (y - 0.01) / 0.99), y the MLP's output (16 -> 32 -> 32 -> 1, tanh,
- *                      sigmoid) on HG_SENSOR_FEATURES modal features (zero below 1 % of the maximum
+ *   HG_SENSOR_LEARNED  G = max(0, (y - 0.05) / 0.95), y the MLP's output (16 -> 32 -> 32 -> 1, tanh,
+ *                      sigmoid) on HG_SENSOR_FEATURES modal features (zero below 5 % of the maximum
  *                      viscosity), or the modal G where a feature leaves [lo, hi] (fallback);
  *                      mlp = HG_MLP_PARAMS floats: W1[32][16] b1[32] W2[32][32] b2[32] W3[32] b3.
  * hg_sensor_eval: per element, the features ([n_el][16] floats, may be NULL) and {modal G, learned G

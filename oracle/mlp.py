@@ -105,7 +105,7 @@ def gauss_nodes(P):
     return 0.5 * (x + 1.0)
 
 
-LEARNED_CUT = 0.01
+LEARNED_CUT = 0.05
 
 
 def learned_g(y, cut=LEARNED_CUT):
