@@ -18,10 +18,21 @@ SOURCES = ["csrc/hg_api.cu", "csrc/hg_spectral.cpp", "csrc/hg_noalloc.cu", "csrc
            "csrc/hg_mesh.cpp", "csrc/hg_restart.cpp", "csrc/hg_mortar.cu", "csrc/hg_autosave.cu",
            "csrc/hg_inst_euler_hi.cu", "csrc/hg_inst_euler_hi_t1.cu", "csrc/hg_inst_ns_hi.cu",
            "csrc/hg_inst_euler.cu", "csrc/hg_inst_euler_t1.cu",
+           "csrc/hg_inst_euler32_hi.cu", "csrc/hg_inst_euler32_hi_t1.cu", "csrc/hg_inst_ns32_hi.cu",
+           "csrc/hg_inst_euler32.cu", "csrc/hg_inst_euler32_t1.cu",
            "csrc/hg_inst_sensor.cu"] + \
     [f"csrc/hg_inst_ns{prec}{part}{t}.cu" for t in ("", "_t1") for prec in ("64", "32") for part in "abcd"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC"]
+# FP32 stage kernels: quotients and square roots with the approximate (about 1-2 ulp) forms instead of
+# the correctly rounded instruction sequences.  Only the FP32 instantiation units get it: the FP64
+# kernels keep IEEE division and square root, which their bitwise parity with the oracle needs.
+FP32_FLAGS = ["-prec-div=false", "-prec-sqrt=false"]
+
+
+def flags_of(src):
+    b = os.path.basename(src)
+    return NVCC_FLAGS + (FP32_FLAGS if b.startswith("hg_inst_ns32") or b.startswith("hg_inst_euler32") else [])
 
 
 def nvcc():
@@ -61,7 +72,7 @@ def build(force=False, verbose=False):
     todo = [s for s in SOURCES if force or stale(obj_path(s), [os.path.join(HERE, s)] + hdr)]
 
     def compile_one(src):
-        cmd = [nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj_path(src)]
+        cmd = [nvcc()] + flags_of(src) + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj_path(src)]
         r = subprocess.run(cmd, cwd=HERE, capture_output=True, text=True)
         return src, r
 

@@ -1,5 +1,5 @@
 // hg_inst_euler_hi.cu -- explicit instantiations: Euler stage and trace kernels, orders 9-12 (the
-// high orders of p-refined meshes), FP64 and FP32.
+// high orders of p-refined meshes), FP64.
 #include "hg_launch.cuh"
 
 template void launch_stage_PV<10, double, 0>(hg_ctx*, const StageArgs<double>&);
@@ -10,11 +10,3 @@ template void launch_stage_PV<12, double, 0>(hg_ctx*, const StageArgs<double>&);
 template void launch_trace_P<12, double>(hg_ctx*);
 template void launch_stage_PV<13, double, 0>(hg_ctx*, const StageArgs<double>&);
 template void launch_trace_P<13, double>(hg_ctx*);
-template void launch_stage_PV<10, float, 0>(hg_ctx*, const StageArgs<float>&);
-template void launch_trace_P<10, float>(hg_ctx*);
-template void launch_stage_PV<11, float, 0>(hg_ctx*, const StageArgs<float>&);
-template void launch_trace_P<11, float>(hg_ctx*);
-template void launch_stage_PV<12, float, 0>(hg_ctx*, const StageArgs<float>&);
-template void launch_trace_P<12, float>(hg_ctx*);
-template void launch_stage_PV<13, float, 0>(hg_ctx*, const StageArgs<float>&);
-template void launch_trace_P<13, float>(hg_ctx*);

@@ -136,7 +136,7 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
   real* scr = scr_all + (le < EPB ? le : 0) * SS;
   real* uh = scr + UH;            // [2][NP] modal coefficients, then energies, of rho, p (k_eta * P + k_xi)
   real* sum = scr + SR_SUM;       // [2 variables][2 directions][P] energies per modal index
-  real* pn = scr + SR_PN;         // [2] modal-decay indicators of rho and p, [2] learned G
+  real* pn = scr + SR_PN;         // [2] modal-decay indicators of rho and p, learned G, constant-state flag
   SensorOut out{0.0, 0.0, 0.0, 0};
   // nodal pressure into uh[NP..) as a staging area, then the transform in place per variable
   real pnode = real(0);
@@ -200,7 +200,9 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
         } else {
           for (int m = 3; m < P; ++m) part += sv[dir * P + m];
         }
-        const real f = log10_r(fmax_r(E > real(0) ? part / E : real(0), real(SENSOR_FLOOR)));
+        // x / x is 1 exactly (also where the build's FP32 division is the approximate one)
+        const real frac = E > real(0) ? (part == E ? real(1) : part / E) : real(0);
+        const real f = log10_r(fmax_r(frac, real(SENSOR_FLOOR)));
         scr[SR_FT + q] = f;
         if (feat_out) feat_out[q] = float(f);
         scr[SR_OOD + q] = (sa.lo && (float(f) < __ldg(sa.lo + q) || float(f) > __ldg(sa.hi + q))) ? real(1) : real(0);
@@ -223,16 +225,28 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
 #pragma unroll
     for (int q = 0; q < MLP_IN; ++q) ood += scr[SR_OOD + q];
     out.ood = ood > real(0);
+    // constant-state element: every energy in the mean mode (fractions 1 and the floor exactly)
+    bool flat = true;
+#pragma unroll
+    for (int q = 0; q < MLP_IN; ++q)
+      flat = flat && scr[SR_FT + q] == ((q & 3) == 0 ? real(0) : log10_r(real(SENSOR_FLOOR)));
+    pn[3] = flat ? real(1) : real(0);
   }
   if (learned) {
     static_assert(MLP_H == 32, "one lane per hidden unit");
     sensor_weights_wait();
     __syncthreads();
     // one warp per element, one lane per hidden unit; inputs and the first hidden layer are read back
-    // as broadcast 16-byte loads, the output unit is a shuffle tree
+    // as broadcast 16-byte loads, the output unit is a shuffle tree.  Constant-state elements all have
+    // the same features: only the first of them in the CTA (rep) is evaluated, the others take its G
+    // (the same inputs through the same code: the same bits).
     const int lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    int rep = -1;
+    for (int el = 0; el < n_active && rep < 0; ++el)
+      if (scr_all[el * SS + SR_PN + 3] != real(0)) rep = el;
     for (int el = threadIdx.x >> 5; el < n_active; el += nw) {
       real* r = scr_all + el * SS;
+      if (r[SR_PN + 3] != real(0) && el != rep) continue;
       float f[MLP_IN];
       load16(r + SR_FT, f);
       float z = s_w[MLP_B1 + lane];
@@ -257,7 +271,7 @@ __device__ __forceinline__ SensorOut element_sensor(const SensorArgs& sa, const 
       if (lane == 0) r[SR_PN + 2] = real(learned_g(mlp_sigmoid(y + s_w[MLP_B3])));
     }
     __syncthreads();
-    if (active && tid == 0) out.g_learned = double(pn[2]);
+    if (active && tid == 0) out.g_learned = double(pn[3] != real(0) ? scr_all[rep * SS + SR_PN + 2] : pn[2]);
   }
   out.g = learned ? (out.ood ? out.g_modal : out.g_learned) : out.g_modal;
   return out;
