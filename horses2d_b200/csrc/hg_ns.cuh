@@ -99,6 +99,7 @@ struct NSTiles {
   real Gc[ST ? 4 : 1][ST ? EPB : 1][ST ? NP : 1];
   real face[12][EPB][FT];   // BR1 u* dS n (8) / F* (4) + gradient-face contravariant fluxes (8)
   real gfd[ST ? 4 : 1][ST ? EPB : 1][ST ? FT : 1];   // gradient-face terms contracted along their side
+  real dl[ST && AFFINE ? 2 : 1][ST && AFFINE ? P : 1];   // (lb0^T D)(l), (lb1^T D)(l): normal derivatives at the sides
   double red[32][4];
 };
 
@@ -485,19 +486,19 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
     if (IP && a.grad_faces && visc) {
       const real* gp = a.NFG + (size_t(sd.x) * P + kk) * 8;
       const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
-      real fJa00, fJa01, fJa10, fJa11, fJ;
-      if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+      real fJa00, fJa01, fJa10, fJa11, fiJ;   // metrics and 1/J at the face node
+      if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fiJ = geoE[4]; }
       else {
         fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
         fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
         fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
         fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
-        fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+        fiJ = real(1) / trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
       }
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        s.face[4 + k][le][t] = (gp[k] * fJa00 + gp[4 + k] * fJa10) / fJ;
-        s.face[8 + k][le][t] = (gp[k] * fJa01 + gp[4 + k] * fJa11) / fJ;
+        s.face[4 + k][le][t] = (gp[k] * fJa00 + gp[4 + k] * fJa10) * fiJ;
+        s.face[8 + k][le][t] = (gp[k] * fJa01 + gp[4 + k] * fJa11) * fiJ;
       }
     }
     return;
@@ -606,19 +607,19 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
   for (int k = 0; k < 4; ++k) s.face[k][le][t] = F[k];
   if (IP && a.grad_faces && visc) {
     // metrics at the face node (interpolated along the other direction) and contravariant G
-    real fJa00, fJa01, fJa10, fJa11, fJ;
-    if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fJ = real(1) / geoE[4]; }
+    real fJa00, fJa01, fJa10, fJa11, fiJ;   // metrics and 1/J at the face node (one division, or none)
+    if constexpr (AFFINE) { fJa00 = geoE[0]; fJa01 = geoE[1]; fJa10 = geoE[2]; fJa11 = geoE[3]; fiJ = geoE[4]; }
     else {
       fJa00 = trace_of(s, s.Ja, 0, le, sd_, kk, lbv);
       fJa01 = trace_of(s, s.Ja, 1, le, sd_, kk, lbv);
       fJa10 = trace_of(s, s.Ja, 2, le, sd_, kk, lbv);
       fJa11 = trace_of(s, s.Ja, 3, le, sd_, kk, lbv);
-      fJ = trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
+      fiJ = real(1) / trace_of(s, s.Ja, 4, le, sd_, kk, lbv);
     }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      s.face[4 + k][le][t] = (Gx[k] * fJa00 + Gy[k] * fJa10) / fJ;
-      s.face[8 + k][le][t] = (Gx[k] * fJa01 + Gy[k] * fJa11) / fJ;
+      s.face[4 + k][le][t] = (Gx[k] * fJa00 + Gy[k] * fJa10) * fiJ;
+      s.face[8 + k][le][t] = (Gx[k] * fJa01 + Gy[k] * fJa11) * fiJ;
     }
   }
 }
@@ -812,7 +813,20 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
       real tr[4];
       trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, tr);
       st4(a.T_out + ((size_t(e) * 4 + sd_) * P + kk) * 4, tr);
+      if (IP && AFFINE && a.fuse && visc) {   // the face tiles are dead since the lift
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s.face[k][le][t] = tr[k];
+      }
     }
+  }
+  if (IP && AFFINE && a.fuse && a.update && visc && flat < 2 * P) {
+    const int sdt = flat / P, l = flat % P;
+    const real* lbv = sdt == 0 ? lb0 : lb1;
+    const real* DT = lbw1 + P;   // transposed D: DT[l * P + i] = D(i, l)
+    real d = real(0);
+#pragma unroll
+    for (int m = 0; m < P; ++m) d += lbv[m] * DT[l * P + m];
+    s.dl[sdt][l] = d;
   }
   if constexpr (IP) {
     // Fused interior penalty: what the next stage's neighbours read of this element's new state --
@@ -820,8 +834,48 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     // after the last stage of a step, its element-local indicator.  a.fuse, a.update, a.viscous and
     // a.last are uniform over the launch.
     if (a.fuse && a.update) {
-      __syncthreads();   // every node's new state is in s.Q
-      if (visc) {
+      __syncthreads();   // every node's new state is in s.Q (and, affine, its traces in s.face[0..3])
+      if (visc && AFFINE) {
+        // Affine element: the traces of the gradient straight from the new state.  Along the side, the
+        // derivative of the side's Q traces (D applied to them); across it, each normal line of nodes
+        // contracted with lb^T D.  The same as the nodal gradient interpolated to the side, without
+        // forming the gradient at every node.
+        if (active) {
+          const real* DT = lbw1 + P;   // transposed D
+          for (int t = tid; t < FT; t += NP) {
+            const int sd_ = t / P, kk = t % P;
+            const real* dlv = s.dl[(sd_ == 0 || sd_ == 3) ? 0 : 1];
+            real dt_[4] = {real(0), real(0), real(0), real(0)}, dn[4] = {real(0), real(0), real(0), real(0)};
+#pragma unroll
+            for (int l = 0; l < P; ++l) {
+              const real dk = DT[l * P + kk];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) dt_[k] += dk * s.face[k][le][sd_ * P + l];
+            }
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+              const int l = trace_step<real>(P, m, kk);
+              const int node = face_node(P, sd_, l, kk);
+              const real w = dlv[l];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) dn[k] += w * s.Q[k][le][node];
+            }
+            // bottom / top: along the side is xi; right / left: along the side is eta
+            const bool alongXi = sd_ == 0 || sd_ == 2;
+            const real Ja00 = geoE[0], Ja01 = geoE[1], Ja10 = geoE[2], Ja11 = geoE[3], iJ = geoE[4];
+            real tx[4], ty[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const real dxi = alongXi ? dt_[k] : dn[k], deta = alongXi ? dn[k] : dt_[k];
+              tx[k] = (dxi * Ja00 + deta * Ja01) * iJ;
+              ty[k] = (dxi * Ja10 + deta * Ja11) * iJ;
+            }
+            real* gp = a.GT_out + ((size_t(e) * 4 + sd_) * P + kk) * 8;
+            st4(gp, tx);
+            st4(gp + 4, ty);
+          }
+        }
+      } else if (visc) {
         element_gradient<P, EPB, real, AFFINE, IP>(a, s, ph, le, tid, e, active, geoE);
         __syncthreads();
         if (active) {
@@ -844,7 +898,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
         // within 48 KB (FP64 at high and low orders); otherwise the indicator declares its own
         constexpr size_t dead = sizeof(s.dQ) + sizeof(s.Fc) + sizeof(s.Gc) + sizeof(s.face) + sizeof(s.gfd);
         constexpr bool lend = dead >= sensor_ext_bytes<P, EPB, real>();
-        __syncthreads();   // the gradient traces above have read s.dQ
+        __syncthreads();   // the gradient traces above have read s.dQ (affine: s.face)
         const SensorOut so = element_sensor<P, EPB, real, lend>(a.sensor, ph, s.Q, n_active, s.mat + 2 * NP + 7 * P,
                                                                 le, tid, active, nullptr, &s.dQ[0][0][0][0]);
         if (active && tid == 0) a.mu_next[e] = a.av_el[2 * size_t(e)] * so.g;
