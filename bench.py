@@ -114,7 +114,10 @@ def build_parts(config):
         x = desc["x"].reshape(-1, 2)
         Q0 = cases.isentropic_vortex(x[:, 0], x[:, 1], mach=0.5, beta=5.0).ravel()
         kw = dict(mach=0.5, node_type=hg.NODES_LG, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
-        return [(desc, Q0, "5/7", 1, kw, 0.3)]
+        # CFL 0.1: at 0.3 the 384^2 box (192^2 too) goes non-finite within 40 steps -- on the oracle as on
+        # the device (at 48^2 and 96^2 it stays finite); at 0.1 the oracle stays finite over 250 steps,
+        # more than the 200 between the load warm-up's restarts
+        return [(desc, Q0, "5/7", 1, kw, 0.1)]
     if config == "cylinder":
         N = 5
         desc = hmesh.build_descriptor(cylinder_mesh(), N, hg.NODES_LG)
@@ -364,7 +367,7 @@ class CpuArm:
                              riemann=O.ROE, mach=0.5, bcs=hmesh.periodic_bcs_cartesian())
                 X = o.coords()
                 o.set_state(cases.isentropic_vortex(X[:, 0], X[:, 1], mach=0.5, beta=5.0).ravel())
-                self.orcs.append((o, o.estimate_dt(0.3, 1.0)))
+                self.orcs.append((o, o.estimate_dt(0.1, 1.0)))
             return
         inst = ensemble_spec() if config == "ensemble" else [dict(n=16, N=4, xc=0.0, yc=0.0, beta=5.0)]
         if config == "box512":
@@ -396,7 +399,8 @@ class CpuArm:
         from concurrent.futures import ThreadPoolExecutor
         if self.config in ("cylinder", "shock", "kh"):
             n, el, steps = self._run(self.orcs[0], budget_s, False)
-            what = ("128 x 128 elements of the 1024 x 1024 kh workload" if self.config == "kh"
+            what = ("scaled: 128 x 128 elements of the 1024 x 1024 kh workload (the rate per DOF-stage "
+                    "does not depend on the element count)" if self.config == "kh"
                     else f"full {self.config} workload")
             return (n / el, self.threads, f"{what} (NDOF {self.orcs[0][0].ndof}), {steps} RK3 "
                     f"steps in {el:.1f} s, OpenMP element loops on {self.threads} threads, FP64"
@@ -446,6 +450,45 @@ def make_contexts(parts, prec, stream):
         tune = g.autotune(trials=10)     # elements-per-CTA variant, timed on this workload's state
         ctxs.append(dict(g=g, Qh=Qh, N=N, ninst=ninst, cfl=cfl, tune=tune))
     return ctxs
+
+
+def bucket_launch_cost(prec, stream, dt, steps=200):
+    """Measured cost of running the ensemble as one context per order: the same group graph (five
+    contexts, one stage launch each per RK stage, the contexts on forked streams) with each context cut
+    to one 2 x 2-element instance, so that the kernels do almost no work, against one context alone
+    (three launches per step, what one kernel over all orders would launch).  ms per step of each."""
+    import torch
+    import horses2d_b200 as hg
+    from horses2d_b200 import mesh as hmesh, cases
+    kw = dict(mach=0.5, node_type=hg.NODES_LGL, riemann=hg.ROE, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+    gs = []
+    for N in (3, 4, 5, 6, 7):
+        d = hmesh.box_descriptor(2, 2, -5.0, 5.0, -5.0, 5.0, N, hg.NODES_LGL)
+        x = d["x"].reshape(-1, 2)
+        g = hg.GpuDGSEM(d, precision=prec, **kw)
+        g.set_stream(stream.cuda_stream)
+        g.set_state(cases.isentropic_vortex(x[:, 0], x[:, 1], mach=0.5, beta=0.0).ravel())   # the uniform stream
+        gs.append(g)
+
+    def timed(run):
+        run(3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    group = hg.GpuGroup(gs)
+    ms5 = timed(lambda n: group.time_steps(hg.SCHEME_RK3, n, 0.0, dt))
+    group.close()
+    ms1 = timed(lambda n: gs[2].time_steps(hg.SCHEME_RK3, n, 0.0, dt))
+    for g in gs:
+        g.close()
+    return {"five_orders_ms_per_step": ms5, "one_order_ms_per_step": ms1, "launches_per_step": [15, 3],
+            "sample": "one 2x2-element instance of the uniform stream per order (kernels with almost no work), "
+                      "group graph vs one context alone"}
 
 
 def tiling_summary(ctxs):
@@ -939,6 +982,11 @@ def main():
             "gpu_launches": launches,
             "roofline": roof["kernel"], "step_roofline": roof["step"], "kernel_share": roof["share"],
             "clocks": clk}
+
+    if args.config == "ensemble":
+        lc = bucket_launch_cost(prec, stream, dt)
+        lc["extra_share_of_step"] = (lc["five_orders_ms_per_step"] - lc["one_order_ms_per_step"]) / (ms / args.steps)
+        line["bucket_launches"] = lc
 
     # ---- FP32-bulk companion on the same workload (FP64 runs): speed and density error after K steps
     if prec == hg.PREC_FP64 and args.config == "cylinder":

@@ -33,7 +33,7 @@ struct hg_ctx {
   double* d_QDot = nullptr;
   double* d_resid = nullptr;      // per-CTA partial maxima of |QDot| of the last stage [grid][4]
   double* d_resid_out = nullptr;  // reduced maxima [4]
-  double* d_elmax = nullptr;      // [n_el][2] umax, amax per element
+  double* d_elmax = nullptr;      // [n_el][4] umax, amax per element and their NaN flags
   int cur = 0;                    // which trace buffer holds the current traces
   bool affine = false;            // per-element constant metrics and per-side constant normals
   bool ns = false, ip = false, grad_faces = false;   // Navier-Stokes kernels; interior penalty; SIPG/NIPG faces
