@@ -470,7 +470,7 @@ __device__ __forceinline__ void ns_volume_flux(const NSArgs<real>& a, NSTiles<P,
 template <int P, int EPB, typename real, bool AFFINE, bool IP, bool AV>
 __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
                                              const Phys<real>& ph, int le, int e, int t, real mu_e, bool visc,
-                                             const real* geoE) {
+                                             const real* geoE, const real (*own)[EPB][4 * P], bool own_g) {
   constexpr int NP = P * P;
   const real mu = ph.mu;
   const real* lb0 = s.mat + NP;
@@ -505,10 +505,19 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
   }
   const real* lbv = (sd_ == 0 || sd_ == 3) ? lb0 : lb1;
   real qo[4], gox[4] = {real(0), real(0), real(0), real(0)}, goy[4] = {real(0), real(0), real(0), real(0)};
-  trace4<P, EPB, real>(s.Q, le, sd_, kk, lbv, qo);
+  // this element's own traces of the current state (Q, and the gradient when viscous): what the previous
+  // stage (or the prologue, or this stage's gradient kernel) wrote for the neighbours, prefetched
+  cp_async_wait_all();
+#pragma unroll
+  for (int k = 0; k < 4; ++k) qo[k] = own[k][le][t];
   if (visc) {
-    trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, gox);
-    trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, goy);
+    if (own_g) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { gox[k] = own[4 + k][le][t]; goy[k] = own[8 + k][le][t]; }
+    } else {   // no shared memory left for them: formed here
+      trace4<P, EPB, real>(s.dQ[0], le, sd_, kk, lbv, gox);
+      trace4<P, EPB, real>(s.dQ[1], le, sd_, kk, lbv, goy);
+    }
   }
   const real* g3 = AFFINE ? a.side_geo + (size_t(e) * 4 + sd_) * 3 : a.side_geo + ((size_t(e) * 4 + sd_) * P + kk) * 3;
   const real nx = real(g3[0]), ny = real(g3[1]), dS = real(g3[2]);
@@ -624,20 +633,32 @@ __device__ __forceinline__ void ns_face_task(const NSArgs<real>& a, NSTiles<P, E
   }
 }
 
-// The neighbour traces that the face tasks of this thread read (Q traces, and the gradient traces
-// when viscous), copied asynchronously at the start of the launch into the task's own face slots:
-// face[0..3][le][t] and face[4..11][le][t] belong to face task t alone, which reads them before it
-// writes its fluxes there, so the copies need no barrier and their latency overlaps the volume phase.
-// The thread-to-task map is that of the face phase (t = tid, tid + NP, ...).
+// The traces that the face tasks of this thread read (Q traces, and the gradient traces when viscous),
+// copied asynchronously at the start of the launch: the neighbour's into the task's own face slots
+// (face[0..3][le][t] and face[4..11][le][t] belong to face task t alone, which reads them before it
+// writes its fluxes there), this element's own into s.own (the trace buffers hold them: the previous
+// stage's output, the prologue's, or this stage's gradient kernel's), so the copies need no barrier
+// and their latency overlaps the volume phase.  The thread-to-task map is that of the face phase
+// (t = tid, tid + NP, ...).
 template <int P, int EPB, typename real, bool AFFINE>
 __device__ __forceinline__ void prefetch_neighbour_traces(const NSArgs<real>& a, NSTiles<P, EPB, real, AFFINE>& s,
-                                                          int le, int e, int tid, bool active, bool visc) {
+                                                          real (*own)[EPB][4 * P], bool own_g, int le, int e,
+                                                          int tid, bool active, bool visc) {
   constexpr int NP = P * P, FT = 4 * P;
   if (active)
     for (int t = tid; t < FT; t += NP) {
       const int sd_ = t / P, kk = t % P;
       const int4 sd = a.side[size_t(e) * 4 + sd_];
       const int kind = sd.y & 15;
+      if (kind != SIDE_FLUX) {
+        const size_t slot = (size_t(e) * 4 + sd_) * P + kk;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cp_async_real(&own[k][le][t], a.T_in + slot * 4 + k);
+        if (visc && own_g) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) cp_async_real(&own[4 + k][le][t], a.GT + slot * 8 + k);
+        }
+      }
       if (kind == SIDE_LEFT || kind == SIDE_RIGHT) {
         const int kn = (sd.y & SIDE_REVERSED) ? (P - 1 - kk) : kk;
         const real* qp = a.T_in + (size_t(sd.x) * P + kn) * 4;
@@ -666,7 +687,11 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   const real mu = ph.mu;
   real geoE[5];
   const bool visc = a.viscous != 0;
-  prefetch_neighbour_traces<P, EPB, real, AFFINE>(a, s, le, e, tid, active, visc);
+  // the own traces of the face tasks: Q and gradient where the static shared memory allows (48 KB),
+  // else Q alone (the gradient traces are then formed in the face task)
+  constexpr bool OWN_G = sizeof(s) + size_t(12) * EPB * FT * sizeof(real) <= 48 * 1024;
+  __shared__ real s_own[OWN_G ? 12 : 4][EPB][FT];
+  prefetch_neighbour_traces<P, EPB, real, AFFINE>(a, s, s_own, OWN_G, le, e, tid, active, visc);
   load_tiles(a, s, flat, le, tid, e, active, geoE);
   const real mu_e = (AV && active) ? real(a.mu_av[e]) : real(0);
   // the element gradient feeds the viscous fluxes and the Laplacian dissipation's volume term; an
@@ -700,7 +725,7 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
   constexpr bool OVERLAP = 4 * (NP - FT) >= NP;
   if constexpr (OVERLAP) {
     if (active) {
-      if (tid < FT) ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, tid, mu_e, visc, geoE);
+      if (tid < FT) ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, tid, mu_e, visc, geoE, s_own, OWN_G);
       else
         for (int n = tid - FT; n < NP; n += NP - FT)
           ns_volume_flux<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, n, mu_e, need_grad, visc, geoE);
@@ -709,7 +734,8 @@ __global__ void __launch_bounds__(block_of(P, EPB)) ns_stage_kernel(NSArgs<real>
     if (active) ns_volume_flux<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, tid, mu_e, need_grad, visc, geoE);
     __syncthreads();
     if (active)
-      for (int t = tid; t < FT; t += NP) ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, t, mu_e, visc, geoE);
+      for (int t = tid; t < FT; t += NP)
+        ns_face_task<P, EPB, real, AFFINE, IP, AV>(a, s, ph, le, e, t, mu_e, visc, geoE, s_own, OWN_G);
   }
   __syncthreads();
   // The gradient-face terms enter the lift as hatD-contractions along their side, which depend on the
