@@ -58,12 +58,14 @@ __global__ void mlp_forward_kernel(const float* __restrict__ W, const float* __r
   y[i] = 1.0f / (1.0f + expf(-z));
 }
 
-// Block b: samples k in [b*TB, b*TB + TB) of the (optionally permuted) sample list.  Adds its
-// share of the gradient (scaled by inv_batch) to grad and of the loss (unscaled) to loss.
+// Block b: samples k in [b*TB, b*TB + TB) of the (optionally permuted) sample list.  Writes its share
+// of the gradient (scaled by inv_batch) to gpart[b][MLP_PARAMS] and of the loss (unscaled) to lpart[b];
+// the sums over blocks run in block order afterwards (mlp_adam_kernel, mlp_reduce_kernel), so that
+// training gives the same bits on every run (atomic adds would sum in arrival order).
 __global__ void __launch_bounds__(TB) mlp_grad_kernel(const float* __restrict__ W, const float* __restrict__ X,
                                                       const float* __restrict__ t, const float* __restrict__ w,
                                                       const int* __restrict__ idx, int64_t n, float inv_batch,
-                                                      float* grad, double* loss) {
+                                                      float* gpart, double* lpart) {
   extern __shared__ float sm[];
   float* sx = sm;                       // [16][LD]
   float* sh1 = sx + MLP_IN * LD;        // [32][LD]
@@ -126,23 +128,51 @@ __global__ void __launch_bounds__(TB) mlp_grad_kernel(const float* __restrict__ 
     } else {
       for (int j = 0; j < TB; ++j) acc += sdz[j];
     }
-    atomicAdd(grad + p, acc);
+    gpart[size_t(blockIdx.x) * MLP_PARAMS + p] = acc;
   }
+  __shared__ double wl[TB / 32];
   for (int off = 16; off > 0; off >>= 1) lossv += __shfl_xor_sync(0xffffffffu, lossv, off);
-  if ((r & 31) == 0) atomicAdd(loss, double(lossv));
+  if ((r & 31) == 0) wl[r >> 5] = double(lossv);
+  __syncthreads();
+  if (r == 0) {
+    double l = 0.0;
+    for (int k = 0; k < TB / 32; ++k) l += wl[k];
+    lpart[blockIdx.x] = l;
+  }
 }
 
-__global__ void mlp_adam_kernel(float* W, float* g, float* m, float* v, int n, float lr, float b1, float b2, float eps,
-                                float c1, float c2) {
+// The block partials of one gradient evaluation summed in block order: grad[p], and the loss into
+// *loss (added to it).
+__global__ void mlp_reduce_kernel(const float* gpart, const double* lpart, int nblk, float* grad, double* loss) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < MLP_PARAMS) {
+    float g = 0.0f;
+    for (int b = 0; b < nblk; ++b) g += gpart[size_t(b) * MLP_PARAMS + p];
+    grad[p] = g;
+  }
+  if (p == 0) {
+    double l = *loss;
+    for (int b = 0; b < nblk; ++b) l += lpart[b];
+    *loss = l;
+  }
+}
+
+__global__ void mlp_adam_kernel(float* W, const float* gpart, const double* lpart, int nblk, double* loss, float* m,
+                                float* v, int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0) {   // the batch's loss, in block order
+    double l = *loss;
+    for (int b = 0; b < nblk; ++b) l += lpart[b];
+    *loss = l;
+  }
   if (p >= n) return;
-  const float gg = g[p];
+  float gg = 0.0f;
+  for (int b = 0; b < nblk; ++b) gg += gpart[size_t(b) * n + p];
   const float mm = b1 * m[p] + (1.0f - b1) * gg;
   const float vv = b2 * v[p] + (1.0f - b2) * gg * gg;
   m[p] = mm;
   v[p] = vv;
   W[p] -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
-  g[p] = 0.0f;
 }
 
 #define MLP_CUDA(call)                                                                           \
@@ -187,16 +217,19 @@ extern "C" int hg_mlp_grad(const float* params, const float* X, const float* t, 
     if (!params || !X || !t || !loss || !grad || n <= 0) return 1;
     grad_smem_attr();
     DevBuf dW(MLP_PARAMS * sizeof(float)), dX(size_t(n) * MLP_IN * sizeof(float)), dt(size_t(n) * sizeof(float));
+    const int nblk = int((n + TB - 1) / TB);
     DevBuf dw(size_t(w ? n : 1) * sizeof(float)), dg(MLP_PARAMS * sizeof(float)), dl(sizeof(double));
+    DevBuf gpart(size_t(nblk) * MLP_PARAMS * sizeof(float)), lpart(size_t(nblk) * sizeof(double));
     MLP_CUDA(cudaMemcpy(dW.p, params, MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
     MLP_CUDA(cudaMemcpy(dX.p, X, size_t(n) * MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
     MLP_CUDA(cudaMemcpy(dt.p, t, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
     if (w) MLP_CUDA(cudaMemcpy(dw.p, w, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
-    MLP_CUDA(cudaMemset(dg.p, 0, MLP_PARAMS * sizeof(float)));
     MLP_CUDA(cudaMemset(dl.p, 0, sizeof(double)));
-    mlp_grad_kernel<<<unsigned((n + TB - 1) / TB), TB, GRAD_SMEM>>>(dW.as<float>(), dX.as<float>(), dt.as<float>(),
-                                                                    w ? dw.as<float>() : nullptr, nullptr, n,
-                                                                    1.0f / float(n), dg.as<float>(), dl.as<double>());
+    mlp_grad_kernel<<<unsigned(nblk), TB, GRAD_SMEM>>>(dW.as<float>(), dX.as<float>(), dt.as<float>(),
+                                                       w ? dw.as<float>() : nullptr, nullptr, n, 1.0f / float(n),
+                                                       gpart.as<float>(), lpart.as<double>());
+    mlp_reduce_kernel<<<(MLP_PARAMS + 255) / 256, 256>>>(gpart.as<float>(), lpart.as<double>(), nblk, dg.as<float>(),
+                                                         dl.as<double>());
     MLP_CUDA(cudaGetLastError());
     MLP_CUDA(cudaMemcpy(grad, dg.p, MLP_PARAMS * sizeof(float), cudaMemcpyDeviceToHost));
     double l = 0.0;
@@ -212,13 +245,14 @@ extern "C" int hg_mlp_train(float* params, const float* X, const float* t, const
     if (!params || !X || !t || n <= 0 || n > INT32_MAX || epochs <= 0 || batch <= 0) return 1;
     grad_smem_attr();
     DevBuf dW(MLP_PARAMS * sizeof(float)), dX(size_t(n) * MLP_IN * sizeof(float)), dt(size_t(n) * sizeof(float));
-    DevBuf dw(size_t(w ? n : 1) * sizeof(float)), dg(MLP_PARAMS * sizeof(float)), dm(MLP_PARAMS * sizeof(float));
+    const int nblk_max = int((std::min<int64_t>(batch, n) + TB - 1) / TB);
+    DevBuf dw(size_t(w ? n : 1) * sizeof(float)), dm(MLP_PARAMS * sizeof(float));
     DevBuf dv(MLP_PARAMS * sizeof(float)), dl(sizeof(double)), didx(size_t(n) * sizeof(int));
+    DevBuf gpart(size_t(nblk_max) * MLP_PARAMS * sizeof(float)), lpart(size_t(nblk_max) * sizeof(double));
     MLP_CUDA(cudaMemcpy(dW.p, params, MLP_PARAMS * sizeof(float), cudaMemcpyHostToDevice));
     MLP_CUDA(cudaMemcpy(dX.p, X, size_t(n) * MLP_IN * sizeof(float), cudaMemcpyHostToDevice));
     MLP_CUDA(cudaMemcpy(dt.p, t, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
     if (w) MLP_CUDA(cudaMemcpy(dw.p, w, size_t(n) * sizeof(float), cudaMemcpyHostToDevice));
-    MLP_CUDA(cudaMemset(dg.p, 0, MLP_PARAMS * sizeof(float)));
     MLP_CUDA(cudaMemset(dm.p, 0, MLP_PARAMS * sizeof(float)));
     MLP_CUDA(cudaMemset(dv.p, 0, MLP_PARAMS * sizeof(float)));
     std::vector<int> perm(static_cast<size_t>(n));
@@ -232,13 +266,15 @@ extern "C" int hg_mlp_train(float* params, const float* X, const float* t, const
       MLP_CUDA(cudaMemset(dl.p, 0, sizeof(double)));
       for (int64_t b0 = 0; b0 < n; b0 += batch) {
         const int64_t bs = std::min<int64_t>(batch, n - b0);
-        mlp_grad_kernel<<<unsigned((bs + TB - 1) / TB), TB, GRAD_SMEM>>>(
+        const int nblk = int((bs + TB - 1) / TB);
+        mlp_grad_kernel<<<unsigned(nblk), TB, GRAD_SMEM>>>(
             dW.as<float>(), dX.as<float>(), dt.as<float>(), w ? dw.as<float>() : nullptr, didx.as<int>() + b0, bs,
-            1.0f / float(bs), dg.as<float>(), dl.as<double>());
+            1.0f / float(bs), gpart.as<float>(), lpart.as<double>());
         ++step;
         const float c1 = 1.0f - std::pow(b1, float(step)), c2 = 1.0f - std::pow(b2, float(step));
-        mlp_adam_kernel<<<(MLP_PARAMS + 255) / 256, 256>>>(dW.as<float>(), dg.as<float>(), dm.as<float>(),
-                                                            dv.as<float>(), MLP_PARAMS, float(lr), b1, b2, eps, c1, c2);
+        mlp_adam_kernel<<<(MLP_PARAMS + 255) / 256, 256>>>(dW.as<float>(), gpart.as<float>(), lpart.as<double>(), nblk,
+                                                            dl.as<double>(), dm.as<float>(), dv.as<float>(), MLP_PARAMS,
+                                                            float(lr), b1, b2, eps, c1, c2);
       }
       MLP_CUDA(cudaGetLastError());
       double l = 0.0;
