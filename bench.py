@@ -875,6 +875,7 @@ def run_kh(args, rank, world, local, dist):
                              "kernel_share": roof32["share"],
                              "sensor": {"training_s": train_s, "training_snapshots": 200,
                                         "troubled_fraction": troubled,
+                                        "fires_on_this_workload": bool(troubled > 0.0),
                                         "ood_fraction": float(out32[:, 2].mean()),
                                         "disagreement_vs_modal": S.disagreement(out32[:, 0], out32[:, 3]),
                                         "note": ("the learned indicator runs every step (inference fused into the "
