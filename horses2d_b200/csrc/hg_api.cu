@@ -1560,6 +1560,15 @@ extern "C" int hg_get_tiling(const hg_ctx* c, int32_t out[3]) {
   return 0;
 }
 
+// A device buffer freed when it goes out of scope (cudaFree waits for the device).
+struct DevMem {
+  double* p = nullptr;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { if (p) cudaFree(p); }
+};
+
 extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* ms_per_variant) {
   if (!c) return 1;
   cudaEvent_t ev[2] = {nullptr, nullptr};
@@ -1599,12 +1608,29 @@ extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* m
     HG_CUDA(cudaEventCreate(&ev[1]));
     double best = 0.0;
     int best_v = 0;
+    // Single-order contexts time whole RK3 steps with dt = 0: every stage's launches as a step runs them
+    // (updates, fused epilogues, the indicator on the last stage).  Q + 0 * G keeps the values but may
+    // turn a -0 into +0, so the state is saved before and put back after, with its traces and indicator
+    // formed again as hg_set_state forms them.  The parts of a mixed-order mesh, which are never stepped
+    // alone, time residual launches of the resident state.
+    const bool steps = !c->is_part;
+    DevMem saved;
+    if (steps) {
+      saved.p = dalloc<double>(size_t(c->ndof));
+      HG_CUDA(cudaMemcpyAsync(saved.p, c->d_Q, size_t(c->ndof) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    }
     for (int v = 0; v < HG_TILINGS; ++v) {
       c->tiling = v;
-      // residual launches of the resident state (no update): the stage's full arithmetic and loads
-      for (int w = 0; w < 2; ++w) ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
+      if (steps) {
+        one_step(c, HG_SCHEME_RK3, 0.0, 0.0);
+      } else {
+        for (int w = 0; w < 2; ++w) ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
+      }
       HG_CUDA(cudaEventRecord(ev[0], c->stream));
-      for (int k = 0; k < trials; ++k) ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
+      for (int k = 0; k < trials; ++k) {
+        if (steps) one_step(c, HG_SCHEME_RK3, 0.0, 0.0);
+        else ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), false);
+      }
       HG_CUDA(cudaEventRecord(ev[1], c->stream));
       HG_CUDA(cudaEventSynchronize(ev[1]));
       float ms = 0.f;
@@ -1614,6 +1640,12 @@ extern "C" int hg_autotune(hg_ctx* c, int32_t trials, int32_t* chosen, double* m
       if (v == 0 || per < best) { best = per; best_v = v; }
     }
     c->tiling = best_v;
+    if (steps) {   // the resident state back, and what hg_set_state forms from it
+      HG_CUDA(cudaMemcpyAsync(c->d_Q, saved.p, size_t(c->ndof) * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      c->cur = 0;
+      traces(c);
+      ns_prologue(c);
+    }
     // leave the residual partials of the resident state in the chosen layout (as hg_time_derivative)
     ctx_stage(c, 0.0, 0.0, 0.0, true, false, qdot_target(c), true);
     HG_CUDA(cudaGetLastError());

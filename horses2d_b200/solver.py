@@ -325,8 +325,9 @@ class GpuDGSEM:
         return out
 
     def autotune(self, trials=10):
-        """Time the elements-per-CTA variants on the resident state and keep the fastest:
-        {"chosen": variant, "ms": [ms per residual evaluation per variant], "tiling": get_tiling()}."""
+        """Time the elements-per-CTA variants on the resident state (RK3 steps with dt = 0; the state is
+        kept) and keep the fastest: {"chosen": variant, "ms": [ms per step per variant -- per residual
+        evaluation on a mixed-order mesh], "tiling": get_tiling()}."""
         ch = C.c_int32(0)
         ms = np.zeros(L.TILINGS)
         self._check(self._lib.hg_autotune(self._h, int(trials), C.byref(ch), ms.ctypes.data_as(L.F64P)))

@@ -266,10 +266,13 @@ const char* hg_group_last_error(const hg_group* group);   /* group may be NULL: 
 /* Elements-per-CTA autotuner (no reference counterpart).  The stage kernels exist in
  * HG_TILINGS tilings: variant 0 packs several elements per CTA (fewer, larger CTAs), variant 1
  * one or two (more CTAs in flight: small meshes, the smaller buckets of an ensemble).
- * hg_autotune times `trials` residual evaluations of the resident state in each variant with
- * CUDA events on the context's stream, keeps the faster one (chosen, and ms per evaluation
- * for each variant in ms_per_variant[HG_TILINGS], both may be NULL), and leaves the residual
- * of the resident state for hg_residuals as hg_time_derivative does; the state is not changed.
+ * hg_autotune times `trials` RK3 steps with dt = 0 in each variant (every stage's launches,
+ * fused epilogues and the indicator included, while Q + 0 * G leaves the state as it was; the
+ * parts of a mixed-order mesh time residual evaluations instead) with CUDA events on the
+ * context's stream, keeps the faster one (chosen, and ms per step -- per evaluation for
+ * mixed-order meshes -- for each variant in ms_per_variant[HG_TILINGS], both may be NULL), and
+ * leaves the residual of the resident state for hg_residuals as hg_time_derivative does; the
+ * state is not changed.
  * hg_set_tiling forces a variant; hg_get_tiling: out = {variant, elements per CTA, threads
  * per CTA}.  Results are the same in every variant to rounding of the per-CTA reductions. */
 #define HG_TILINGS 2

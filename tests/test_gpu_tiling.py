@@ -83,3 +83,35 @@ def test_autotune_keeps_state_and_residual():
     assert t["elements_per_cta"] >= 1 and t["threads_per_cta"] % 32 == 0
     with pytest.raises(hg.HorsesGpuError):
         g.set_tiling(hg.lib.TILINGS)
+
+
+def test_autotune_of_a_fused_ip_context_leaves_it_as_set_state_does():
+    """The autotuner times RK3 steps with dt = 0 and puts the state back; a fused interior-penalty context
+    with the modal indicator (gradient traces and indicator formed in the stage epilogues) then steps
+    exactly as a context that was only given the state, in the same tiling."""
+    from horses2d_b200 import mesh as hmesh, cases
+    n, N = 12, 5
+    m = hmesh.cartesian(n, n, 0.0, 1.0, 0.0, 1.0)
+    orc = O.Oracle(m, N, nodes=O.LG, riemann=O.ROE, mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=O.IP,
+                   ip_method=0, sigma0_ip=10.0, bcs=hmesh.periodic_bcs_cartesian())
+    X = orc.coords()
+    Q = perturbed(cases.kelvin_helmholtz(X[:, 0], X[:, 1], seed=5).ravel(), 1e-3, seed=6)
+
+    def ctx():
+        g = hg.GpuDGSEM(orc.export_mesh(), mach=0.3, reynolds=1.0e4, navier_stokes=1, viscous=hg.IP,
+                        ip_method=hg.SIPG, sigma0_ip=10.0, node_type=hg.NODES_LG, riemann=hg.ROE,
+                        av_type=hg.AV_LAPLACIAN, av_intensity=1.0, bcs=[dict(type=hg.BC_PERIODIC)] * 4)
+        g.set_sensor(hg.SENSOR_MODAL)
+        g.set_state(Q)
+        return g
+
+    a, b = ctx(), ctx()
+    r = a.autotune(trials=3)
+    assert np.array_equal(a.state(), Q)
+    b.set_tiling(r["chosen"])
+    dt = 0.05 / n ** 2
+    for s in range(3):
+        a.time_step(hg.SCHEME_RK3, s * dt, dt)
+        b.time_step(hg.SCHEME_RK3, s * dt, dt)
+    assert np.array_equal(a.state(), b.state())
+    np.testing.assert_array_equal(a.element_viscosity(), b.element_viscosity())
